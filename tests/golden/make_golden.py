@@ -1,0 +1,156 @@
+"""Regenerates the golden fixtures in this directory from the reference itself.
+
+Run from the repository root, on a machine where the reference sources are
+present (they are compiled by oracle/Makefile into oracle/_ref/):
+
+    python tests/golden/make_golden.py
+
+What it writes, and where each number comes from:
+
+* graph500-scale10.el64 -- written by the reference's own generator
+  (oracle/_ref/rmat_dataset_dump graph500-scale10, one OpenMP thread: its
+  output depends on the thread count).  Pins the el64 format end to end.
+* ref_scale10.npz -- oracle/_ref/ref_dump on that file: the reference's CSR
+  (insertion order), the 8 roots of lcg(0), and for each of the four
+  reference algorithms the parent array, bottom-up flags, queue level
+  boundaries, m_c and the reference's own check() verdict.
+* ref_gen12.npz -- the same reference run on the project's seeded generator
+  output at scale 12 (seed 12), so parents/levels can be compared at full
+  detail on a graph the device generator must reproduce byte for byte.
+* golden.json -- hashes and per-root summaries: sha256 of the generator's
+  el64 files (scale 12 and 16), and for scale 16 (seed 16, 8 roots of lcg(0))
+  the reference's m_c, per-step discovered counts, per-level directions and
+  the sha256 of the depth array derived from the reference's parent tree.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from oracle import oracle as O  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_ALGS = ["beamer_hybrid", "migrating_threads", "remote_writes", "remote_writes_hybrid"]
+
+
+def sha256_file(path):
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for chunk in iter(lambda: f.read(1 << 20), b""):
+            h.update(chunk)
+    return h.hexdigest()
+
+
+def ref_dump(graph, out, alg="beamer_hybrid", roots=8, dump_graph=False):
+    cmd = [os.path.join(O.REF_DIR, "ref_dump"), "--graph_filename", graph, "--out", out,
+           "--algorithm", alg, "--num_trials", str(roots)]
+    if dump_graph:
+        cmd.append("--dump_graph")
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+    return O.read_ref_dump(out)
+
+
+def level_dirs(parent, flags, root):
+    """Direction that produced each non-empty level, from the reference's
+    new_parent_ marks (>= 0 exactly for bottom-up discoveries)."""
+    depth = O.depth_from_parents(parent, root)
+    out = []
+    for lv in range(1, int(depth.max()) + 1):
+        f = flags[depth == lv]
+        assert f.min() == f.max(), "mixed directions within one level"
+        out.append("B" if f[0] else "T")
+    return "".join(out), depth
+
+
+def pack_roots(d):
+    k = len(d["roots"])
+    n = d["n"]
+    heads_len = max(len(r["heads"]) for r in d["roots"])
+    heads = np.full((k, heads_len), -1, np.int64)
+    for i, r in enumerate(d["roots"]):
+        heads[i, : len(r["heads"])] = r["heads"]
+    return {
+        "roots": np.array([r["root"] for r in d["roots"]], np.int64),
+        "parent": np.stack([r["parent"] for r in d["roots"]]).reshape(k, n),
+        "bottom_up": np.stack([r["bottom_up"] for r in d["roots"]]).reshape(k, n),
+        "heads": heads,
+        "m_c": np.array([r["m_c"] for r in d["roots"]], np.int64),
+        "check": np.array([r["check"] for r in d["roots"]], np.bool_),
+    }
+
+
+def main():
+    O.build()
+    if not os.path.exists(os.path.join(O.REF_DIR, "ref_dump")):
+        sys.exit("reference builds missing: the reference sources are needed")
+    golden = {"generator": {"a": 0.57, "b": 0.19, "c": 0.19, "d": 0.05, "edge_factor": 16}}
+
+    # 1. reference generator output, scale 10
+    el10 = os.path.join(HERE, "graph500-scale10.el64")
+    with tempfile.TemporaryDirectory() as tmp:
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        subprocess.run([os.path.join(O.REF_DIR, "rmat_dataset_dump"), "graph500-scale10"],
+                       cwd=tmp, env=env, check=True, stderr=subprocess.DEVNULL)
+        os.replace(os.path.join(tmp, "graph500-scale10"), el10)
+        arrays = {}
+        for i, alg in enumerate(REF_ALGS):
+            d = ref_dump(el10, os.path.join(tmp, "s10.bin"), alg, 8, dump_graph=(i == 0))
+            if i == 0:
+                arrays["offsets"] = d["offsets"]
+                arrays["adj"] = d["adj"]
+            for key, val in pack_roots(d).items():
+                arrays[f"{alg}.{key}"] = val
+        np.savez_compressed(os.path.join(HERE, "ref_scale10.npz"), **arrays)
+        golden["graph500-scale10.el64"] = {"sha256": sha256_file(el10)}
+
+        # 2. project generator, scale 12, full detail
+        n, src, dst = O.rmat_graph(12, seed=12)
+        el12 = os.path.join(tmp, "gen12.el64")
+        O.el64_write(el12, n, src, dst)
+        d = ref_dump(el12, os.path.join(tmp, "g12.bin"), "beamer_hybrid", 8)
+        arrays = pack_roots(d)
+        arrays["num_edges"] = np.array([len(src)], np.int64)
+        np.savez_compressed(os.path.join(HERE, "ref_gen12.npz"), **arrays)
+        golden["gen12"] = {"scale": 12, "seed": 12, "num_edges": int(len(src)),
+                           "el64_sha256": sha256_file(el12)}
+
+        # 3. project generator, scale 16: hashes and per-root summaries
+        n, src, dst = O.rmat_graph(16, seed=16)
+        el16 = os.path.join(tmp, "gen16.el64")
+        O.el64_write(el16, n, src, dst)
+        off, adj = O.csr_build(n, src, dst)
+        d = ref_dump(el16, os.path.join(tmp, "g16.bin"), "beamer_hybrid", 8)
+        roots = []
+        for r in d["roots"]:
+            dirs, depth = level_dirs(r["parent"], r["bottom_up"], r["root"])
+            roots.append({
+                "root": r["root"],
+                "check": r["check"],
+                "m_c": r["m_c"],
+                "found": np.diff(r["heads"]).tolist(),
+                "level_dirs": dirs,
+                "depth_sha256": hashlib.sha256(depth.astype("<i4").tobytes()).hexdigest(),
+                "reference_ms": round(r["ms"], 3),
+            })
+        golden["gen16"] = {
+            "scale": 16, "seed": 16, "num_edges": int(len(src)),
+            "el64_sha256": sha256_file(el16),
+            "csr_sha256": hashlib.sha256(off.astype("<i8").tobytes()
+                                         + adj.astype("<u4").tobytes()).hexdigest(),
+            "alpha": 15, "beta": 18, "roots": roots,
+        }
+    with open(os.path.join(HERE, "golden.json"), "w") as f:
+        json.dump(golden, f, indent=1)
+        f.write("\n")
+
+
+if __name__ == "__main__":
+    main()
