@@ -1,0 +1,397 @@
+"""beedrill_b200 -- Python view of the B200 direction-optimizing BFS.
+
+A thin ctypes layer over the C ABI in include/beedrill_b200.h
+(beedrill_b200/lib/libbeedrill_b200.so).  Class and method names follow the
+reference's hybrid_bfs class (hybrid_bfs.h:11-47) so code written against the
+reference reads the same:
+
+    g = Graph.from_el64("graph500-scale16")
+    bfs = HybridBFS(g)                      # hybrid_bfs(graph&)
+    bfs.clear()                             # hybrid_bfs::clear
+    bfs.run_beamer(src, 15, 18)             # hybrid_bfs::run_beamer
+    assert bfs.check(src)                   # hybrid_bfs::check
+    m_c = bfs.count_num_traversed_edges()   # hybrid_bfs::count_num_traversed_edges
+
+Every call runs on the GPU through the shared library; there is no CPU
+fallback.  If the library is missing or no sm_100 device is present the
+calls raise BeedrillError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, Structure, byref, c_char_p, c_double, c_int, c_int32, c_int64, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+__all__ = ["BeedrillError", "Graph", "HybridBFS", "Step", "ALGORITHMS", "lib", "LIB_PATH"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libbeedrill_b200.so")
+
+BD_OK = 0
+STATUS_NAMES = {
+    0: "BD_OK", -1: "BD_ERR_INVALID", -2: "BD_ERR_IO", -3: "BD_ERR_FORMAT", -4: "BD_ERR_OOM",
+    -5: "BD_ERR_CUDA", -6: "BD_ERR_TIMEOUT", -7: "BD_ERR_RANGE", -8: "BD_ERR_STATE",
+    -9: "BD_ERR_NODEV", -10: "BD_ERR_LIMIT",
+}
+ORDER_INSERTION, ORDER_SORTED = 0, 1
+ALG_BEAMER, ALG_TOP_DOWN, ALG_BOTTOM_UP, ALG_LEARNED = 0, 1, 2, 3
+
+# The reference's --algorithm values (hybrid_bfs_main.cc:228-245) plus the
+# directions and the learned policy of this implementation.
+ALGORITHMS = {
+    "beamer_hybrid": ALG_BEAMER,
+    "remote_writes_hybrid": ALG_BEAMER,
+    "migrating_threads": ALG_TOP_DOWN,
+    "remote_writes": ALG_TOP_DOWN,
+    "top_down": ALG_TOP_DOWN,
+    "bottom_up": ALG_BOTTOM_UP,
+    "learned": ALG_LEARNED,
+}
+
+
+class BeedrillError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        msg = _lib_status_string(status)
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)} ({msg})")
+
+
+class BfsOpts(Structure):
+    _fields_ = [
+        ("alg", c_int32), ("min_parent", c_int32), ("alpha", c_int64), ("beta", c_int64),
+        ("block_size", c_int32), ("large_degree", c_int32), ("chunk_edges", c_int32),
+        ("bu_prefix", c_int32), ("spin_limit", c_int64), ("test_extra_ctas", c_int32),
+        ("reserved", c_int32),
+    ]
+
+
+class Step(Structure):
+    _fields_ = [
+        ("dir", c_int32), ("level", c_int32), ("frontier", c_int64), ("frontier_edges", c_int64),
+        ("unexplored_edges", c_int64), ("found", c_int64), ("ns", c_int64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class RunStats(Structure):
+    _fields_ = [
+        ("ms", c_double), ("num_steps", c_int64), ("reached", c_int64),
+        ("traversed_edges", c_int64), ("top_down_steps", c_int64), ("bottom_up_steps", c_int64),
+    ]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libbeedrill_b200.so (built by `make`); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `make` (or __graft_entry__.build())")
+    L = ctypes.CDLL(LIB_PATH)
+    i64p, u32p, i32p = POINTER(c_int64), POINTER(c_uint32), POINTER(c_int32)
+    vpp = POINTER(c_void_p)
+    sig = {
+        "bd_status_string": (c_char_p, [c_int]),
+        "bd_version": (c_char_p, []),
+        "bd_set_device": (c_int, [c_int]),
+        "bd_graph_from_el64": (c_int, [c_char_p, c_int32, vpp]),
+        "bd_graph_from_edges": (c_int, [c_int64, c_int64, i64p, i64p, c_int32, vpp]),
+        "bd_graph_from_csr": (c_int, [c_int64, c_int64, i64p, u32p, vpp]),
+        "bd_graph_rmat": (c_int, [c_int32, c_int64, c_double, c_double, c_double, c_double,
+                                  c_uint64, c_int32, vpp]),
+        "bd_graph_concat": (c_int, [vpp, c_int64, vpp, i64p]),
+        "bd_graph_info": (c_int, [c_void_p, i64p, i64p]),
+        "bd_graph_copy_csr": (c_int, [c_void_p, i64p, u32p]),
+        "bd_graph_copy_edges": (c_int, [c_void_p, i64p, i64p]),
+        "bd_graph_write_el64": (c_int, [c_void_p, c_char_p]),
+        "bd_graph_check": (c_int, [c_void_p, i32p]),
+        "bd_graph_pick_roots": (c_int, [c_void_p, c_uint64, c_int64, i64p]),
+        "bd_graph_device_csr": (c_int, [c_void_p, vpp, vpp]),
+        "bd_graph_destroy": (c_int, [c_void_p]),
+        "bd_bfs_default_opts": (None, [POINTER(BfsOpts)]),
+        "bd_bfs_create": (c_int, [c_void_p, POINTER(BfsOpts), vpp]),
+        "bd_bfs_clear": (c_int, [c_void_p]),
+        "bd_bfs_run": (c_int, [c_void_p, c_int64, POINTER(RunStats)]),
+        "bd_bfs_run_beamer": (c_int, [c_void_p, c_int64, c_int64, c_int64, POINTER(RunStats)]),
+        "bd_bfs_run_top_down": (c_int, [c_void_p, c_int64, POINTER(RunStats)]),
+        "bd_bfs_run_bottom_up": (c_int, [c_void_p, c_int64, POINTER(RunStats)]),
+        "bd_bfs_run_multi": (c_int, [c_void_p, i64p, c_int64, POINTER(RunStats)]),
+        "bd_bfs_run_many": (c_int, [c_void_p, i64p, c_int64, POINTER(c_double), i64p, i64p,
+                                    POINTER(c_double)]),
+        "bd_bfs_get_depths": (c_int, [c_void_p, i32p]),
+        "bd_bfs_get_parents": (c_int, [c_void_p, i64p]),
+        "bd_bfs_device_ptrs": (c_int, [c_void_p, vpp, vpp]),
+        "bd_bfs_count_traversed_edges": (c_int, [c_void_p, i64p]),
+        "bd_bfs_check": (c_int, [c_void_p, c_int64, i32p]),
+        "bd_bfs_get_steps": (c_int, [c_void_p, POINTER(Step), c_int64, i64p]),
+        "bd_bfs_destroy": (c_int, [c_void_p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _lib_status_string(status: int) -> str:
+    try:
+        return lib().bd_status_string(status).decode()
+    except Exception:  # library not loadable: the caller's message says why
+        return "?"
+
+
+def _check(status: int, what: str) -> None:
+    if status != BD_OK:
+        raise BeedrillError(status, what)
+
+
+def _ptr(a: np.ndarray, ct):
+    return a.ctypes.data_as(POINTER(ct))
+
+
+class Graph:
+    """A graph resident in HBM (CSR: int64 offsets, uint32 neighbour ids)."""
+
+    def __init__(self, handle: c_void_p):
+        self._h = handle
+
+    # -- construction -------------------------------------------------------
+    @classmethod
+    def from_el64(cls, path: str, order: int = ORDER_INSERTION) -> "Graph":
+        h = c_void_p()
+        _check(lib().bd_graph_from_el64(os.fsencode(path), order, byref(h)), f"load {path}")
+        return cls(h)
+
+    @classmethod
+    def from_edges(cls, num_vertices: int, src, dst, order: int = ORDER_INSERTION) -> "Graph":
+        src = np.ascontiguousarray(src, np.int64)
+        dst = np.ascontiguousarray(dst, np.int64)
+        if src.shape != dst.shape:
+            raise ValueError("src and dst differ in length")
+        h = c_void_p()
+        _check(lib().bd_graph_from_edges(num_vertices, len(src), _ptr(src, c_int64),
+                                         _ptr(dst, c_int64), order, byref(h)), "from_edges")
+        return cls(h)
+
+    @classmethod
+    def from_csr(cls, offsets, adjacency) -> "Graph":
+        off = np.ascontiguousarray(offsets, np.int64)
+        adj = np.ascontiguousarray(adjacency, np.uint32)
+        h = c_void_p()
+        _check(lib().bd_graph_from_csr(len(off) - 1, len(adj), _ptr(off, c_int64),
+                                       _ptr(adj, c_uint32), byref(h)), "from_csr")
+        return cls(h)
+
+    @classmethod
+    def rmat(cls, scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19,
+             c: float = 0.19, d: float = 0.05, seed: int = 0,
+             order: int = ORDER_INSERTION) -> "Graph":
+        h = c_void_p()
+        _check(lib().bd_graph_rmat(scale, edge_factor, a, b, c, d, seed, order, byref(h)),
+               f"rmat(scale={scale})")
+        return cls(h)
+
+    @classmethod
+    def concat(cls, graphs) -> tuple["Graph", np.ndarray]:
+        arr = (c_void_p * len(graphs))(*[g._h.value for g in graphs])
+        base = np.zeros(len(graphs) + 1, np.int64)
+        h = c_void_p()
+        _check(lib().bd_graph_concat(ctypes.cast(arr, POINTER(c_void_p)), len(graphs), byref(h),
+                                     _ptr(base, c_int64)), "concat")
+        return cls(h), base
+
+    # -- queries ------------------------------------------------------------
+    def num_vertices(self) -> int:
+        n = c_int64()
+        _check(lib().bd_graph_info(self._h, byref(n), None), "info")
+        return n.value
+
+    def num_edges(self) -> int:
+        m = c_int64()
+        _check(lib().bd_graph_info(self._h, None, byref(m)), "info")
+        return m.value
+
+    def csr(self):
+        n = self.num_vertices()
+        off = np.empty(n + 1, np.int64)
+        lib().bd_graph_copy_csr(self._h, _ptr(off, c_int64), None)
+        adj = np.empty(int(off[-1]), np.uint32)
+        _check(lib().bd_graph_copy_csr(self._h, _ptr(off, c_int64), _ptr(adj, c_uint32)), "csr")
+        return off, adj
+
+    def edges(self):
+        m = self.num_edges()
+        src = np.empty(m, np.int64)
+        dst = np.empty(m, np.int64)
+        _check(lib().bd_graph_copy_edges(self._h, _ptr(src, c_int64), _ptr(dst, c_int64)), "edges")
+        return src, dst
+
+    def write_el64(self, path: str) -> None:
+        _check(lib().bd_graph_write_el64(self._h, os.fsencode(path)), f"write {path}")
+
+    def check(self) -> bool:
+        ok = c_int32()
+        _check(lib().bd_graph_check(self._h, byref(ok)), "graph check")
+        return bool(ok.value)
+
+    def pick_roots(self, seed: int, k: int) -> np.ndarray:
+        roots = np.empty(k, np.int64)
+        _check(lib().bd_graph_pick_roots(self._h, seed, k, _ptr(roots, c_int64)), "pick_roots")
+        return roots
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            lib().bd_graph_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HybridBFS:
+    """Mirror of the reference's hybrid_bfs class on the GPU."""
+
+    def __init__(self, graph: Graph, alg: str = "beamer_hybrid", alpha: int = 15,
+                 beta: int = 18, min_parent: bool = False, block_size: int = 0,
+                 large_degree: int = 0, chunk_edges: int = 0, bu_prefix: int = 0,
+                 spin_limit: int = 0, test_extra_ctas: int = 0):
+        if alg not in ALGORITHMS:
+            raise ValueError(f"Algorithm '{alg}' not implemented!")
+        self.graph = graph  # keeps the graph alive
+        o = BfsOpts()
+        lib().bd_bfs_default_opts(byref(o))
+        o.alg = ALGORITHMS[alg]
+        o.alpha, o.beta = alpha, beta
+        o.min_parent = int(bool(min_parent))
+        o.block_size, o.large_degree, o.chunk_edges = block_size, large_degree, chunk_edges
+        o.bu_prefix, o.spin_limit, o.test_extra_ctas = bu_prefix, spin_limit, test_extra_ctas
+        self.alg = alg
+        self.alpha, self.beta = alpha, beta
+        self._h = c_void_p()
+        _check(lib().bd_bfs_create(graph._h, byref(o), byref(self._h)), "hybrid_bfs")
+        self.last_stats = RunStats()
+
+    # hybrid_bfs::clear (hybrid_bfs.cc:433-443)
+    def clear(self) -> None:
+        _check(lib().bd_bfs_clear(self._h), "clear")
+
+    def run(self, source: int) -> RunStats:
+        """Run with the policy chosen at construction (the --alg dispatch of
+        hybrid_bfs_main.cc:268-281)."""
+        _check(lib().bd_bfs_run(self._h, source, byref(self.last_stats)), "run")
+        return self.last_stats
+
+    # hybrid_bfs::run_beamer (hybrid_bfs.cc:152-191)
+    def run_beamer(self, source: int, alpha: int = 15, beta: int = 18) -> RunStats:
+        _check(lib().bd_bfs_run_beamer(self._h, source, alpha, beta, byref(self.last_stats)),
+               "run_beamer")
+        return self.last_stats
+
+    # hybrid_bfs::run_with_remote_writes_hybrid (hybrid_bfs.cc:243-277): the
+    # same Beamer switch; its top-down flavour is an Emu artefact.
+    def run_with_remote_writes_hybrid(self, source: int, alpha: int = 15, beta: int = 18):
+        return self.run_beamer(source, alpha, beta)
+
+    def run_top_down(self, source: int) -> RunStats:
+        _check(lib().bd_bfs_run_top_down(self._h, source, byref(self.last_stats)), "top_down")
+        return self.last_stats
+
+    # hybrid_bfs::run_with_migrating_threads / run_with_remote_writes
+    # (hybrid_bfs.cc:196-235): top-down only.
+    run_with_migrating_threads = run_top_down
+    run_with_remote_writes = run_top_down
+
+    def run_bottom_up(self, source: int) -> RunStats:
+        _check(lib().bd_bfs_run_bottom_up(self._h, source, byref(self.last_stats)), "bottom_up")
+        return self.last_stats
+
+    def run_multi(self, sources) -> RunStats:
+        src = np.ascontiguousarray(sources, np.int64)
+        _check(lib().bd_bfs_run_multi(self._h, _ptr(src, c_int64), len(src),
+                                      byref(self.last_stats)), "run_multi")
+        return self.last_stats
+
+    def run_many(self, sources, with_reached: bool = False):
+        """k BFSs back to back (clear() before each); returns per-root ms,
+        per-root m_c, [per-root n_c,] and the device time of the whole call
+        including the root upload and the result download."""
+        src = np.ascontiguousarray(sources, np.int64)
+        ms = np.empty(len(src), np.float64)
+        edges = np.empty(len(src), np.int64)
+        reached = np.empty(len(src), np.int64)
+        e2e = c_double()
+        _check(lib().bd_bfs_run_many(self._h, _ptr(src, c_int64), len(src), _ptr(ms, c_double),
+                                     _ptr(edges, c_int64), _ptr(reached, c_int64), byref(e2e)),
+               "run_many")
+        if with_reached:
+            return ms, edges, reached, e2e.value
+        return ms, edges, e2e.value
+
+    # hybrid_bfs::check (hybrid_bfs.cc:281-379)
+    def check(self, source: int) -> bool:
+        ok = c_int32()
+        _check(lib().bd_bfs_check(self._h, source, byref(ok)), "check")
+        return bool(ok.value)
+
+    # hybrid_bfs::count_num_traversed_edges (hybrid_bfs.cc:401-414)
+    def count_num_traversed_edges(self) -> int:
+        out = c_int64()
+        _check(lib().bd_bfs_count_traversed_edges(self._h, byref(out)), "count")
+        return out.value
+
+    def depths(self) -> np.ndarray:
+        d = np.empty(self.graph.num_vertices(), np.int32)
+        _check(lib().bd_bfs_get_depths(self._h, _ptr(d, c_int32)), "depths")
+        return d
+
+    def parents(self) -> np.ndarray:
+        p = np.empty(self.graph.num_vertices(), np.int64)
+        _check(lib().bd_bfs_get_parents(self._h, _ptr(p, c_int64)), "parents")
+        return p
+
+    def steps(self) -> list[dict]:
+        count = c_int64()
+        _check(lib().bd_bfs_get_steps(self._h, None, 0, byref(count)), "steps")
+        buf = (Step * max(count.value, 1))()
+        _check(lib().bd_bfs_get_steps(self._h, buf, count.value, byref(count)), "steps")
+        return [buf[i].as_dict() for i in range(count.value)]
+
+    def directions(self) -> str:
+        return "".join("B" if s["dir"] else "T" for s in self.steps())
+
+    # hybrid_bfs::print_tree (hybrid_bfs.cc:381-399)
+    def print_tree(self) -> None:
+        parent = self.parents()
+        for v in range(len(parent)):
+            p = int(parent[v])
+            if p < 0:
+                continue
+            line = f"{v:4d}"
+            while True:
+                line += f" <- {p:4d}"
+                if p == -1 or p == parent[p]:
+                    break
+                p = int(parent[p])
+            print(line)
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            lib().bd_bfs_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,1259 @@
+// bd_bfs.cu -- the B200 direction-optimizing BFS (hybrid_bfs) and its C ABI.
+//
+// Data layout in HBM for one handle (n vertices, arcs = 2m):
+//   depth   int32[n]      -1 = unvisited; claimed by atomicCAS in top-down
+//   parent  int64[n]      written once per reached vertex; the reference's
+//                         -deg / -1 encoding of unreached vertices is filled
+//                         in lazily (finalize_parents_kernel) when read
+//   vis[2]  uint32[n/32]  visited bitmaps; a bottom-up step reads vis[cur]
+//                         (frozen) and writes whole words of vis[cur^1]
+//   qs[2]   uint32[n]     frontier queue of vertices with degree < large_deg
+//   ql[2], qlb[2]         frontier vertices with degree >= large_deg, with the
+//                         prefix sum of their chunk counts (work units of
+//                         `chunk` edges spread over all warps)
+//   ctrl                  Ctrl block: barrier, Beamer state, step counters
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "bd_bfs_device.cuh"
+#include "bd_internal.h"
+
+namespace bd {
+
+namespace {
+
+constexpr int64_t kRecCap = 1 << 15;
+constexpr long long kDefaultSpin = 4000000;  // ~2 s of polling
+
+// ---------------------------------------------------------------------------
+// small device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return (long long)t;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T x)
+{
+    const int lane = lane_id();
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        T y = __shfl_up_sync(kFull, x, d);
+        if (lane >= d) { x += y; }
+    }
+    return x;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T x)
+{
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) { x += __shfl_xor_sync(kFull, x, d); }
+    return x;
+}
+
+// Per-thread accumulators of one step, reduced once per CTA at its end.
+struct Local {
+    unsigned long long found;
+    unsigned long long degsum;
+};
+
+// The view every CTA takes of the control block at the start of a step.
+struct StepView {
+    int dir;
+    int level;
+    int vis_cur;
+    int q_cur;
+    int step;
+    long long f_small;
+    long long f_large;
+    long long f_chunks;
+};
+
+__device__ __forceinline__ StepView read_view(const Ctrl *c)
+{
+    const volatile Ctrl *vc = c;
+    StepView v;
+    v.dir = vc->dir;
+    v.level = vc->level;
+    v.vis_cur = vc->vis_cur;
+    v.q_cur = vc->q_cur;
+    v.step = vc->step;
+    v.f_small = vc->f_small;
+    v.f_large = vc->f_large;
+    v.f_chunks = vc->f_chunks;
+    return v;
+}
+
+// Warp-collective: appends the lanes' newly discovered vertices (has) to the
+// next frontier, binned by degree.  Small vertices get one slot each in qs;
+// large ones get a slot in ql plus a contiguous range of chunk ids.
+__device__ __forceinline__ void warp_append(const BfsParams &p, Acc *acc, int qout, bool has,
+                                            uint32_t v, int64_t deg, Local &loc)
+{
+    if (has) {
+        loc.found += 1;
+        loc.degsum += (unsigned long long)deg;
+    }
+    const int lane = lane_id();
+    const bool large = has && deg >= (int64_t)p.large_deg;
+    const unsigned sm = __ballot_sync(kFull, has && !large);
+    if (sm) {
+        const int leader = __ffs(sm) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) { base = atomicAdd(&acc->small_cnt, (unsigned long long)__popc(sm)); }
+        base = __shfl_sync(kFull, base, leader);
+        if (has && !large) { p.qs[qout][base + __popc(sm & lanemask_lt())] = v; }
+    }
+    const unsigned lm = __ballot_sync(kFull, large);
+    if (lm) {
+        const unsigned long long nch =
+            large ? (unsigned long long)((deg + p.chunk - 1) / p.chunk) : 0ull;
+        const unsigned long long incl = warp_incl_scan(nch);
+        const unsigned long long total = __shfl_sync(kFull, incl, 31);
+        const int leader = __ffs(lm) - 1;
+        unsigned long long old = 0;
+        if (lane == leader) {
+            old = atomicAdd(&acc->large_packed,
+                            ((unsigned long long)__popc(lm) << kLargeShift) | total);
+        }
+        old = __shfl_sync(kFull, old, leader);
+        if (large) {
+            const unsigned long long pos = (old >> kLargeShift) + __popc(lm & lanemask_lt());
+            p.ql[qout][pos] = v;
+            p.qlb[qout][pos] = (old & kChunkMask) + incl - nch;
+        }
+    }
+}
+
+// Top-down claim (hybrid_bfs.cc:83-96): visited-bit filter, then atomicCAS
+// on the depth word decides the single winner, which writes the parent.
+__device__ __forceinline__ bool td_claim(const BfsParams &p, uint32_t *vis, uint32_t v,
+                                         uint32_t u, int new_level)
+{
+    const uint32_t w = __ldcg(&vis[v >> 5]);
+    if ((w >> (v & 31)) & 1u) { return false; }
+    if (atomicCAS(&p.depth[v], -1, new_level) != -1) { return false; }
+    p.parent[v] = (int64_t)u;
+    atomicOr(&vis[v >> 5], 1u << (v & 31));
+    return true;
+}
+
+__device__ __forceinline__ int64_t degree_of(const BfsParams &p, uint32_t v)
+{
+    return __ldg(&p.off[v + 1]) - __ldg(&p.off[v]);
+}
+
+constexpr int kILP = 4;
+
+// Processes arcs [b, e) of vertex u with all 32 lanes (coalesced reads).
+__device__ __forceinline__ void td_edges_warp(const BfsParams &p, Acc *acc, uint32_t *vis,
+                                              int qout, int new_level, uint32_t u, int64_t b,
+                                              int64_t e, Local &loc)
+{
+    const int lane = lane_id();
+    for (int64_t base = b; base < e; base += 32 * kILP) {
+        uint32_t v[kILP];
+        bool ok[kILP];
+#pragma unroll
+        for (int i = 0; i < kILP; ++i) {
+            const int64_t k = base + i * 32 + lane;
+            ok[i] = k < e;
+            v[i] = ok[i] ? __ldg(&p.adj[k]) : 0u;
+        }
+#pragma unroll
+        for (int i = 0; i < kILP; ++i) {
+            bool c = ok[i] && td_claim(p, vis, v[i], u, new_level);
+            int64_t deg = c ? degree_of(p, v[i]) : 0;
+            warp_append(p, acc, qout, c, v[i], deg, loc);
+        }
+    }
+}
+
+struct WarpScratch {
+    int32_t incl[32];
+    uint32_t u[32];
+    int64_t beg[32];
+};
+
+template <int BLOCK>
+struct SharedState {
+    WarpScratch warp[BLOCK / 32];
+    unsigned long long red_found[BLOCK / 32];
+    unsigned long long red_deg[BLOCK / 32];
+    int is_last;
+    unsigned gen;
+    int exit_flag;
+    float feat[kPolicyIn];
+    float h1[kPolicyH];
+    float h2[kPolicyH];
+    float logit[kPolicyOut];
+    int beamer_dir;
+};
+
+template <int BLOCK>
+__device__ void td_step(const BfsParams &p, const StepView &sv, SharedState<BLOCK> &sh,
+                        Local &loc)
+{
+    const int lane = lane_id();
+    const int warp = threadIdx.x >> 5;
+    const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
+    const long long nw = (long long)gridDim.x * (BLOCK / 32);
+    const int qin = sv.q_cur, qout = sv.q_cur ^ 1;
+    uint32_t *vis = p.vis[sv.vis_cur];
+    Acc *acc = &p.ctrl->acc[sv.step & 1];
+    const int new_level = sv.level + 1;
+
+    // Phase A: chunks of large-degree frontier vertices.
+    const long long nl = sv.f_large;
+    for (long long c = gw; c < sv.f_chunks; c += nw) {
+        long long lo = 0, hi = nl - 1;  // last i with qlb[i] <= c
+        while (lo < hi) {
+            long long mid = (lo + hi + 1) >> 1;
+            if ((long long)__ldcg(&p.qlb[qin][mid]) <= c) { lo = mid; } else { hi = mid - 1; }
+        }
+        const uint32_t u = __ldcg(&p.ql[qin][lo]);
+        const long long j = c - (long long)__ldcg(&p.qlb[qin][lo]);
+        const int64_t ub = __ldg(&p.off[u]), ue = __ldg(&p.off[u + 1]);
+        const int64_t b = ub + j * (int64_t)p.chunk;
+        const int64_t e = min(ue, b + (int64_t)p.chunk);
+        td_edges_warp(p, acc, vis, qout, new_level, u, b, e, loc);
+    }
+
+    // Phase B: small-degree frontier vertices, 32 per warp; their arcs are
+    // laid end to end and dealt to the lanes 32 at a time.
+    WarpScratch &ws = sh.warp[warp];
+    for (long long g = gw; g * 32 < sv.f_small; g += nw) {
+        const long long idx = g * 32 + lane;
+        uint32_t u = 0;
+        int64_t beg = 0;
+        int32_t deg = 0;
+        if (idx < sv.f_small) {
+            u = __ldcg(&p.qs[qin][idx]);
+            beg = __ldg(&p.off[u]);
+            deg = (int32_t)(__ldg(&p.off[u + 1]) - beg);
+        }
+        const int32_t incl = warp_incl_scan(deg);
+        const int32_t total = __shfl_sync(kFull, incl, 31);
+        ws.incl[lane] = incl;
+        ws.u[lane] = u;
+        ws.beg[lane] = beg;
+        __syncwarp();
+        for (int32_t base = 0; base < total; base += 32 * kILP) {
+            uint32_t v[kILP], src[kILP];
+            bool ok[kILP];
+#pragma unroll
+            for (int i = 0; i < kILP; ++i) {
+                const int32_t e = base + i * 32 + lane;
+                ok[i] = e < total;
+                v[i] = 0;
+                src[i] = 0;
+                if (ok[i]) {
+                    int lo = 0, hi = 31;  // first owner with incl > e
+                    while (lo < hi) {
+                        int mid = (lo + hi) >> 1;
+                        if (ws.incl[mid] > e) { hi = mid; } else { lo = mid + 1; }
+                    }
+                    const int32_t excl = lo ? ws.incl[lo - 1] : 0;
+                    src[i] = ws.u[lo];
+                    v[i] = __ldg(&p.adj[ws.beg[lo] + (e - excl)]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < kILP; ++i) {
+                bool c = ok[i] && td_claim(p, vis, v[i], src[i], new_level);
+                int64_t d = c ? degree_of(p, v[i]) : 0;
+                warp_append(p, acc, qout, c, v[i], d, loc);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Bottom-up step (hybrid_bfs.cc:111-143): each warp owns one bitmap word
+// (32 vertices).  Unvisited lanes scan their own neighbour lists (first
+// bu_prefix arcs, 4 loads in flight); lists longer than that are finished by
+// the whole warp, 32 arcs per ballot, stopping at the first hit.  Reads only
+// the frozen bitmap vis[cur]; writes whole words of vis[cur^1].
+template <int BLOCK>
+__device__ void bu_step(const BfsParams &p, const StepView &sv, Local &loc)
+{
+    const int lane = lane_id();
+    const int warp = threadIdx.x >> 5;
+    const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
+    const long long nw = (long long)gridDim.x * (BLOCK / 32);
+    const uint32_t *vin = p.vis[sv.vis_cur];
+    uint32_t *vout = p.vis[sv.vis_cur ^ 1];
+    const int qout = sv.q_cur ^ 1;
+    Acc *acc = &p.ctrl->acc[sv.step & 1];
+    const int new_level = sv.level + 1;
+
+    for (long long w = gw; w < p.words; w += nw) {
+        const uint32_t word = __ldcg(&vin[w]);
+        if (word == kFull) {
+            if (lane == 0) { vout[w] = word; }
+            continue;
+        }
+        const uint32_t v = (uint32_t)(w * 32 + lane);
+        const bool unvisited = !((word >> lane) & 1u);
+        bool found = false;
+        uint32_t par = 0;
+        int64_t beg = 0, end = 0, next = 0;
+        if (unvisited) {
+            beg = __ldg(&p.off[v]);
+            end = __ldg(&p.off[v + 1]);
+            const int64_t lim = min(end, beg + (int64_t)p.bu_prefix);
+            int64_t k = beg;
+            for (; k < lim && !found; k += 4) {
+                uint32_t x[4];
+                uint32_t bits[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) { x[i] = (k + i < lim) ? __ldg(&p.adj[k + i]) : 0u; }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) { bits[i] = (k + i < lim) ? __ldcg(&vin[x[i] >> 5]) : 0u; }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (!found && ((bits[i] >> (x[i] & 31)) & 1u)) {
+                        found = true;
+                        par = x[i];
+                    }
+                }
+            }
+            next = found ? end : lim;
+        }
+        unsigned pending = __ballot_sync(kFull, unvisited && !found && next < end);
+        while (pending) {
+            const int owner = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const int64_t b = __shfl_sync(kFull, next, owner);
+            const int64_t e = __shfl_sync(kFull, end, owner);
+            for (int64_t base = b; base < e; base += 32) {
+                const int64_t k = base + lane;
+                bool hit = false;
+                uint32_t x = 0;
+                if (k < e) {
+                    x = __ldg(&p.adj[k]);
+                    hit = (__ldcg(&vin[x >> 5]) >> (x & 31)) & 1u;
+                }
+                const unsigned hm = __ballot_sync(kFull, hit);
+                if (hm) {
+                    const uint32_t hx = __shfl_sync(kFull, x, __ffs(hm) - 1);
+                    if (lane == owner) {
+                        found = true;
+                        par = hx;
+                    }
+                    break;
+                }
+            }
+        }
+        const unsigned fm = __ballot_sync(kFull, found);
+        if (lane == 0) { vout[w] = word | fm; }
+        if (found) {
+            p.depth[v] = new_level;
+            p.parent[v] = (int64_t)par;
+        }
+        warp_append(p, acc, qout, found, v, end - beg, loc);
+    }
+}
+
+// Beamer's rule (hybrid_bfs.cc:152-191) for the step about to run, given the
+// frontier in ctrl.  Updates the Beamer state like the reference loop does
+// when it commits to that direction.
+__device__ int beamer_choose(Ctrl *c, const BfsParams &p, bool commit)
+{
+    if (c->in_bu) { return kDirBU; }
+    if (c->scout > c->etc / p.alpha) {
+        if (commit) {
+            c->in_bu = 1;
+            c->awake = c->f_count;  // queue_.combined_size()
+        }
+        return kDirBU;
+    }
+    if (commit) { c->etc -= c->scout; }
+    return kDirTD;
+}
+
+// After a step of direction `dir` found `found` vertices of degree sum
+// `degsum`: the reference's bookkeeping (scout after top-down, the awake
+// test of the bottom-up do-while, scout = 1 on leaving it).
+__device__ void beamer_after_step(Ctrl *c, const BfsParams &p, int dir, long long found,
+                                  long long degsum)
+{
+    if (dir == kDirTD) {
+        c->scout = degsum;
+    } else if (c->in_bu) {
+        c->old_awake = c->awake;
+        c->awake = found;
+        if (!(c->awake >= c->old_awake || c->awake > p.n / p.beta)) {
+            c->in_bu = 0;
+            c->scout = 1;
+        }
+    }
+}
+
+__device__ __forceinline__ float log2p1(double x) { return (float)log2(1.0 + (x > 0 ? x : 0)); }
+
+// Picks the direction of the next step.  Called by one CTA (the last to
+// reach the barrier, or the init kernel) with the frontier already in ctrl.
+template <int BLOCK>
+__device__ void choose_next(Ctrl *c, const BfsParams &p, SharedState<BLOCK> *sh)
+{
+    const int tid = threadIdx.x;
+    // thread 0: the rule-based choice, and the learned-policy features
+    if (tid == 0) {
+        int d;
+        if (c->f_count == 0) {
+            d = kDirDone;
+        } else if (p.alg == BD_ALG_TOP_DOWN) {
+            d = kDirTD;
+        } else if (p.alg == BD_ALG_BOTTOM_UP) {
+            d = kDirBU;
+        } else if (p.alg == BD_ALG_LEARNED && p.policy) {
+            d = beamer_choose(c, p, false);
+        } else {
+            d = beamer_choose(c, p, true);
+        }
+        if (sh) {
+            sh->beamer_dir = d;
+            const long long m_u = 2 * p.m - c->visited_degsum;
+            sh->feat[0] = log2p1((double)c->f_count);
+            sh->feat[1] = log2p1((double)c->f_degsum);
+            sh->feat[2] = log2p1((double)m_u);
+            sh->feat[3] = (float)c->level;
+            sh->feat[4] = log2p1((double)p.n);
+            sh->feat[5] = log2p1((double)p.m);
+            sh->feat[6] = (float)c->prev_dir;
+            sh->feat[7] = log2p1((double)c->prev_ns * 1e-3);
+        } else {
+            c->dir = d;
+        }
+    }
+    if (!sh) { return; }
+    __syncthreads();
+    const bool learned = p.alg == BD_ALG_LEARNED && p.policy && sh->beamer_dir != kDirDone;
+    if (learned && tid < 32) {
+        const PolicyBlob *w = p.policy;
+        const int j = tid;
+        float acc1 = w->b1[j];
+#pragma unroll
+        for (int i = 0; i < kPolicyIn; ++i) {
+            acc1 += w->w1[j][i] * ((sh->feat[i] - w->mean[i]) * w->inv_std[i]);
+        }
+        sh->h1[j] = fmaxf(acc1, 0.f);
+        __syncwarp();
+        float acc2 = w->b2[j];
+#pragma unroll 8
+        for (int i = 0; i < kPolicyH; ++i) { acc2 += w->w2[j][i] * sh->h1[i]; }
+        const float h2 = fmaxf(acc2, 0.f);
+        const float o0 = warp_sum(w->w3[0][j] * h2);
+        const float o1 = warp_sum(w->w3[1][j] * h2);
+        if (j == 0) {
+            sh->logit[0] = o0 + w->b3[0];
+            sh->logit[1] = o1 + w->b3[1];
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int d = sh->beamer_dir;
+        if (learned) {
+            const float gap = sh->logit[1] - sh->logit[0];
+            int pick = d;
+            if (isfinite(gap) && fabsf(gap) >= p.policy->margin) {
+                pick = gap > 0.f ? kDirBU : kDirTD;
+            }
+            if (pick != d) { c->policy_overrides += 1; }
+            d = pick;
+            // keep the rule's state consistent with the step actually taken
+            if (d == kDirTD) {
+                c->in_bu = 0;
+                c->etc -= c->scout;
+            } else if (!c->in_bu) {
+                c->in_bu = 1;
+                c->awake = c->f_count;
+            }
+        }
+        c->dir = d;
+    }
+    __syncthreads();
+}
+
+// Bookkeeping after a step; run by thread 0 of the deciding CTA.
+__device__ void finish_step(Ctrl *c, const BfsParams &p)
+{
+    const int s = c->step;
+    volatile Acc *a = &c->acc[s & 1];
+    const long long found = (long long)a->found;
+    const long long degsum = (long long)a->degsum;
+    const long long nsmall = (long long)a->small_cnt;
+    const unsigned long long lp = a->large_packed;
+    const long long now = globaltimer();
+    const long long ns = now - c->t_last;
+    const int dir = c->dir;
+    if (s < p.rec_cap) {
+        bd_step r;
+        r.dir = dir;
+        r.level = c->level;
+        r.frontier = c->f_count;
+        r.frontier_edges = c->f_degsum;
+        r.unexplored_edges = 2 * p.m - c->visited_degsum;
+        r.found = found;
+        r.ns = ns;
+        p.rec[s] = r;
+    }
+    c->visited_degsum += degsum;
+    c->reached += found;
+    c->f_count = found;
+    c->f_degsum = degsum;
+    c->f_small = nsmall;
+    c->f_large = (long long)(lp >> kLargeShift);
+    c->f_chunks = (long long)(lp & kChunkMask);
+    c->prev_dir = dir;
+    c->prev_ns = ns;
+    if (dir == kDirTD) { c->td_steps += 1; } else { c->bu_steps += 1; }
+    c->level += 1;
+    c->q_cur ^= 1;
+    if (dir == kDirBU) { c->vis_cur ^= 1; }
+    beamer_after_step(c, p, dir, found, degsum);
+    Acc *z = &c->acc[(s + 1) & 1];
+    z->found = 0;
+    z->degsum = 0;
+    z->small_cnt = 0;
+    z->large_packed = 0;
+    c->step = s + 1;
+    c->t_last = now;
+}
+
+// Grid barrier; the last CTA to arrive closes the step and picks the next
+// direction before releasing the others.  Every wait is bounded by
+// p.spin_limit polls; running out sets ctrl->error = BD_ERR_TIMEOUT.
+template <int BLOCK>
+__device__ void barrier_decide(const BfsParams &p, SharedState<BLOCK> &sh)
+{
+    Ctrl *c = p.ctrl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = ld_acquire(&c->bar_gen);
+        __threadfence();
+        const unsigned prev = atomicAdd(&c->bar_count, 1u);
+        sh.is_last = (prev == p.expected_ctas - 1);
+        sh.gen = gen;
+    }
+    __syncthreads();
+    if (sh.is_last) {
+        __threadfence();
+        if (threadIdx.x == 0) { finish_step(c, p); }
+        __syncthreads();
+        choose_next<BLOCK>(c, p, &sh);
+        if (threadIdx.x == 0) {
+            atomicExch(&c->bar_count, 0u);
+            __threadfence();
+            st_release(&c->bar_gen, sh.gen + 1);
+        }
+    } else if (threadIdx.x == 0) {
+        long long it = 0;
+        while (ld_acquire(&c->bar_gen) == sh.gen) {
+            if (++it > p.spin_limit) {
+                atomicExch(&c->error, (int)BD_ERR_TIMEOUT);
+                break;
+            }
+            __nanosleep(64);
+        }
+    }
+    __syncthreads();
+}
+
+template <int BLOCK>
+__device__ void reduce_and_publish(const BfsParams &p, const StepView &sv, SharedState<BLOCK> &sh,
+                                   Local &loc)
+{
+    const int lane = lane_id();
+    const int warp = threadIdx.x >> 5;
+    unsigned long long f = warp_sum(loc.found);
+    unsigned long long d = warp_sum(loc.degsum);
+    if (lane == 0) {
+        sh.red_found[warp] = f;
+        sh.red_deg[warp] = d;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long tf = 0, td = 0;
+        for (int i = 0; i < BLOCK / 32; ++i) {
+            tf += sh.red_found[i];
+            td += sh.red_deg[i];
+        }
+        Acc *acc = &p.ctrl->acc[sv.step & 1];
+        if (tf) { atomicAdd(&acc->found, tf); }
+        if (td) { atomicAdd(&acc->degsum, td); }
+    }
+    loc.found = 0;
+    loc.degsum = 0;
+}
+
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) bfs_persistent_kernel(BfsParams p)
+{
+    __shared__ SharedState<BLOCK> sh;
+    Ctrl *c = p.ctrl;
+    if (blockIdx.x == 0 && threadIdx.x == 0) { c->t_last = globaltimer(); }
+    Local loc{0, 0};
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const volatile Ctrl *vc = c;
+            sh.exit_flag = (vc->error != 0) || (vc->dir == kDirDone);
+        }
+        __syncthreads();
+        if (sh.exit_flag) { break; }
+        const StepView sv = read_view(c);
+        if (sv.dir == kDirTD) {
+            td_step<BLOCK>(p, sv, sh, loc);
+        } else {
+            bu_step<BLOCK>(p, sv, loc);
+        }
+        reduce_and_publish<BLOCK>(p, sv, sh, loc);
+        barrier_decide<BLOCK>(p, sh);
+    }
+}
+
+// clear() + the source frontier (hybrid_bfs.cc:152-160 for one source; any
+// number of sources start as one frontier).  One CTA of 32 threads.
+__global__ void init_sources_kernel(BfsParams p, const int64_t *sources, int64_t count,
+                                    int64_t source_index)
+{
+    __shared__ SharedState<32> sh;
+    Ctrl *c = p.ctrl;
+    if (threadIdx.x == 0) {
+        memset(c, 0, sizeof(Ctrl));
+        long long degsum = 0, nf = 0, nsmall = 0;
+        unsigned long long lp = 0;
+        const int64_t first = source_index >= 0 ? source_index : 0;
+        const int64_t last = source_index >= 0 ? source_index + 1 : count;
+        for (int64_t i = first; i < last; ++i) {
+            const uint32_t s = (uint32_t)sources[i];
+            if (p.depth[s] == 0) { continue; }  // repeated source
+            p.depth[s] = 0;
+            p.parent[s] = (int64_t)s;
+            p.vis[0][s >> 5] |= 1u << (s & 31);
+            const int64_t deg = p.off[s + 1] - p.off[s];
+            degsum += deg;
+            nf += 1;
+            if (deg >= (int64_t)p.large_deg) {
+                const unsigned long long pos = lp >> kLargeShift;
+                p.ql[0][pos] = s;
+                p.qlb[0][pos] = lp & kChunkMask;
+                lp += (1ull << kLargeShift) | (unsigned long long)((deg + p.chunk - 1) / p.chunk);
+            } else {
+                p.qs[0][nsmall++] = s;
+            }
+        }
+        c->f_count = nf;
+        c->f_degsum = degsum;
+        c->f_small = nsmall;
+        c->f_large = (long long)(lp >> kLargeShift);
+        c->f_chunks = (long long)(lp & kChunkMask);
+        c->visited_degsum = degsum;
+        c->reached = nf;
+        c->etc = 2 * p.m;       // edges_to_check = num_edges * 2
+        c->scout = degsum;      // scout_count = out_degree(source)
+        c->prev_dir = kDirTD;
+    }
+    __syncthreads();
+    choose_next<32>(c, p, &sh);
+}
+
+// Deterministic tree: parent(v) = min{u in N(v) : depth[u] == depth[v]-1}.
+// Warp per 32 vertices; short lists per lane, long lists by the whole warp.
+__global__ void min_parent_kernel(const int64_t *off, const uint32_t *adj, int64_t n,
+                                  const int32_t *depth, int64_t *parent)
+{
+    const int lane = threadIdx.x & 31;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long words = (n + 31) / 32;
+    for (long long w = gw; w < words; w += nw) {
+        const int64_t v = w * 32 + lane;
+        int32_t dv = v < n ? depth[v] : -1;
+        int64_t b = 0, e = 0;
+        uint32_t best = 0xFFFFFFFFu;
+        const bool want = dv > 0;
+        if (want) {
+            b = off[v];
+            e = off[v + 1];
+            if (e - b <= 32) {
+                for (int64_t k = b; k < e; ++k) {
+                    uint32_t u = adj[k];
+                    if (u < best && depth[u] == dv - 1) { best = u; }
+                }
+            }
+        }
+        unsigned big = __ballot_sync(kFull, want && e - b > 32);
+        while (big) {
+            const int owner = __ffs(big) - 1;
+            big &= big - 1;
+            const int64_t bb = __shfl_sync(kFull, b, owner);
+            const int64_t ee = __shfl_sync(kFull, e, owner);
+            const int32_t d = __shfl_sync(kFull, dv, owner);
+            uint32_t mine = 0xFFFFFFFFu;
+            for (int64_t k = bb + lane; k < ee; k += 32) {
+                uint32_t u = adj[k];
+                if (u < mine && depth[u] == d - 1) { mine = u; }
+            }
+#pragma unroll
+            for (int s = 16; s > 0; s >>= 1) { mine = min(mine, __shfl_xor_sync(kFull, mine, s)); }
+            if (lane == owner) { best = mine; }
+        }
+        if (want) { parent[v] = (int64_t)best; }
+    }
+}
+
+// The reference's encoding of unreached vertices (hybrid_bfs.cc:433-443).
+__global__ void finalize_parents_kernel(const int64_t *off, int64_t n, const int32_t *depth,
+                                        int64_t *parent)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        if (depth[v] < 0) {
+            const int64_t d = off[v + 1] - off[v];
+            parent[v] = d != 0 ? -d : -1;
+        }
+    }
+}
+
+__global__ void save_result_kernel(const Ctrl *c, int64_t *out, int64_t i)
+{
+    out[2 * i] = c->visited_degsum / 2;
+    out[2 * i + 1] = c->reached;
+}
+
+int grid_for(int64_t items, int threads = 256)
+{
+    int64_t b = (items + threads - 1) / threads;
+    if (b < 1) { b = 1; }
+    if (b > 148 * 32) { b = 148 * 32; }
+    return (int)b;
+}
+
+using KernelFn = void (*)(BfsParams);
+
+struct KernelChoice {
+    KernelFn fn;
+    int block;
+};
+
+KernelChoice pick_kernel(int block)
+{
+    switch (block) {
+        case 256: return {bfs_persistent_kernel<256, 4>, 256};
+        case 1024: return {bfs_persistent_kernel<1024, 1>, 1024};
+        default: return {bfs_persistent_kernel<512, 2>, 512};
+    }
+}
+
+}  // namespace
+
+}  // namespace bd
+
+using namespace bd;
+
+struct bd_bfs {
+    bd_graph *g = nullptr;
+    bd_bfs_opts opts{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int32_t *depth = nullptr;
+    int64_t *parent = nullptr;
+    uint32_t *vis[2] = {nullptr, nullptr};
+    uint32_t *qs[2] = {nullptr, nullptr};
+    uint32_t *ql[2] = {nullptr, nullptr};
+    unsigned long long *qlb[2] = {nullptr, nullptr};
+    Ctrl *ctrl = nullptr;
+    bd_step *rec = nullptr;
+    int64_t *d_sources = nullptr;
+    int64_t sources_cap = 0;
+    PolicyBlob *policy = nullptr;  // device copy, or null
+    KernelFn kernel = nullptr;
+    int block = 512;
+    int grid = 0;
+    int64_t cap_large = 0;
+    bool cleared = false;
+    bool ran = false;
+    bool parents_final = false;
+    int64_t last_source = -1;
+    Ctrl last{};
+};
+
+namespace bd {
+namespace {
+
+BfsParams make_params(bd_bfs *b)
+{
+    BfsParams p{};
+    p.off = b->g->d_off;
+    p.adj = b->g->d_adj;
+    p.n = b->g->n;
+    p.m = b->g->m;
+    p.depth = b->depth;
+    p.parent = b->parent;
+    p.vis[0] = b->vis[0];
+    p.vis[1] = b->vis[1];
+    p.words = bitmap_words(b->g->n);
+    for (int i = 0; i < 2; ++i) {
+        p.qs[i] = b->qs[i];
+        p.ql[i] = b->ql[i];
+        p.qlb[i] = b->qlb[i];
+    }
+    p.ctrl = b->ctrl;
+    p.rec = b->rec;
+    p.rec_cap = kRecCap;
+    p.alg = b->opts.alg;
+    p.alpha = b->opts.alpha;
+    p.beta = b->opts.beta;
+    p.large_deg = (uint32_t)b->opts.large_degree;
+    p.chunk = (uint32_t)b->opts.chunk_edges;
+    p.bu_prefix = b->opts.bu_prefix;
+    p.spin_limit = b->opts.spin_limit;
+    p.expected_ctas = (unsigned)(b->grid + b->opts.test_extra_ctas);
+    p.policy = b->policy;
+    return p;
+}
+
+bd_status enqueue_clear(bd_bfs *b)
+{
+    const int64_t n = b->g->n;
+    BD_CUDA(cudaMemsetAsync(b->depth, 0xFF, sizeof(int32_t) * n, b->stream));
+    BD_CUDA(cudaMemcpyAsync(b->vis[0], b->g->d_isolated, sizeof(uint32_t) * bitmap_words(n),
+                            cudaMemcpyDeviceToDevice, b->stream));
+    return BD_OK;
+}
+
+bd_status ensure_sources(bd_bfs *b, int64_t count)
+{
+    if (count <= b->sources_cap) { return BD_OK; }
+    cudaFree(b->d_sources);
+    b->d_sources = nullptr;
+    b->sources_cap = 0;
+    BD_CUDA(cudaMalloc(&b->d_sources, sizeof(int64_t) * count));
+    b->sources_cap = count;
+    return BD_OK;
+}
+
+// Enqueues init + the persistent kernel (+ min-parent pass) for either a
+// set of sources (index < 0) or source d_sources[index].
+bd_status enqueue_bfs(bd_bfs *b, int64_t count, int64_t index, cudaEvent_t start,
+                      cudaEvent_t stop)
+{
+    BfsParams p = make_params(b);
+    // The timed region starts with the source setup, as run_beamer's does
+    // (hybrid_bfs.cc:158-160); clear() stays outside it.
+    if (start) { BD_CUDA(cudaEventRecord(start, b->stream)); }
+    init_sources_kernel<<<1, 32, 0, b->stream>>>(p, b->d_sources, count, index);
+    BD_CUDA(cudaGetLastError());
+    void *args[] = {&p};
+    BD_CUDA(cudaLaunchCooperativeKernel((const void *)b->kernel, dim3(b->grid), dim3(b->block),
+                                        args, 0, b->stream));
+    if (b->opts.min_parent) {
+        min_parent_kernel<<<grid_for(bitmap_words(b->g->n) * 32), 256, 0, b->stream>>>(
+            b->g->d_off, b->g->d_adj, b->g->n, b->depth, b->parent);
+        BD_CUDA(cudaGetLastError());
+    }
+    if (stop) { BD_CUDA(cudaEventRecord(stop, b->stream)); }
+    return BD_OK;
+}
+
+bd_status collect(bd_bfs *b, bd_run_stats *stats, double ms)
+{
+    BD_CUDA(cudaMemcpyAsync(&b->last, b->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, b->stream));
+    BD_CUDA(cudaStreamSynchronize(b->stream));
+    b->ran = true;
+    b->cleared = false;
+    b->parents_final = false;
+    if (b->last.error) { return (bd_status)b->last.error; }
+    if (stats) {
+        stats->ms = ms;
+        stats->num_steps = b->last.step;
+        stats->reached = b->last.reached;
+        stats->traversed_edges = b->last.visited_degsum / 2;
+        stats->top_down_steps = b->last.td_steps;
+        stats->bottom_up_steps = b->last.bu_steps;
+    }
+    return BD_OK;
+}
+
+bd_status run_sources(bd_bfs *b, const int64_t *sources, int64_t count, bd_run_stats *stats)
+{
+    if (!b || !sources || count <= 0) { return BD_ERR_INVALID; }
+    for (int64_t i = 0; i < count; ++i) {
+        if (sources[i] < 0 || sources[i] >= b->g->n) { return BD_ERR_RANGE; }
+    }
+    BD_CUDA(cudaSetDevice(b->device));
+    BD_TRY(ensure_sources(b, count));
+    if (!b->cleared) { BD_TRY(enqueue_clear(b)); }
+    BD_CUDA(cudaMemcpyAsync(b->d_sources, sources, sizeof(int64_t) * count,
+                            cudaMemcpyHostToDevice, b->stream));
+    BD_TRY(enqueue_bfs(b, count, -1, b->ev0, b->ev1));
+    BD_CUDA(cudaEventSynchronize(b->ev1));
+    float ms = 0.f;
+    BD_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    b->last_source = count == 1 ? sources[0] : -1;
+    return collect(b, stats, (double)ms);
+}
+
+bd_status finalize_parents(bd_bfs *b)
+{
+    if (!b->ran) { return BD_ERR_STATE; }
+    if (b->parents_final) { return BD_OK; }
+    finalize_parents_kernel<<<grid_for(b->g->n), 256, 0, b->stream>>>(b->g->d_off, b->g->n,
+                                                                      b->depth, b->parent);
+    BD_CUDA(cudaGetLastError());
+    BD_CUDA(cudaStreamSynchronize(b->stream));
+    b->parents_final = true;
+    return BD_OK;
+}
+
+void bfs_free(bd_bfs *b)
+{
+    if (!b) { return; }
+    cudaSetDevice(b->device);
+    if (b->stream) { cudaStreamSynchronize(b->stream); }
+    cudaFree(b->depth);
+    cudaFree(b->parent);
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(b->vis[i]);
+        cudaFree(b->qs[i]);
+        cudaFree(b->ql[i]);
+        cudaFree(b->qlb[i]);
+    }
+    cudaFree(b->ctrl);
+    cudaFree(b->rec);
+    cudaFree(b->d_sources);
+    cudaFree(b->policy);
+    if (b->ev0) { cudaEventDestroy(b->ev0); }
+    if (b->ev1) { cudaEventDestroy(b->ev1); }
+    if (b->stream) { cudaStreamDestroy(b->stream); }
+    delete b;
+}
+
+}  // namespace
+}  // namespace bd
+
+extern "C" {
+
+void bd_bfs_default_opts(bd_bfs_opts *o)
+{
+    if (!o) { return; }
+    memset(o, 0, sizeof(*o));
+    o->alg = BD_ALG_BEAMER;
+    o->alpha = 15;
+    o->beta = 18;
+}
+
+bd_status bd_bfs_create(bd_graph *g, const bd_bfs_opts *opts, bd_bfs **out)
+{
+    if (!g || !out) { return BD_ERR_INVALID; }
+    bd_bfs_opts o;
+    bd_bfs_default_opts(&o);
+    if (opts) { o = *opts; }
+    if (o.alg < BD_ALG_BEAMER || o.alg > BD_ALG_LEARNED || o.alpha <= 0 || o.beta <= 0) {
+        return BD_ERR_INVALID;
+    }
+    if (o.block_size == 0) { o.block_size = 512; }
+    if (o.block_size != 256 && o.block_size != 512 && o.block_size != 1024) { return BD_ERR_INVALID; }
+    if (o.large_degree <= 0) { o.large_degree = 1024; }
+    if (o.chunk_edges <= 0) { o.chunk_edges = 1024; }
+    if (o.bu_prefix <= 0) { o.bu_prefix = 32; }
+    if (o.spin_limit <= 0) { o.spin_limit = kDefaultSpin; }
+    if (o.test_extra_ctas < 0) { return BD_ERR_INVALID; }
+    BD_TRY(ensure_device());
+    auto *b = new bd_bfs();
+    b->g = g;
+    b->opts = o;
+    b->device = current_device();
+    const int64_t n = g->n;
+    const int64_t words = bitmap_words(n);
+    b->cap_large = std::min<int64_t>(n, g->arcs / o.large_degree + 1);
+    auto fail = [&](bd_status st) { bfs_free(b); return st; };
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+        return fail(BD_ERR_CUDA);
+    }
+    bool ok = cudaMalloc(&b->depth, sizeof(int32_t) * n) == cudaSuccess &&
+              cudaMalloc(&b->parent, sizeof(int64_t) * n) == cudaSuccess &&
+              cudaMalloc(&b->ctrl, sizeof(Ctrl)) == cudaSuccess &&
+              cudaMalloc(&b->rec, sizeof(bd_step) * kRecCap) == cudaSuccess;
+    for (int i = 0; i < 2 && ok; ++i) {
+        ok = cudaMalloc(&b->vis[i], sizeof(uint32_t) * words) == cudaSuccess &&
+             cudaMalloc(&b->qs[i], sizeof(uint32_t) * n) == cudaSuccess &&
+             cudaMalloc(&b->ql[i], sizeof(uint32_t) * b->cap_large) == cudaSuccess &&
+             cudaMalloc(&b->qlb[i], sizeof(unsigned long long) * b->cap_large) == cudaSuccess;
+    }
+    if (!ok) { return fail(BD_ERR_OOM); }
+    KernelChoice kc = pick_kernel(o.block_size);
+    b->kernel = kc.fn;
+    b->block = kc.block;
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)b->kernel, b->block, 0) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess ||
+        per_sm < 1) {
+        return fail(BD_ERR_CUDA);
+    }
+    b->grid = per_sm * sms;
+    *out = b;
+    return BD_OK;
+}
+
+bd_status bd_bfs_clear(bd_bfs *b)
+{
+    if (!b) { return BD_ERR_INVALID; }
+    BD_CUDA(cudaSetDevice(b->device));
+    BD_TRY(enqueue_clear(b));
+    BD_CUDA(cudaStreamSynchronize(b->stream));
+    b->cleared = true;
+    b->ran = false;
+    return BD_OK;
+}
+
+bd_status bd_bfs_run(bd_bfs *b, int64_t source, bd_run_stats *stats)
+{
+    return run_sources(b, &source, 1, stats);
+}
+
+bd_status bd_bfs_run_multi(bd_bfs *b, const int64_t *sources, int64_t count, bd_run_stats *stats)
+{
+    return run_sources(b, sources, count, stats);
+}
+
+static bd_status run_with_alg(bd_bfs *b, int alg, int64_t alpha, int64_t beta, int64_t source,
+                              bd_run_stats *stats)
+{
+    if (!b) { return BD_ERR_INVALID; }
+    if (alpha <= 0 || beta <= 0) { return BD_ERR_INVALID; }
+    bd_bfs_opts saved = b->opts;
+    b->opts.alg = alg;
+    b->opts.alpha = alpha;
+    b->opts.beta = beta;
+    bd_status st = run_sources(b, &source, 1, stats);
+    b->opts = saved;
+    return st;
+}
+
+bd_status bd_bfs_run_beamer(bd_bfs *b, int64_t source, int64_t alpha, int64_t beta,
+                            bd_run_stats *stats)
+{
+    return run_with_alg(b, BD_ALG_BEAMER, alpha, beta, source, stats);
+}
+
+bd_status bd_bfs_run_top_down(bd_bfs *b, int64_t source, bd_run_stats *stats)
+{
+    if (!b) { return BD_ERR_INVALID; }
+    return run_with_alg(b, BD_ALG_TOP_DOWN, b->opts.alpha, b->opts.beta, source, stats);
+}
+
+bd_status bd_bfs_run_bottom_up(bd_bfs *b, int64_t source, bd_run_stats *stats)
+{
+    if (!b) { return BD_ERR_INVALID; }
+    return run_with_alg(b, BD_ALG_BOTTOM_UP, b->opts.alpha, b->opts.beta, source, stats);
+}
+
+bd_status bd_bfs_run_many(bd_bfs *b, const int64_t *sources, int64_t k, double *ms_out,
+                          int64_t *edges_out, int64_t *reached_out, double *e2e_ms)
+{
+    if (!b || !sources || k <= 0) { return BD_ERR_INVALID; }
+    for (int64_t i = 0; i < k; ++i) {
+        if (sources[i] < 0 || sources[i] >= b->g->n) { return BD_ERR_RANGE; }
+    }
+    BD_CUDA(cudaSetDevice(b->device));
+    BD_TRY(ensure_sources(b, k));
+    int64_t *d_edges = nullptr;
+    std::vector<cudaEvent_t> ev(2 * k, nullptr);
+    bd_status st = BD_OK;
+    cudaEvent_t wall0 = nullptr, wall1 = nullptr;
+    auto cleanup = [&]() {
+        for (auto e : ev) { if (e) { cudaEventDestroy(e); } }
+        if (wall0) { cudaEventDestroy(wall0); }
+        if (wall1) { cudaEventDestroy(wall1); }
+        cudaFree(d_edges);
+    };
+    if (cudaMalloc(&d_edges, sizeof(int64_t) * 2 * k) != cudaSuccess ||
+        cudaEventCreate(&wall0) != cudaSuccess || cudaEventCreate(&wall1) != cudaSuccess) {
+        cleanup();
+        return BD_ERR_OOM;
+    }
+    for (auto &e : ev) {
+        if (cudaEventCreate(&e) != cudaSuccess) { cleanup(); return BD_ERR_CUDA; }
+    }
+    std::vector<int64_t> host_edges(2 * k);
+    cudaEventRecord(wall0, b->stream);
+    if (cudaMemcpyAsync(b->d_sources, sources, sizeof(int64_t) * k, cudaMemcpyHostToDevice,
+                        b->stream) != cudaSuccess) {
+        cleanup();
+        return BD_ERR_CUDA;
+    }
+    for (int64_t i = 0; i < k && st == BD_OK; ++i) {
+        st = enqueue_clear(b);
+        if (st == BD_OK) { st = enqueue_bfs(b, k, i, ev[2 * i], ev[2 * i + 1]); }
+        if (st == BD_OK) {
+            save_result_kernel<<<1, 1, 0, b->stream>>>(b->ctrl, d_edges, i);
+            if (cudaGetLastError() != cudaSuccess) { st = BD_ERR_CUDA; }
+        }
+    }
+    if (st == BD_OK &&
+        (cudaMemcpyAsync(host_edges.data(), d_edges, sizeof(int64_t) * 2 * k, cudaMemcpyDeviceToHost,
+                         b->stream) != cudaSuccess ||
+         cudaEventRecord(wall1, b->stream) != cudaSuccess ||
+         cudaStreamSynchronize(b->stream) != cudaSuccess)) {
+        st = BD_ERR_CUDA;
+    }
+    if (st == BD_OK) {
+        float w = 0.f;
+        cudaEventElapsedTime(&w, wall0, wall1);
+        if (e2e_ms) { *e2e_ms = (double)w; }
+        for (int64_t i = 0; i < k; ++i) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+            if (ms_out) { ms_out[i] = (double)ms; }
+            if (edges_out) { edges_out[i] = host_edges[2 * i]; }
+            if (reached_out) { reached_out[i] = host_edges[2 * i + 1]; }
+        }
+        b->last_source = sources[k - 1];
+        st = collect(b, nullptr, 0.0);
+    }
+    cleanup();
+    return st;
+}
+
+bd_status bd_bfs_get_depths(bd_bfs *b, int32_t *depth)
+{
+    if (!b || !depth) { return BD_ERR_INVALID; }
+    if (!b->ran) { return BD_ERR_STATE; }
+    BD_CUDA(cudaSetDevice(b->device));
+    BD_CUDA(cudaMemcpy(depth, b->depth, sizeof(int32_t) * b->g->n, cudaMemcpyDeviceToHost));
+    return BD_OK;
+}
+
+bd_status bd_bfs_get_parents(bd_bfs *b, int64_t *parent)
+{
+    if (!b || !parent) { return BD_ERR_INVALID; }
+    BD_CUDA(cudaSetDevice(b->device));
+    BD_TRY(finalize_parents(b));
+    BD_CUDA(cudaMemcpy(parent, b->parent, sizeof(int64_t) * b->g->n, cudaMemcpyDeviceToHost));
+    return BD_OK;
+}
+
+bd_status bd_bfs_device_ptrs(bd_bfs *b, const int32_t **depth, const int64_t **parent)
+{
+    if (!b) { return BD_ERR_INVALID; }
+    BD_CUDA(cudaSetDevice(b->device));
+    BD_TRY(finalize_parents(b));
+    if (depth) { *depth = b->depth; }
+    if (parent) { *parent = b->parent; }
+    return BD_OK;
+}
+
+bd_status bd_bfs_count_traversed_edges(bd_bfs *b, int64_t *out)
+{
+    if (!b || !out) { return BD_ERR_INVALID; }
+    if (!b->ran) { return BD_ERR_STATE; }
+    *out = b->last.visited_degsum / 2;
+    return BD_OK;
+}
+
+// hybrid_bfs::check (hybrid_bfs.cc:281-379) on the host: a serial queue BFS
+// for depths, then every reached vertex must have its parent in its
+// adjacency list exactly one level up, and reachability must agree.
+bd_status bd_bfs_check(bd_bfs *b, int64_t source, int32_t *ok)
+{
+    if (!b || !ok) { return BD_ERR_INVALID; }
+    if (source < 0 || source >= b->g->n) { return BD_ERR_RANGE; }
+    const int64_t n = b->g->n;
+    std::vector<int64_t> off(n + 1), parent(n);
+    std::vector<uint32_t> adj(b->g->arcs);
+    BD_TRY(bd_graph_copy_csr(b->g, off.data(), adj.data()));
+    BD_TRY(bd_bfs_get_parents(b, parent.data()));
+    std::vector<int64_t> depth(n, -1), q;
+    q.reserve(n);
+    q.push_back(source);
+    depth[source] = 0;
+    for (size_t h = 0; h < q.size(); ++h) {
+        int64_t u = q[h];
+        for (int64_t e = off[u]; e < off[u + 1]; ++e) {
+            int64_t v = adj[e];
+            if (depth[v] == -1) {
+                depth[v] = depth[u] + 1;
+                q.push_back(v);
+            }
+        }
+    }
+    *ok = 1;
+    for (int64_t u = 0; u < n; ++u) {
+        if (depth[u] >= 0 && parent[u] >= 0) {
+            if (u == source) {
+                if (!(parent[u] == u && depth[u] == 0)) { *ok = 0; break; }
+                continue;
+            }
+            bool found = false;
+            for (int64_t e = off[u]; e < off[u + 1]; ++e) {
+                if ((int64_t)adj[e] == parent[u]) {
+                    found = depth[parent[u]] == depth[u] - 1;
+                    break;
+                }
+            }
+            if (!found) { *ok = 0; break; }
+        } else if ((depth[u] < 0) != (parent[u] < 0)) {
+            *ok = 0;
+            break;
+        }
+    }
+    return BD_OK;
+}
+
+bd_status bd_bfs_get_steps(bd_bfs *b, bd_step *steps, int64_t capacity, int64_t *count)
+{
+    if (!b || !count || capacity < 0 || (!steps && capacity)) { return BD_ERR_INVALID; }
+    if (!b->ran) { return BD_ERR_STATE; }
+    int64_t have = std::min<int64_t>(b->last.step, kRecCap);
+    int64_t take = std::min(have, capacity);
+    if (take) {
+        BD_CUDA(cudaSetDevice(b->device));
+        BD_CUDA(cudaMemcpy(steps, b->rec, sizeof(bd_step) * take, cudaMemcpyDeviceToHost));
+    }
+    *count = have;
+    return BD_OK;
+}
+
+bd_status bd_bfs_destroy(bd_bfs *b)
+{
+    if (!b) { return BD_ERR_INVALID; }
+    bfs_free(b);
+    return BD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+// bd_bfs_device.cuh -- device-side pieces of the direction-optimizing BFS.
+//
+// One cooperative ("persistent") kernel runs a whole BFS: every CTA loops
+// over levels; each level is a top-down step (frontier queue -> CAS claims)
+// or a bottom-up step (visited-bitmap scan with early exit), followed by a
+// grid barrier whose last-arriving CTA makes the direction decision for the
+// next level.  No host round trip happens inside a BFS.
+//
+// Reference counterparts:
+//   run_beamer                hybrid_bfs.cc:152-191   (decide_next / beamer_*)
+//   top-down step             hybrid_bfs.cc:71-100    (td_step)
+//   bottom-up step            hybrid_bfs.cc:111-143   (bu_step)
+//   sliding_queue windows     sliding_queue.h:77-99   (queue ping-pong)
+#pragma once
+
+#include <stdint.h>
+
+#include "beedrill_b200.h"
+
+namespace bd {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr int kDirTD = BD_DIR_TOP_DOWN;
+constexpr int kDirBU = BD_DIR_BOTTOM_UP;
+constexpr int kDirDone = 2;
+constexpr int kLargeShift = 38;  // large-queue counter: count << 38 | chunks
+constexpr unsigned long long kChunkMask = (1ull << kLargeShift) - 1;
+
+// Counters the CTAs accumulate during one step (ring of two: the decider
+// clears the slot of the step after next).
+struct Acc {
+    unsigned long long found;
+    unsigned long long degsum;
+    unsigned long long small_cnt;
+    unsigned long long large_packed;
+};
+
+// Device-resident control block of one BFS handle.
+struct Ctrl {
+    unsigned int bar_count;
+    unsigned int bar_gen;
+    int error;
+    int dir;        // direction of the step about to run, or kDirDone
+    int level;      // depth of the current frontier
+    int vis_cur;    // parity of the visited bitmap that is current
+    int q_cur;      // parity of the queues holding the current frontier
+    int step;       // index of the step about to run
+    long long etc;        // Beamer edges_to_check
+    long long scout;      // Beamer scout_count
+    long long awake;      // Beamer awake_count
+    long long old_awake;
+    int in_bu;            // inside Beamer's bottom-up do-while
+    int prev_dir;
+    long long prev_ns;
+    long long f_count, f_degsum, f_small, f_large, f_chunks;
+    long long visited_degsum;
+    long long reached;
+    long long t_last;
+    long long td_steps, bu_steps;
+    long long policy_overrides;  // learned decisions that differed from Beamer
+    Acc acc[2];
+};
+
+// Learned direction policy: 8-32-32-2 MLP, fp32, row-major weights.
+constexpr int kPolicyIn = 8;
+constexpr int kPolicyH = 32;
+constexpr int kPolicyOut = 2;
+constexpr int kPolicyParams = kPolicyH * kPolicyIn + kPolicyH + kPolicyH * kPolicyH + kPolicyH +
+                              kPolicyOut * kPolicyH + kPolicyOut;  // 1410
+struct PolicyBlob {
+    float w1[kPolicyH][kPolicyIn];
+    float b1[kPolicyH];
+    float w2[kPolicyH][kPolicyH];
+    float b2[kPolicyH];
+    float w3[kPolicyOut][kPolicyH];
+    float b3[kPolicyOut];
+    float mean[kPolicyIn];   // feature standardisation
+    float inv_std[kPolicyIn];
+    float margin;            // |logit gap| below which Beamer decides
+    float pad[3];
+};
+
+struct BfsParams {
+    const int64_t *off;
+    const uint32_t *adj;
+    int64_t n;
+    int64_t m;
+    int32_t *depth;
+    int64_t *parent;
+    uint32_t *vis[2];
+    int64_t words;
+    uint32_t *qs[2];
+    uint32_t *ql[2];
+    unsigned long long *qlb[2];
+    Ctrl *ctrl;
+    bd_step *rec;
+    int64_t rec_cap;
+    int alg;
+    int64_t alpha;
+    int64_t beta;
+    uint32_t large_deg;
+    uint32_t chunk;
+    int bu_prefix;
+    long long spin_limit;
+    unsigned expected_ctas;
+    const PolicyBlob *policy;  // null: no learned policy loaded
+};
+
+}  // namespace bd

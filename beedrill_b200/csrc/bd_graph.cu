@@ -1,0 +1,958 @@
+// bd_graph.cu -- graphs in HBM: el64 loading, CSR construction, the seeded
+// RMAT generator, disjoint unions, the lcg root picker and graph::check.
+//
+// Reference counterparts:
+//   edge_list.cc:20-89 / dist_edge_list.cc:50-143  el64 header + body
+//   graph_base.h:335-436                          CSR in insertion order
+//   graph_base.h:110-134                          graph::check
+//   generator/rmat_generator.h:91-193,
+//   generator/rmat_dataset_dump.cc:30-57          RMAT edges + post-processing
+//   hybrid_bfs_main.cc:136-144, lcg.h:4-32        root picker
+//
+// Graph construction is off the BFS hot path; it uses CUB's radix sort,
+// unique and scan where a sort or scan is needed.
+#include <cub/cub.cuh>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bd_internal.h"
+
+namespace bd {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kMaxAttempts = 4096;  // self-loop re-rolls per edge
+
+int grid_for(int64_t items, int threads = kThreads)
+{
+    int64_t b = (items + threads - 1) / threads;
+    if (b < 1) { b = 1; }
+    if (b > 148 * 64) { b = 148 * 64; }  // grid-stride beyond this
+    return (int)b;
+}
+
+// RAII device buffer for temporaries of the construction pipeline.
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t count = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { if (p) { cudaFree(p); } }
+    cudaError_t alloc(size_t n)
+    {
+        count = n;
+        return cudaMalloc(&p, sizeof(T) * (n ? n : 1));
+    }
+    T *release() { T *q = p; p = nullptr; return q; }
+    void reset()
+    {
+        if (p) { cudaFree(p); }
+        p = nullptr;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void philox(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c[0]);
+        uint32_t lo0 = 0xD2511F53u * c[0];
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]);
+        uint32_t lo1 = 0xCD9E8D57u * c[2];
+        uint32_t n0 = hi1 ^ c[1] ^ k0;
+        uint32_t n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = lo1;
+        c[2] = n2;
+        c[3] = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// Counter-based uniform stream of one (edge, attempt): draw j is half of
+// Philox block j/2, top 53 bits scaled into [0, 1).
+struct RmatStream {
+    uint32_t i_lo, i_hi, t, k0, k1;
+    uint32_t block[4];
+    uint32_t j = 0;
+    __device__ double next()
+    {
+        if ((j & 1) == 0) {
+            block[0] = i_lo;
+            block[1] = i_hi;
+            block[2] = t;
+            block[3] = j >> 1;
+            philox(block, k0, k1);
+        }
+        uint64_t w = (j & 1) ? (((uint64_t)block[2] << 32) | block[3])
+                             : (((uint64_t)block[0] << 32) | block[1]);
+        ++j;
+        return __dmul_rn(__ull2double_rn(w >> 11), 1.0 / 9007199254740992.0);
+    }
+};
+
+// One attempt of rmat_generator.h:91-140.  Every double operation is an
+// explicitly rounded intrinsic so no multiply-add is contracted: the result
+// is bit-identical to the step-by-step rounded host restatement.
+__device__ void rmat_attempt(int scale, double a, double b, double c, double d, uint64_t seed,
+                             int64_t i, uint32_t t, int64_t *src, int64_t *dst)
+{
+    RmatStream rs;
+    rs.i_lo = (uint32_t)(uint64_t)i;
+    rs.i_hi = (uint32_t)((uint64_t)i >> 32);
+    rs.t = t;
+    rs.k0 = (uint32_t)seed;
+    rs.k1 = (uint32_t)(seed >> 32);
+    double A = a, B = b, C = c, D = d;
+    int64_t si = 0, sj = 0;
+    int64_t bit = (int64_t)1 << (scale - 1);
+    for (;;) {
+        double r = rs.next();
+        if (r > A) {
+            double ab = __dadd_rn(A, B);
+            if (r <= ab) {
+                sj |= bit;
+            } else if (r <= __dadd_rn(ab, C)) {
+                si |= bit;
+            } else {
+                sj |= bit;
+                si |= bit;
+            }
+        }
+        if (bit == 1) { break; }
+        A = __dmul_rn(A, __ddiv_rn(__dadd_rn(9.5, rs.next()), 10.0));
+        B = __dmul_rn(B, __ddiv_rn(__dadd_rn(9.5, rs.next()), 10.0));
+        C = __dmul_rn(C, __ddiv_rn(__dadd_rn(9.5, rs.next()), 10.0));
+        D = __dmul_rn(D, __ddiv_rn(__dadd_rn(9.5, rs.next()), 10.0));
+        double norm = __ddiv_rn(1.0, __dadd_rn(__dadd_rn(__dadd_rn(A, B), C), D));
+        A = __dmul_rn(A, norm);
+        B = __dmul_rn(B, norm);
+        C = __dmul_rn(C, norm);
+        D = __dsub_rn(1.0, __dadd_rn(__dadd_rn(A, B), C));
+        bit >>= 1;
+    }
+    *src = si;
+    *dst = sj;
+}
+
+// Generated edge i -> flipped (src < dst) packed key src << scale | dst.
+__global__ void rmat_keys_kernel(int scale, int64_t num_edges, double a, double b, double c,
+                                 double d, uint64_t seed, uint64_t *keys)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < num_edges;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t s = 0, t = 0;
+        for (uint32_t att = 0; att < kMaxAttempts; ++att) {
+            rmat_attempt(scale, a, b, c, d, seed, i, att, &s, &t);
+            if (s != t) { break; }
+        }
+        uint64_t lo = (uint64_t)(s < t ? s : t), hi = (uint64_t)(s < t ? t : s);
+        keys[i] = (lo << scale) | hi;
+    }
+}
+
+// Sort key of item idx in a permutation domain (vertex relabel / shuffle).
+__device__ __forceinline__ uint64_t perm_key(uint64_t seed, uint64_t idx, uint32_t tag)
+{
+    uint32_t c[4] = {(uint32_t)idx, (uint32_t)(idx >> 32), tag, 0u};
+    philox(c, (uint32_t)seed ^ 0xA5A5A5A5u, (uint32_t)(seed >> 32) ^ 0x3C3C3C3Cu);
+    return ((uint64_t)c[0] << 32) | c[1];
+}
+
+constexpr uint32_t kTagRelabel = 0x52454C42u;  // "RELB"
+constexpr uint32_t kTagShuffle = 0x53485546u;  // "SHUF"
+
+__global__ void perm_keys_kernel(uint64_t seed, uint32_t tag, int64_t count, uint64_t *keys,
+                                 uint32_t *idx)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        keys[i] = perm_key(seed, (uint64_t)i, tag);
+        if (idx) { idx[i] = (uint32_t)i; }
+    }
+}
+
+__global__ void edge_shuffle_keys_kernel(uint64_t seed, int64_t count, uint64_t *keys)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        keys[i] = perm_key(seed, (uint64_t)i, kTagShuffle);
+    }
+}
+
+__global__ void scatter_rank_kernel(const uint32_t *sorted_v, int64_t n, uint32_t *new_id)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        new_id[sorted_v[k]] = (uint32_t)k;
+    }
+}
+
+__global__ void unpack_relabel_kernel(const uint64_t *packed, int64_t m, int scale,
+                                      const uint32_t *new_id, int64_t *src, int64_t *dst)
+{
+    const uint64_t mask = (1ull << scale) - 1;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t p = packed[k];
+        src[k] = new_id[p >> scale];
+        dst[k] = new_id[p & mask];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CSR construction
+// ---------------------------------------------------------------------------
+
+// Arc 2k = (src_k -> dst_k), arc 2k+1 = (dst_k -> src_k): the insertion
+// order of graph_base.h:423-427.  Flags endpoints outside [0, n).
+__global__ void make_arcs_kernel(const int64_t *src, const int64_t *dst, int64_t m, int64_t n,
+                                 uint32_t *key, uint32_t *val, int *bad)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t s = src[k], d = dst[k];
+        if (s < 0 || s >= n || d < 0 || d >= n) {
+            atomicExch(bad, 1);
+            s = 0;
+            d = 0;
+        }
+        key[2 * k] = (uint32_t)s;
+        val[2 * k] = (uint32_t)d;
+        key[2 * k + 1] = (uint32_t)d;
+        val[2 * k + 1] = (uint32_t)s;
+    }
+}
+
+__global__ void make_sorted_arcs_kernel(const int64_t *src, const int64_t *dst, int64_t m,
+                                        int64_t n, uint64_t *key, int *bad)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t s = src[k], d = dst[k];
+        if (s < 0 || s >= n || d < 0 || d >= n) {
+            atomicExch(bad, 1);
+            s = 0;
+            d = 0;
+        }
+        key[2 * k] = ((uint64_t)s << 32) | (uint64_t)d;
+        key[2 * k + 1] = ((uint64_t)d << 32) | (uint64_t)s;
+    }
+}
+
+__global__ void split_sorted_arcs_kernel(const uint64_t *key, int64_t arcs, uint32_t *src32,
+                                         uint32_t *adj)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < arcs;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t k = key[i];
+        src32[i] = (uint32_t)(k >> 32);
+        adj[i] = (uint32_t)k;
+    }
+}
+
+// offsets[v] = first arc whose (sorted) source is >= v.
+__global__ void offsets_from_sorted_kernel(const uint32_t *sorted_src, int64_t arcs, int64_t n,
+                                           int64_t *off)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= arcs;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t prev = i == 0 ? -1 : (int64_t)sorted_src[i - 1];
+        int64_t cur = i == arcs ? n : (int64_t)sorted_src[i];
+        for (int64_t v = prev + 1; v <= cur; ++v) { off[v] = i; }
+    }
+}
+
+__global__ void isolated_bitmap_kernel(const int64_t *off, int64_t n, uint32_t *bits)
+{
+    int64_t words = (n + 31) / 32;
+    for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < words;
+         w += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t b = 0;
+        for (int k = 0; k < 32; ++k) {
+            int64_t v = w * 32 + k;
+            if (v >= n || off[v + 1] == off[v]) { b |= 1u << k; }
+        }
+        bits[w] = b;
+    }
+}
+
+__global__ void validate_csr_kernel(const int64_t *off, const uint32_t *adj, int64_t n,
+                                    int64_t arcs, int *bad)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        int64_t b = off[v], e = off[v + 1];
+        if (b < 0 || e < b || e > arcs) { atomicExch(bad, 1); continue; }
+        if (v == 0 && b != 0) { atomicExch(bad, 1); }
+        if (v == n - 1 && e != arcs) { atomicExch(bad, 1); }
+        for (int64_t k = b; k < e; ++k) {
+            if ((int64_t)adj[k] >= n) { atomicExch(bad, 1); break; }
+        }
+    }
+}
+
+__global__ void split_pairs_kernel(const int64_t *pairs, int64_t count, int64_t *src,
+                                   int64_t *dst)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        src[i] = pairs[2 * i];
+        dst[i] = pairs[2 * i + 1];
+    }
+}
+
+__global__ void shift_csr_kernel(const int64_t *off_in, const uint32_t *adj_in, int64_t n,
+                                 int64_t arcs, int64_t vbase, int64_t abase, int64_t *off_out,
+                                 uint32_t *adj_out)
+{
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (int64_t v = t; v < n; v += stride) { off_out[vbase + v] = off_in[v] + abase; }
+    for (int64_t e = t; e < arcs; e += stride) {
+        adj_out[abase + e] = adj_in[e] + (uint32_t)vbase;
+    }
+}
+
+__global__ void set_last_offset_kernel(int64_t *off, int64_t n, int64_t arcs) { off[n] = arcs; }
+
+// graph::check: each edge present in both lists; no equal adjacent entries.
+__global__ void graph_check_kernel(const int64_t *src, const int64_t *dst, int64_t m,
+                                   const int64_t *off, const uint32_t *adj, int64_t arcs,
+                                   int sorted, int *bad)
+{
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (int64_t k = t; k < m; k += stride) {
+        for (int dir = 0; dir < 2; ++dir) {
+            int64_t u = dir ? dst[k] : src[k];
+            uint32_t v = (uint32_t)(dir ? src[k] : dst[k]);
+            int64_t b = off[u], e = off[u + 1];
+            bool found = false;
+            if (sorted) {
+                while (b < e) {
+                    int64_t mid = (b + e) / 2;
+                    if (adj[mid] < v) { b = mid + 1; } else { e = mid; }
+                }
+                found = b < off[u + 1] && adj[b] == v;
+            } else {
+                for (int64_t i = b; i < e && !found; ++i) { found = adj[i] == v; }
+            }
+            if (!found) { atomicExch(bad, 1); }
+        }
+    }
+    (void)arcs;
+}
+
+__global__ void adjacent_dup_kernel(const int64_t *off, const uint32_t *adj, int64_t n, int *bad)
+{
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += stride) {
+        for (int64_t i = off[v] + 1; i < off[v + 1]; ++i) {
+            if (adj[i] == adj[i - 1]) { atomicExch(bad, 1); break; }
+        }
+    }
+}
+
+// lcg(seed) (lcg.h:11-27) and pick_random_vertex (hybrid_bfs_main.cc:136-144):
+// rng() % n until the vertex has nonzero degree.  Bounded so a pathological
+// graph cannot loop forever; *status gets 1 if the bound was hit.
+__global__ void pick_roots_kernel(const int64_t *off, int64_t n, uint64_t seed, int64_t k,
+                                  int64_t *roots, int *status)
+{
+    const uint64_t mul = 6364136223846793005ull;
+    uint64_t mul_k = mul, add_k = 1, ran = 1;
+    for (uint64_t un = seed; un; un >>= 1) {
+        if (un & 1) { ran = mul_k * ran + add_k; }
+        add_k *= (mul_k + 1);
+        mul_k *= mul_k;
+    }
+    uint64_t state = ran;
+    int64_t budget = (int64_t)1 << 34;
+    for (int64_t s = 0; s < k; ++s) {
+        int64_t v;
+        do {
+            if (--budget < 0) { *status = 1; return; }
+            state = mul * state + 1;
+            v = (int64_t)(state % (uint64_t)n);
+        } while (off[v + 1] == off[v]);
+        roots[s] = v;
+    }
+}
+
+// Runs a CUB algorithm in the usual two calls: size query, then work.
+template <typename F>
+cudaError_t cub_run(F &&f, cudaStream_t s)
+{
+    size_t bytes = 0;
+    cudaError_t e = f(nullptr, bytes);
+    if (e != cudaSuccess) { return e; }
+    void *tmp = nullptr;
+    e = cudaMalloc(&tmp, bytes ? bytes : 1);
+    if (e != cudaSuccess) { return e; }
+    e = f(tmp, bytes);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    return e != cudaSuccess ? e : e2;
+}
+
+int bits_for(int64_t n)
+{
+    int b = 1;
+    while (b < 32 && ((int64_t)1 << b) < n) { ++b; }
+    return b;
+}
+
+bd_status read_flag(const int *d_flag, int *out)
+{
+    BD_CUDA(cudaMemcpy(out, d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    return BD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// el64 header (edge_list.cc:20-89): one text line shorter than 256 bytes
+// ending in '\n', parsed like a long-option command line; then the checks
+// of dist_edge_list.cc:56-76.
+// ---------------------------------------------------------------------------
+bd_status parse_el64_header(FILE *fp, int64_t *nv, int64_t *ne)
+{
+    char line[256];
+    if (!fgets(line, sizeof line, fp)) { return BD_ERR_FORMAT; }
+    size_t len = strlen(line);
+    if (len == 0 || line[len - 1] != '\n') { return BD_ERR_FORMAT; }
+    line[len - 1] = '\0';
+    int64_t num_v = -1, num_e = -1;
+    bool deduped = false, el64 = false;
+    std::vector<std::string> tok;
+    for (char *save = nullptr, *t = strtok_r(line, " ", &save); t; t = strtok_r(nullptr, " ", &save)) {
+        tok.emplace_back(t);
+    }
+    for (size_t i = 0; i < tok.size(); ++i) {
+        const std::string &t = tok[i];
+        auto value = [&](int64_t *dst) -> bool {
+            if (i + 1 >= tok.size()) { return false; }
+            *dst = atoll(tok[++i].c_str());
+            return true;
+        };
+        if (t == "--num_vertices") {
+            if (!value(&num_v)) { return BD_ERR_FORMAT; }
+        } else if (t == "--num_edges") {
+            if (!value(&num_e)) { return BD_ERR_FORMAT; }
+        } else if (t == "--format") {
+            if (i + 1 >= tok.size()) { return BD_ERR_FORMAT; }
+            el64 = tok[++i] == "el64";
+        } else if (t == "--is_deduped") {
+            deduped = true;
+        } else if (t == "--is_sorted" || t == "--is_permuted" || t == "--is_directed" ||
+                   t == "--is_undirected") {
+        } else {
+            return BD_ERR_FORMAT;
+        }
+    }
+    if (num_v <= 0 || num_e <= 0 || !el64 || !deduped) { return BD_ERR_FORMAT; }
+    *nv = num_v;
+    *ne = num_e;
+    return BD_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Construction pipeline shared by every graph source
+// ---------------------------------------------------------------------------
+
+void graph_free(bd_graph *g)
+{
+    if (!g) { return; }
+    cudaFree(g->d_off);
+    cudaFree(g->d_adj);
+    cudaFree(g->d_isolated);
+    cudaFree(g->d_src);
+    cudaFree(g->d_dst);
+    delete g;
+}
+
+bd_status graph_finish(bd_graph *g, cudaStream_t s)
+{
+    int64_t words = bitmap_words(g->n);
+    BD_CUDA(cudaMalloc(&g->d_isolated, sizeof(uint32_t) * (words ? words : 1)));
+    isolated_bitmap_kernel<<<grid_for(words), kThreads, 0, s>>>(g->d_off, g->n, g->d_isolated);
+    BD_CUDA(cudaGetLastError());
+    BD_CUDA(cudaStreamSynchronize(s));
+    return BD_OK;
+}
+
+bd_status graph_from_device_edges(int64_t n, int64_t m, int64_t *d_src, int64_t *d_dst,
+                                  int32_t order, bd_graph **out)
+{
+    auto *g = new bd_graph();
+    g->device = current_device();
+    g->n = n;
+    g->m = m;
+    g->arcs = 2 * m;
+    g->order = order;
+    g->d_src = d_src;
+    g->d_dst = d_dst;
+    cudaStream_t s = 0;
+    const int64_t arcs = g->arcs;
+    DevBuf<int> bad;
+    auto fail = [&](bd_status st) { graph_free(g); return st; };
+    if (bad.alloc(1) != cudaSuccess) { return fail(BD_ERR_OOM); }
+    if (cudaMemset(bad.p, 0, sizeof(int)) != cudaSuccess) { return fail(BD_ERR_CUDA); }
+    if (cudaMalloc(&g->d_off, sizeof(int64_t) * (n + 1)) != cudaSuccess ||
+        cudaMalloc(&g->d_adj, sizeof(uint32_t) * (arcs ? arcs : 1)) != cudaSuccess) {
+        return fail(BD_ERR_OOM);
+    }
+    DevBuf<uint32_t> sorted_src;
+    if (sorted_src.alloc(arcs) != cudaSuccess) { return fail(BD_ERR_OOM); }
+    if (order == BD_ORDER_SORTED) {
+        DevBuf<uint64_t> k_in, k_out;
+        if (k_in.alloc(arcs) != cudaSuccess || k_out.alloc(arcs) != cudaSuccess) {
+            return fail(BD_ERR_OOM);
+        }
+        make_sorted_arcs_kernel<<<grid_for(m), kThreads, 0, s>>>(d_src, d_dst, m, n, k_in.p, bad.p);
+        cudaError_t e = cub_run([&](void *tmp, size_t &bytes) {
+            return cub::DeviceRadixSort::SortKeys(tmp, bytes, k_in.p, k_out.p, arcs, 0, 64, s);
+        }, s);
+        if (e != cudaSuccess) { return fail(cuda_fail(e, "SortKeys(arcs)", __FILE__, __LINE__)); }
+        split_sorted_arcs_kernel<<<grid_for(arcs), kThreads, 0, s>>>(k_out.p, arcs, sorted_src.p,
+                                                                     g->d_adj);
+    } else {
+        DevBuf<uint32_t> k_in, v_in;
+        if (k_in.alloc(arcs) != cudaSuccess || v_in.alloc(arcs) != cudaSuccess) {
+            return fail(BD_ERR_OOM);
+        }
+        make_arcs_kernel<<<grid_for(m), kThreads, 0, s>>>(d_src, d_dst, m, n, k_in.p, v_in.p, bad.p);
+        int end_bit = bits_for(n);
+        // Radix sort is stable: arcs with the same source keep insertion order.
+        cudaError_t e = cub_run([&](void *tmp, size_t &bytes) {
+            return cub::DeviceRadixSort::SortPairs(tmp, bytes, k_in.p, sorted_src.p, v_in.p,
+                                                   g->d_adj, arcs, 0, end_bit, s);
+        }, s);
+        if (e != cudaSuccess) { return fail(cuda_fail(e, "SortPairs(arcs)", __FILE__, __LINE__)); }
+    }
+    offsets_from_sorted_kernel<<<grid_for(arcs + 1), kThreads, 0, s>>>(sorted_src.p, arcs, n,
+                                                                        g->d_off);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+        return fail(BD_ERR_CUDA);
+    }
+    int flag = 0;
+    if (read_flag(bad.p, &flag) != BD_OK) { return fail(BD_ERR_CUDA); }
+    if (flag) { return fail(BD_ERR_RANGE); }
+    bd_status st = graph_finish(g, s);
+    if (st != BD_OK) { return fail(st); }
+    *out = g;
+    return BD_OK;
+}
+
+}  // namespace bd
+
+using namespace bd;
+
+extern "C" {
+
+bd_status bd_graph_from_edges(int64_t num_vertices, int64_t num_edges, const int64_t *src,
+                              const int64_t *dst, int32_t adjacency_order, bd_graph **out)
+{
+    if (!out || (!src && num_edges) || (!dst && num_edges) || num_vertices <= 0 || num_edges < 0) {
+        return BD_ERR_INVALID;
+    }
+    if (adjacency_order != BD_ORDER_INSERTION && adjacency_order != BD_ORDER_SORTED) {
+        return BD_ERR_INVALID;
+    }
+    if (num_vertices > (int64_t)UINT32_MAX) { return BD_ERR_LIMIT; }
+    BD_TRY(ensure_device());
+    int64_t *d_src = nullptr, *d_dst = nullptr;
+    size_t bytes = sizeof(int64_t) * (num_edges ? num_edges : 1);
+    if (cudaMalloc(&d_src, bytes) != cudaSuccess || cudaMalloc(&d_dst, bytes) != cudaSuccess) {
+        cudaFree(d_src);
+        cudaFree(d_dst);
+        return BD_ERR_OOM;
+    }
+    if (num_edges) {
+        cudaError_t e1 = cudaMemcpy(d_src, src, bytes, cudaMemcpyHostToDevice);
+        cudaError_t e2 = cudaMemcpy(d_dst, dst, bytes, cudaMemcpyHostToDevice);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            cudaFree(d_src);
+            cudaFree(d_dst);
+            return cuda_fail(e1 != cudaSuccess ? e1 : e2, "cudaMemcpy(edges)", __FILE__, __LINE__);
+        }
+    }
+    return graph_from_device_edges(num_vertices, num_edges, d_src, d_dst, adjacency_order, out);
+}
+
+bd_status bd_graph_from_el64(const char *path, int32_t adjacency_order, bd_graph **out)
+{
+    if (!path || !out) { return BD_ERR_INVALID; }
+    if (adjacency_order != BD_ORDER_INSERTION && adjacency_order != BD_ORDER_SORTED) {
+        return BD_ERR_INVALID;
+    }
+    FILE *fp = fopen(path, "rb");
+    if (!fp) { return BD_ERR_IO; }
+    int64_t nv = 0, ne = 0;
+    bd_status st = parse_el64_header(fp, &nv, &ne);
+    if (st != BD_OK) { fclose(fp); return st; }
+    if (nv > (int64_t)UINT32_MAX) { fclose(fp); return BD_ERR_LIMIT; }
+    st = ensure_device();
+    if (st != BD_OK) { fclose(fp); return st; }
+    // Stream the body through two pinned staging buffers into a device array
+    // of (src, dst) pairs, then split it.
+    int64_t *d_pairs = nullptr, *d_src = nullptr, *d_dst = nullptr;
+    const size_t chunk_pairs = (size_t)1 << 22;  // 64 MiB per staging buffer
+    int64_t *stage[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    cudaStream_t s = nullptr;
+    auto cleanup = [&]() {
+        if (s) { cudaStreamSynchronize(s); }
+        for (int i = 0; i < 2; ++i) {
+            if (stage[i]) { cudaFreeHost(stage[i]); }
+            if (done[i]) { cudaEventDestroy(done[i]); }
+        }
+        if (s) { cudaStreamDestroy(s); }
+        cudaFree(d_pairs);
+        fclose(fp);
+    };
+    if (cudaMalloc(&d_pairs, sizeof(int64_t) * 2 * ne) != cudaSuccess ||
+        cudaHostAlloc(&stage[0], sizeof(int64_t) * 2 * chunk_pairs, 0) != cudaSuccess ||
+        cudaHostAlloc(&stage[1], sizeof(int64_t) * 2 * chunk_pairs, 0) != cudaSuccess ||
+        cudaEventCreate(&done[0]) != cudaSuccess || cudaEventCreate(&done[1]) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        cleanup();
+        return BD_ERR_OOM;
+    }
+    int64_t pos = 0;
+    int which = 0;
+    while (pos < ne) {
+        size_t want = (size_t)std::min<int64_t>((int64_t)chunk_pairs, ne - pos);
+        if (cudaEventSynchronize(done[which]) != cudaSuccess) { cleanup(); return BD_ERR_CUDA; }
+        size_t got = fread(stage[which], sizeof(int64_t) * 2, want, fp);
+        if (got != want) { cleanup(); return BD_ERR_FORMAT; }  // unexpected EOF
+        if (cudaMemcpyAsync(d_pairs + 2 * pos, stage[which], sizeof(int64_t) * 2 * want,
+                            cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaEventRecord(done[which], s) != cudaSuccess) {
+            cleanup();
+            return BD_ERR_CUDA;
+        }
+        pos += (int64_t)want;
+        which ^= 1;
+    }
+    if (cudaMalloc(&d_src, sizeof(int64_t) * ne) != cudaSuccess ||
+        cudaMalloc(&d_dst, sizeof(int64_t) * ne) != cudaSuccess) {
+        cudaFree(d_src);
+        cudaFree(d_dst);
+        cleanup();
+        return BD_ERR_OOM;
+    }
+    split_pairs_kernel<<<grid_for(ne), kThreads, 0, s>>>(d_pairs, ne, d_src, d_dst);
+    cudaError_t e = cudaGetLastError();
+    cleanup();
+    if (e != cudaSuccess) {
+        cudaFree(d_src);
+        cudaFree(d_dst);
+        return cuda_fail(e, "split_pairs_kernel", __FILE__, __LINE__);
+    }
+    return graph_from_device_edges(nv, ne, d_src, d_dst, adjacency_order, out);
+}
+
+bd_status bd_graph_from_csr(int64_t num_vertices, int64_t num_arcs, const int64_t *offsets,
+                            const uint32_t *adjacency, bd_graph **out)
+{
+    if (!out || !offsets || (!adjacency && num_arcs) || num_vertices <= 0 || num_arcs < 0) {
+        return BD_ERR_INVALID;
+    }
+    if (num_vertices > (int64_t)UINT32_MAX) { return BD_ERR_LIMIT; }
+    BD_TRY(ensure_device());
+    auto *g = new bd_graph();
+    g->device = current_device();
+    g->n = num_vertices;
+    g->arcs = num_arcs;
+    g->m = num_arcs / 2;
+    if (cudaMalloc(&g->d_off, sizeof(int64_t) * (num_vertices + 1)) != cudaSuccess ||
+        cudaMalloc(&g->d_adj, sizeof(uint32_t) * (num_arcs ? num_arcs : 1)) != cudaSuccess) {
+        graph_free(g);
+        return BD_ERR_OOM;
+    }
+    DevBuf<int> bad;
+    if (bad.alloc(1) != cudaSuccess || cudaMemset(bad.p, 0, sizeof(int)) != cudaSuccess ||
+        cudaMemcpy(g->d_off, offsets, sizeof(int64_t) * (num_vertices + 1),
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        (num_arcs && cudaMemcpy(g->d_adj, adjacency, sizeof(uint32_t) * num_arcs,
+                                cudaMemcpyHostToDevice) != cudaSuccess)) {
+        graph_free(g);
+        return BD_ERR_CUDA;
+    }
+    validate_csr_kernel<<<grid_for(num_vertices), kThreads>>>(g->d_off, g->d_adj, num_vertices,
+                                                             num_arcs, bad.p);
+    int flag = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess || read_flag(bad.p, &flag) != BD_OK) {
+        graph_free(g);
+        return BD_ERR_CUDA;
+    }
+    if (flag) { graph_free(g); return BD_ERR_FORMAT; }
+    bd_status st = graph_finish(g, 0);
+    if (st != BD_OK) { graph_free(g); return st; }
+    *out = g;
+    return BD_OK;
+}
+
+bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, double c,
+                        double d, uint64_t seed, int32_t adjacency_order, bd_graph **out)
+{
+    if (!out || scale < 1 || scale > 30 || edge_factor < 1 || edge_factor > 1024) {
+        return BD_ERR_INVALID;
+    }
+    if (!(a >= 0 && b >= 0 && c >= 0 && d >= 0 && a <= 1 && b <= 1 && c <= 1 && d <= 1)) {
+        return BD_ERR_INVALID;
+    }
+    if (adjacency_order != BD_ORDER_INSERTION && adjacency_order != BD_ORDER_SORTED) {
+        return BD_ERR_INVALID;
+    }
+    BD_TRY(ensure_device());
+    const int64_t n = (int64_t)1 << scale;
+    const int64_t E = edge_factor << scale;
+    cudaStream_t s = 0;
+    DevBuf<uint64_t> keys, keys_sorted;
+    if (keys.alloc(E) != cudaSuccess || keys_sorted.alloc(E) != cudaSuccess) { return BD_ERR_OOM; }
+    rmat_keys_kernel<<<grid_for(E), kThreads, 0, s>>>(scale, E, a, b, c, d, seed, keys.p);
+    BD_CUDA(cudaGetLastError());
+    // flip + sort + dedup (rmat_dataset_dump.cc:48-53)
+    BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
+        return cub::DeviceRadixSort::SortKeys(tmp, bytes, keys.p, keys_sorted.p, E, 0, 2 * scale, s);
+    }, s));
+    DevBuf<int64_t> num_unique;
+    if (num_unique.alloc(1) != cudaSuccess) { return BD_ERR_OOM; }
+    BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
+        return cub::DeviceSelect::Unique(tmp, bytes, keys_sorted.p, keys.p, num_unique.p, E, s);
+    }, s));
+    int64_t m = 0;
+    BD_CUDA(cudaMemcpy(&m, num_unique.p, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    // relabel (rmat_dataset_dump.cc:55): vertex with the k-th smallest key -> k
+    DevBuf<uint64_t> vkeys, vkeys_sorted;
+    DevBuf<uint32_t> vidx, vidx_sorted, new_id;
+    if (vkeys.alloc(n) != cudaSuccess || vkeys_sorted.alloc(n) != cudaSuccess ||
+        vidx.alloc(n) != cudaSuccess || vidx_sorted.alloc(n) != cudaSuccess ||
+        new_id.alloc(n) != cudaSuccess) {
+        return BD_ERR_OOM;
+    }
+    perm_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(seed, kTagRelabel, n, vkeys.p, vidx.p);
+    BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
+        return cub::DeviceRadixSort::SortPairs(tmp, bytes, vkeys.p, vkeys_sorted.p, vidx.p,
+                                               vidx_sorted.p, n, 0, 64, s);
+    }, s));
+    scatter_rank_kernel<<<grid_for(n), kThreads, 0, s>>>(vidx_sorted.p, n, new_id.p);
+    // shuffle (rmat_dataset_dump.cc:57): order edges by a keyed permutation
+    DevBuf<uint64_t> ekeys, ekeys_sorted;
+    if (ekeys.alloc(m) != cudaSuccess || ekeys_sorted.alloc(m) != cudaSuccess) { return BD_ERR_OOM; }
+    edge_shuffle_keys_kernel<<<grid_for(m), kThreads, 0, s>>>(seed, m, ekeys.p);
+    BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
+        return cub::DeviceRadixSort::SortPairs(tmp, bytes, ekeys.p, ekeys_sorted.p, keys.p,
+                                               keys_sorted.p, m, 0, 64, s);
+    }, s));
+    int64_t *d_src = nullptr, *d_dst = nullptr;
+    if (cudaMalloc(&d_src, sizeof(int64_t) * (m ? m : 1)) != cudaSuccess ||
+        cudaMalloc(&d_dst, sizeof(int64_t) * (m ? m : 1)) != cudaSuccess) {
+        cudaFree(d_src);
+        cudaFree(d_dst);
+        return BD_ERR_OOM;
+    }
+    unpack_relabel_kernel<<<grid_for(m), kThreads, 0, s>>>(keys_sorted.p, m, scale, new_id.p,
+                                                           d_src, d_dst);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) { e = cudaStreamSynchronize(s); }
+    if (e != cudaSuccess) {
+        cudaFree(d_src);
+        cudaFree(d_dst);
+        return cuda_fail(e, "unpack_relabel_kernel", __FILE__, __LINE__);
+    }
+    // free the generator temporaries before the CSR build needs its memory
+    keys.reset();
+    keys_sorted.reset();
+    ekeys.reset();
+    ekeys_sorted.reset();
+    vkeys.reset();
+    vkeys_sorted.reset();
+    return graph_from_device_edges(n, m, d_src, d_dst, adjacency_order, out);
+}
+
+bd_status bd_graph_concat(bd_graph *const *graphs, int64_t count, bd_graph **out,
+                          int64_t *vertex_base)
+{
+    if (!graphs || count <= 0 || !out) { return BD_ERR_INVALID; }
+    int64_t n = 0, arcs = 0, m = 0;
+    for (int64_t i = 0; i < count; ++i) {
+        if (!graphs[i]) { return BD_ERR_INVALID; }
+        if (vertex_base) { vertex_base[i] = n; }
+        n += graphs[i]->n;
+        arcs += graphs[i]->arcs;
+        m += graphs[i]->m;
+    }
+    if (vertex_base) { vertex_base[count] = n; }
+    if (n > (int64_t)UINT32_MAX) { return BD_ERR_LIMIT; }
+    BD_TRY(ensure_device());
+    auto *g = new bd_graph();
+    g->device = current_device();
+    g->n = n;
+    g->arcs = arcs;
+    g->m = m;
+    g->order = graphs[0]->order;
+    if (cudaMalloc(&g->d_off, sizeof(int64_t) * (n + 1)) != cudaSuccess ||
+        cudaMalloc(&g->d_adj, sizeof(uint32_t) * (arcs ? arcs : 1)) != cudaSuccess) {
+        graph_free(g);
+        return BD_ERR_OOM;
+    }
+    int64_t vb = 0, ab = 0;
+    for (int64_t i = 0; i < count; ++i) {
+        const bd_graph *p = graphs[i];
+        shift_csr_kernel<<<grid_for(std::max(p->n, p->arcs)), kThreads>>>(
+            p->d_off, p->d_adj, p->n, p->arcs, vb, ab, g->d_off, g->d_adj);
+        vb += p->n;
+        ab += p->arcs;
+    }
+    set_last_offset_kernel<<<1, 1>>>(g->d_off, n, arcs);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+        graph_free(g);
+        return BD_ERR_CUDA;
+    }
+    bd_status st = graph_finish(g, 0);
+    if (st != BD_OK) { graph_free(g); return st; }
+    *out = g;
+    return BD_OK;
+}
+
+bd_status bd_graph_info(const bd_graph *g, int64_t *num_vertices, int64_t *num_edges)
+{
+    if (!g) { return BD_ERR_INVALID; }
+    if (num_vertices) { *num_vertices = g->n; }
+    if (num_edges) { *num_edges = g->m; }
+    return BD_OK;
+}
+
+bd_status bd_graph_copy_csr(const bd_graph *g, int64_t *offsets, uint32_t *adjacency)
+{
+    if (!g) { return BD_ERR_INVALID; }
+    BD_TRY(ensure_device());
+    if (offsets) {
+        BD_CUDA(cudaMemcpy(offsets, g->d_off, sizeof(int64_t) * (g->n + 1), cudaMemcpyDeviceToHost));
+    }
+    if (adjacency && g->arcs) {
+        BD_CUDA(cudaMemcpy(adjacency, g->d_adj, sizeof(uint32_t) * g->arcs, cudaMemcpyDeviceToHost));
+    }
+    return BD_OK;
+}
+
+bd_status bd_graph_copy_edges(const bd_graph *g, int64_t *src, int64_t *dst)
+{
+    if (!g) { return BD_ERR_INVALID; }
+    if (!g->d_src || !g->d_dst) { return BD_ERR_STATE; }
+    BD_TRY(ensure_device());
+    if (src && g->m) {
+        BD_CUDA(cudaMemcpy(src, g->d_src, sizeof(int64_t) * g->m, cudaMemcpyDeviceToHost));
+    }
+    if (dst && g->m) {
+        BD_CUDA(cudaMemcpy(dst, g->d_dst, sizeof(int64_t) * g->m, cudaMemcpyDeviceToHost));
+    }
+    return BD_OK;
+}
+
+// Same layout as dump_bin (generator/edge_list_utils.h:170-197).
+bd_status bd_graph_write_el64(const bd_graph *g, const char *path)
+{
+    if (!g || !path) { return BD_ERR_INVALID; }
+    if (!g->d_src || !g->d_dst) { return BD_ERR_STATE; }
+    BD_TRY(ensure_device());
+    FILE *fp = fopen(path, "wb");
+    if (!fp) { return BD_ERR_IO; }
+    fprintf(fp, " --format el64 --num_edges %lld --num_vertices %lld --is_undirected"
+                " --is_deduped --is_permuted\n",
+            (long long)g->m, (long long)g->n);
+    const int64_t chunk = (int64_t)1 << 22;
+    std::vector<int64_t> s(chunk), d(chunk), pairs(2 * chunk);
+    for (int64_t pos = 0; pos < g->m; pos += chunk) {
+        int64_t cnt = std::min(chunk, g->m - pos);
+        if (cudaMemcpy(s.data(), g->d_src + pos, sizeof(int64_t) * cnt, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(d.data(), g->d_dst + pos, sizeof(int64_t) * cnt, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            fclose(fp);
+            return BD_ERR_CUDA;
+        }
+        for (int64_t i = 0; i < cnt; ++i) {
+            pairs[2 * i] = s[i];
+            pairs[2 * i + 1] = d[i];
+        }
+        if (fwrite(pairs.data(), sizeof(int64_t) * 2, cnt, fp) != (size_t)cnt) {
+            fclose(fp);
+            return BD_ERR_IO;
+        }
+    }
+    if (fclose(fp) != 0) { return BD_ERR_IO; }
+    return BD_OK;
+}
+
+bd_status bd_graph_check(const bd_graph *g, int32_t *ok)
+{
+    if (!g || !ok) { return BD_ERR_INVALID; }
+    if (!g->d_src || !g->d_dst) { return BD_ERR_STATE; }
+    BD_TRY(ensure_device());
+    DevBuf<int> bad;
+    if (bad.alloc(1) != cudaSuccess) { return BD_ERR_OOM; }
+    BD_CUDA(cudaMemset(bad.p, 0, sizeof(int)));
+    graph_check_kernel<<<grid_for(g->m), kThreads>>>(g->d_src, g->d_dst, g->m, g->d_off, g->d_adj,
+                                                     g->arcs, g->order == BD_ORDER_SORTED, bad.p);
+    adjacent_dup_kernel<<<grid_for(g->n), kThreads>>>(g->d_off, g->d_adj, g->n, bad.p);
+    BD_CUDA(cudaGetLastError());
+    BD_CUDA(cudaDeviceSynchronize());
+    int flag = 0;
+    BD_TRY(read_flag(bad.p, &flag));
+    *ok = flag ? 0 : 1;
+    return BD_OK;
+}
+
+bd_status bd_graph_pick_roots(const bd_graph *g, uint64_t seed, int64_t k, int64_t *roots)
+{
+    if (!g || k < 0 || (!roots && k)) { return BD_ERR_INVALID; }
+    if (k == 0) { return BD_OK; }
+    if (g->arcs == 0) { return BD_ERR_INVALID; }  // no vertex of nonzero degree
+    BD_TRY(ensure_device());
+    DevBuf<int64_t> d_roots;
+    DevBuf<int> status;
+    if (d_roots.alloc(k) != cudaSuccess || status.alloc(1) != cudaSuccess) { return BD_ERR_OOM; }
+    BD_CUDA(cudaMemset(status.p, 0, sizeof(int)));
+    pick_roots_kernel<<<1, 1>>>(g->d_off, g->n, seed, k, d_roots.p, status.p);
+    BD_CUDA(cudaGetLastError());
+    BD_CUDA(cudaDeviceSynchronize());
+    int flag = 0;
+    BD_TRY(read_flag(status.p, &flag));
+    if (flag) { return BD_ERR_LIMIT; }
+    BD_CUDA(cudaMemcpy(roots, d_roots.p, sizeof(int64_t) * k, cudaMemcpyDeviceToHost));
+    return BD_OK;
+}
+
+bd_status bd_graph_device_csr(const bd_graph *g, const int64_t **offsets,
+                              const uint32_t **adjacency)
+{
+    if (!g) { return BD_ERR_INVALID; }
+    if (offsets) { *offsets = g->d_off; }
+    if (adjacency) { *adjacency = g->d_adj; }
+    return BD_OK;
+}
+
+bd_status bd_graph_destroy(bd_graph *g)
+{
+    if (!g) { return BD_ERR_INVALID; }
+    cudaSetDevice(g->device);
+    graph_free(g);
+    return BD_OK;
+}
+
+}  // extern "C"

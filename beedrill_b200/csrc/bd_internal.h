@@ -1,0 +1,66 @@
+// bd_internal.h -- shared definitions of the B200 BFS library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "beedrill_b200.h"
+
+namespace bd {
+
+// Records the failing CUDA call for bd_status_string-style diagnostics and
+// returns BD_ERR_CUDA.
+bd_status cuda_fail(cudaError_t err, const char *what, const char *file, int line);
+// Library-wide device selection (bd_set_device).
+int current_device();
+// Checks that the selected device is usable (sm_100) and makes it current.
+bd_status ensure_device();
+
+}  // namespace bd
+
+#define BD_CUDA(call)                                                        \
+    do {                                                                     \
+        cudaError_t bd_e_ = (call);                                          \
+        if (bd_e_ != cudaSuccess) {                                          \
+            return bd::cuda_fail(bd_e_, #call, __FILE__, __LINE__);          \
+        }                                                                    \
+    } while (0)
+
+#define BD_TRY(expr)                                                         \
+    do {                                                                     \
+        bd_status bd_s_ = (expr);                                            \
+        if (bd_s_ != BD_OK) { return bd_s_; }                                \
+    } while (0)
+
+// A graph resident in HBM: CSR with int64 offsets and uint32 neighbour ids,
+// plus a bitmap with one bit per vertex of degree zero (padding bits past n
+// are set too, so bit scans can treat them as already finished).
+struct bd_graph {
+    int device = 0;
+    int64_t n = 0;          // vertices
+    int64_t m = 0;          // undirected edges (arcs / 2)
+    int64_t arcs = 0;       // entries of the adjacency array
+    int32_t order = BD_ORDER_INSERTION;
+    int64_t *d_off = nullptr;     // [n + 1]
+    uint32_t *d_adj = nullptr;    // [arcs]
+    uint32_t *d_isolated = nullptr;  // [words(n)]
+    // Edge list in file / generation order, kept for el64 export and check.
+    int64_t *d_src = nullptr;     // [m] or null
+    int64_t *d_dst = nullptr;     // [m] or null
+};
+
+namespace bd {
+
+inline int64_t bitmap_words(int64_t n) { return (n + 31) / 32; }
+
+// Builds the CSR of an edge list that is already on the device (src/dst
+// int64[m]); takes ownership of d_src/d_dst.
+bd_status graph_from_device_edges(int64_t n, int64_t m, int64_t *d_src, int64_t *d_dst,
+                                  int32_t order, bd_graph **out);
+// Fills d_isolated from d_off.
+bd_status graph_finish(bd_graph *g, cudaStream_t s);
+void graph_free(bd_graph *g);
+
+}  // namespace bd

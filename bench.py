@@ -1,0 +1,329 @@
+"""Benchmark: harmonic-mean GTEPS over 64 roots on a seeded RMAT scale-24 graph.
+
+One "step" is one pass of the hot path over one batch of synthetic input: a
+BFS from each of 64 roots (lcg(0) picker of hybrid_bfs_main.cc:136-144) on a
+seeded RMAT scale-24 graph (A=.57 B=.19 C=.19 D=.05, edge factor 16,
+deduplicated, symmetrised; int64 offsets, uint32 ids), generated on the
+device.  Per root, time covers run_* only, as in the reference
+(hybrid_bfs_main.cc:267-282): clear() is outside, the source setup inside.
+TEPS = count_num_traversed_edges() / time; the metric is the harmonic mean of
+the per-root GTEPS (combined.cc:124-128).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs an independent
+replica on its own 64 roots (lcg(rank)); there is no collective on the data
+path.  value = N x harmonic mean over all ranks' roots, timed as the max over
+ranks.
+
+--impl reference times the reference's own CPU build (oracle/_ref/hybrid_bfs,
+the unmodified hybrid_bfs sources compiled as a Cilk serial elision: 1 core)
+on the same graph, written as an el64 file, over a bounded sample of roots.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "harmonic-mean GTEPS over 64 roots, RMAT scale 24, learned vs plain switch, 1 B200"
+UNIT = "GTEPS"
+SCALE = 24
+EDGE_FACTOR = 16
+GRAPH_SEED = 24
+NUM_ROOTS = 64
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "hybrid_bfs")
+
+
+def hmean(x):
+    x = np.asarray(x, np.float64)
+    return float(len(x) / np.sum(1.0 / x))
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_cpu_run(el64_path: str, trials: int, timeout: float):
+    """Runs the reference CLI (serial elision, one core) and returns the
+    per-trial (edges, ms) it prints (hybrid_bfs_main.cc:297-301)."""
+    cmd = [REF_BIN, "--graph_filename", el64_path, "--algorithm", "beamer_hybrid",
+           "--num_trials", str(trials)]
+    try:
+        cmd = ["taskset", "-c", str(max(0, (os.cpu_count() or 1) - 1))] + cmd
+        out = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                             timeout=timeout).stdout
+    except (subprocess.TimeoutExpired, FileNotFoundError, OSError) as e:
+        return None, str(e)
+    rows = [(int(a), float(b)) for a, b in
+            re.findall(r"Traversed (\d+) edges in ([0-9.]+) ms", out)]
+    return rows, out[-400:]
+
+
+def impl_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    if not os.path.exists(REF_BIN):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/hybrid_bfs was not built (reference sources absent at build time)"}))
+        return 0
+    import beedrill_b200 as bd
+    g = bd.Graph.rmat(SCALE, EDGE_FACTOR, seed=GRAPH_SEED)
+    n, m = g.num_vertices(), g.num_edges()
+    with tempfile.TemporaryDirectory(dir=os.environ.get("BD_TMP", None)) as tmp:
+        path = os.path.join(tmp, f"rmat{SCALE}.el64")
+        g.write_el64(path)
+        g.close()
+        trials = args.warmup + args.steps
+        t0 = time.time()
+        rows, tail = reference_cpu_run(path, trials, timeout=3000)
+        wall = time.time() - t0
+    if not rows or len(rows) < trials:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {tail}"}))
+        return 0
+    timed = rows[args.warmup:]
+    gteps = [e / (ms * 1e-3) / 1e9 for e, ms in timed]
+    value = hmean(gteps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": float(np.mean([ms for _, ms in timed])), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "i64", "data": "synthetic",
+        "config": {"workload": f"rmat-scale{SCALE}-ef{EDGE_FACTOR} lcg(0) roots, one root per step",
+                   "scale": SCALE, "edge_factor": EDGE_FACTOR, "graph_seed": GRAPH_SEED,
+                   "num_vertices": n, "num_edges": m},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"{args.steps} timed roots after {args.warmup} warm-up roots of "
+                                   f"lcg(0), reference serial-elision build on 1 pinned core; "
+                                   f"process wall {wall:.0f} s incl. el64 load + graph build"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=SCALE)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-roots", type=int, default=3)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return impl_reference(args)
+
+    world, rank, local = dist_setup()
+    import beedrill_b200 as bd
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    bd.lib().bd_set_device(local)
+
+    scale = args.scale
+    t_gen = time.time()
+    g = bd.Graph.rmat(scale, EDGE_FACTOR, seed=GRAPH_SEED)
+    gen_s = time.time() - t_gen
+    n, m = g.num_vertices(), g.num_edges()
+    roots = g.pick_roots(rank, NUM_ROOTS)
+
+    # CPU baseline: the reference's own build on a bounded sample of the same
+    # workload, in the background while the GPU is measured (rank 0, N = 1).
+    cpu_thread = None
+    cpu_result = {}
+    tmpdir = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_BIN):
+        tmpdir = tempfile.TemporaryDirectory(dir=os.environ.get("BD_TMP", None))
+        el64 = os.path.join(tmpdir.name, f"rmat{scale}.el64")
+        g.write_el64(el64)
+
+        def cpu_job():
+            t0 = time.time()
+            rows, tail = reference_cpu_run(el64, args.cpu_roots, timeout=1200)
+            cpu_result["rows"], cpu_result["tail"] = rows, tail
+            cpu_result["wall"] = time.time() - t0
+
+        cpu_thread = threading.Thread(target=cpu_job, daemon=True)
+        cpu_thread.start()
+
+    bfs = bd.HybridBFS(g, alg="beamer_hybrid")
+    for _ in range(args.warmup):
+        bfs.run_many(roots)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    barrier()
+    per_root_ms, per_root_edges, per_root_reached, e2e_ms = [], [], [], []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            ms, edges, reached, e2e = bfs.run_many(roots, with_reached=True)
+            per_root_ms.append(ms)
+            per_root_edges.append(edges)
+            per_root_reached.append(reached)
+            e2e_ms.append(e2e)
+    barrier()
+    ms = np.concatenate(per_root_ms)
+    edges = np.concatenate(per_root_edges)
+    reached = np.concatenate(per_root_reached)
+    gteps = edges / (ms * 1e-3) / 1e9
+    value_rank = hmean(gteps)
+    step_ms = float(np.mean([x.sum() for x in per_root_ms]))
+    e2e_gteps = hmean(np.concatenate([e / (t / NUM_ROOTS * 1e-3) / 1e9
+                                      for e, t in zip(per_root_edges, e2e_ms)]))
+    if world > 1:
+        import torch
+        t = torch.tensor([step_ms, -value_rank, -e2e_gteps], device=f"cuda:{local}",
+                         dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms, worst, worst_e2e = float(t[0]), -float(t[1]), -float(t[2])
+        value = world * worst
+        e2e_value = world * worst_e2e
+    else:
+        value, e2e_value = value_rank, e2e_gteps
+
+    # roofline of the dominant kernel (the persistent BFS kernel, one launch
+    # per root): B_alg = 8(n+1) + 4*(2 m_c) + 12 n_c bytes per root.
+    b_alg = 8.0 * (n + 1) + 8.0 * edges + 12.0 * reached
+    achieved = float(b_alg.sum() / (ms.sum() * 1e-3) / 1e9)
+    peak, peak_kind = peaks()
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(f"rmat{scale}", {}).get("bytes_per_launch")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {
+            "workload": f"rmat-scale{scale}-ef{EDGE_FACTOR} seed {GRAPH_SEED}, {NUM_ROOTS} roots per step, "
+                        f"one persistent launch per root",
+            "scale": scale, "edge_factor": EDGE_FACTOR, "graph_seed": GRAPH_SEED,
+            "num_vertices": n, "num_edges": m, "roots": NUM_ROOTS, "root_seed": rank,
+            "policy": "beamer_hybrid alpha=15 beta=18",
+            "l2": "inputs larger than L2 (CSR %.2f GB)" % ((8 * (n + 1) + 8 * m) / 1e9),
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "graph_build_s": round(gen_s, 2),
+        },
+        "plain_beamer_gteps": value,
+        "per_root_ms": {"min": float(ms.min()), "median": float(np.median(ms)), "max": float(ms.max())},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_kind": peak_kind,
+                     "note": "B_alg = 8(n+1) + 8 m_c + 12 n_c per root over the run time"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * NUM_ROOTS,
+                "d2h_bytes_per_step": 16 * NUM_ROOTS,
+                "note": "run_many: root upload, clear + run per root, m_c/n_c download"},
+        "gpu_launches": 3 * NUM_ROOTS * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if cpu_thread is not None:
+        cpu_thread.join()
+        rows = cpu_result.get("rows")
+        if rows:
+            cg = [e / (t * 1e-3) / 1e9 for e, t in rows]
+            line["cpu_baseline"] = {
+                "value": hmean(cg), "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"{len(rows)} lcg(0) roots of the same graph, reference serial-elision "
+                          f"build (oracle/_ref/hybrid_bfs) pinned to 1 core; wall "
+                          f"{cpu_result['wall']:.0f} s incl. el64 load + graph build"}
+        else:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                                    "sample": f"failed: {cpu_result.get('tail')}"}
+        tmpdir.cleanup()
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

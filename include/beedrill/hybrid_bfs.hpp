@@ -1,0 +1,208 @@
+// beedrill/hybrid_bfs.hpp -- C++ facade over the C ABI, keeping the public
+// surface of the reference's hybrid_bfs class (hybrid_bfs.h:11-47) and the
+// graph / edge-list calls its driver makes (hybrid_bfs_main.cc:164-246).
+//
+// Differences from the reference, by design:
+//   * errors throw beedrill::error (carrying the bd_status) instead of
+//     assert() / exit(1);
+//   * the graph and BFS state live in HBM; results are copied to the host
+//     only when asked for (depths(), parents(), check(), print_tree()).
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "beedrill_b200.h"
+
+namespace beedrill {
+
+class error : public std::runtime_error {
+public:
+    error(bd_status s, const std::string &what)
+        : std::runtime_error(what + ": " + bd_status_string(s)), status(s) {}
+    bd_status status;
+};
+
+inline void throw_if(bd_status s, const char *what)
+{
+    if (s != BD_OK) { throw error(s, what); }
+}
+
+// The graph (graph_base.h): a CSR in HBM.
+class graph {
+public:
+    static graph from_el64(const std::string &path, int32_t order = BD_ORDER_INSERTION)
+    {
+        bd_graph *h = nullptr;
+        throw_if(bd_graph_from_el64(path.c_str(), order, &h), "load_binary");
+        return graph(h);
+    }
+    static graph rmat(int32_t scale, int64_t edge_factor = 16, uint64_t seed = 0,
+                      double a = 0.57, double b = 0.19, double c = 0.19, double d = 0.05,
+                      int32_t order = BD_ORDER_INSERTION)
+    {
+        bd_graph *h = nullptr;
+        throw_if(bd_graph_rmat(scale, edge_factor, a, b, c, d, seed, order, &h), "rmat");
+        return graph(h);
+    }
+    explicit graph(bd_graph *h) : h_(h) {}
+    graph(graph &&o) noexcept : h_(std::exchange(o.h_, nullptr)) {}
+    graph &operator=(graph &&o) noexcept
+    {
+        std::swap(h_, o.h_);
+        return *this;
+    }
+    graph(const graph &) = delete;
+    graph &operator=(const graph &) = delete;
+    ~graph()
+    {
+        if (h_) { bd_graph_destroy(h_); }
+    }
+
+    long num_vertices() const
+    {
+        int64_t n = 0;
+        throw_if(bd_graph_info(h_, &n, nullptr), "num_vertices");
+        return (long)n;
+    }
+    long num_edges() const
+    {
+        int64_t m = 0;
+        throw_if(bd_graph_info(h_, nullptr, &m), "num_edges");
+        return (long)m;
+    }
+    // graph::check (graph_base.h:110-134)
+    bool check() const
+    {
+        int32_t ok = 0;
+        throw_if(bd_graph_check(h_, &ok), "check_graph");
+        return ok != 0;
+    }
+    // pick_random_vertex with lcg(seed) (hybrid_bfs_main.cc:136-144)
+    std::vector<int64_t> pick_roots(uint64_t seed, int64_t k) const
+    {
+        std::vector<int64_t> r(k);
+        throw_if(bd_graph_pick_roots(h_, seed, k, r.data()), "pick_roots");
+        return r;
+    }
+    void csr(std::vector<int64_t> &offsets, std::vector<uint32_t> &adjacency) const
+    {
+        offsets.resize(num_vertices() + 1);
+        throw_if(bd_graph_copy_csr(h_, offsets.data(), nullptr), "csr");
+        adjacency.resize(offsets.back());
+        throw_if(bd_graph_copy_csr(h_, offsets.data(), adjacency.data()), "csr");
+    }
+    void write_el64(const std::string &path) const
+    {
+        throw_if(bd_graph_write_el64(h_, path.c_str()), "write_el64");
+    }
+    bd_graph *handle() const { return h_; }
+
+private:
+    bd_graph *h_ = nullptr;
+};
+
+// hybrid_bfs (hybrid_bfs.h:11-47).
+class hybrid_bfs {
+public:
+    explicit hybrid_bfs(graph &g, const bd_bfs_opts *opts = nullptr) : g_(g)
+    {
+        throw_if(bd_bfs_create(g.handle(), opts, &h_), "hybrid_bfs");
+    }
+    hybrid_bfs(const hybrid_bfs &) = delete;
+    hybrid_bfs &operator=(const hybrid_bfs &) = delete;
+    ~hybrid_bfs()
+    {
+        if (h_) { bd_bfs_destroy(h_); }
+    }
+
+    void clear() { throw_if(bd_bfs_clear(h_), "clear"); }
+    void run_beamer(long source, long alpha, long beta)
+    {
+        throw_if(bd_bfs_run_beamer(h_, source, alpha, beta, &stats_), "run_beamer");
+    }
+    void run_with_migrating_threads(long source)
+    {
+        throw_if(bd_bfs_run_top_down(h_, source, &stats_), "run_with_migrating_threads");
+    }
+    void run_with_remote_writes(long source)
+    {
+        throw_if(bd_bfs_run_top_down(h_, source, &stats_), "run_with_remote_writes");
+    }
+    void run_with_remote_writes_hybrid(long source, long alpha, long beta)
+    {
+        throw_if(bd_bfs_run_beamer(h_, source, alpha, beta, &stats_),
+                 "run_with_remote_writes_hybrid");
+    }
+    void run_top_down(long source) { throw_if(bd_bfs_run_top_down(h_, source, &stats_), "top_down"); }
+    void run_bottom_up(long source)
+    {
+        throw_if(bd_bfs_run_bottom_up(h_, source, &stats_), "bottom_up");
+    }
+    // Runs the policy the handle was created with (beamer / learned / ...).
+    void run(long source) { throw_if(bd_bfs_run(h_, source, &stats_), "run"); }
+
+    bool check(long source)
+    {
+        int32_t ok = 0;
+        throw_if(bd_bfs_check(h_, source, &ok), "check");
+        return ok != 0;
+    }
+    long count_num_traversed_edges()
+    {
+        int64_t m = 0;
+        throw_if(bd_bfs_count_traversed_edges(h_, &m), "count_num_traversed_edges");
+        return (long)m;
+    }
+    // print_tree (hybrid_bfs.cc:381-399)
+    void print_tree()
+    {
+        std::vector<int64_t> p = parents();
+        for (size_t v = 0; v < p.size(); ++v) {
+            long parent = (long)p[v];
+            if (parent < 0) { continue; }
+            printf("%4zu", v);
+            while (true) {
+                printf(" <- %4li", parent);
+                if (parent == -1) { break; }
+                if (parent == p[parent]) { break; }
+                parent = (long)p[parent];
+            }
+            printf("\n");
+        }
+        fflush(stdout);
+    }
+    std::vector<int32_t> depths()
+    {
+        std::vector<int32_t> d(g_.num_vertices());
+        throw_if(bd_bfs_get_depths(h_, d.data()), "depths");
+        return d;
+    }
+    std::vector<int64_t> parents()
+    {
+        std::vector<int64_t> p(g_.num_vertices());
+        throw_if(bd_bfs_get_parents(h_, p.data()), "parents");
+        return p;
+    }
+    std::vector<bd_step> steps()
+    {
+        int64_t count = 0;
+        throw_if(bd_bfs_get_steps(h_, nullptr, 0, &count), "steps");
+        std::vector<bd_step> s(count);
+        throw_if(bd_bfs_get_steps(h_, s.data(), count, &count), "steps");
+        return s;
+    }
+    const bd_run_stats &last_stats() const { return stats_; }
+    bd_bfs *handle() const { return h_; }
+
+private:
+    graph &g_;
+    bd_bfs *h_ = nullptr;
+    bd_run_stats stats_{};
+};
+
+}  // namespace beedrill

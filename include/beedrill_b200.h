@@ -1,0 +1,176 @@
+/* beedrill_b200.h -- C ABI of the B200 direction-optimizing BFS.
+ *
+ * This is the drop-in boundary for Beedrill's `hybrid_bfs` class
+ * (hybrid_bfs.h:11-47) and the graph/edge-list layer it sits on
+ * (graph_base.h, dist_edge_list.h, edge_list.h).  Plain C types only: host
+ * pointers and sizes in, status codes out.  Every entry point returns
+ * BD_OK (0) or a negative bd_status; none of them calls exit() or traps.
+ *
+ * Ownership: handles are opaque.  Device memory allocated by the library is
+ * released only by the matching *_destroy call.  A handle is not thread
+ * safe; use one host thread per handle.  Each bd_bfs owns a CUDA stream.
+ *
+ * Reference interface -> entry point:
+ *   dist_edge_list::load_binary (dist_edge_list.cc:50-143)
+ *     + create_graph_from_edge_list (graph_base.h:335-436)  -> bd_graph_from_el64
+ *   create_graph_from_edge_list on in-memory edges          -> bd_graph_from_edges
+ *   graph::check (graph_base.h:110-134)                     -> bd_graph_check
+ *   generator/rmat_dataset_dump.cc (seeded, on the device)  -> bd_graph_rmat
+ *   pick_random_vertex + lcg (hybrid_bfs_main.cc:136-144)   -> bd_graph_pick_roots
+ *   hybrid_bfs::hybrid_bfs(graph&) (hybrid_bfs.cc:10-18)    -> bd_bfs_create
+ *   hybrid_bfs::clear (hybrid_bfs.cc:433-443)               -> bd_bfs_clear
+ *   hybrid_bfs::run_beamer (hybrid_bfs.cc:152-191)          -> bd_bfs_run_beamer
+ *   run_with_migrating_threads / run_with_remote_writes
+ *     (hybrid_bfs.cc:196-235)                               -> bd_bfs_run_top_down
+ *   run_with_remote_writes_hybrid (hybrid_bfs.cc:243-277)   -> bd_bfs_run_beamer
+ *   hybrid_bfs::check (hybrid_bfs.cc:281-379)               -> bd_bfs_check
+ *   hybrid_bfs::count_num_traversed_edges (:401-414)        -> bd_bfs_count_traversed_edges
+ *   hybrid_bfs::print_tree (hybrid_bfs.cc:381-399)          -> bd_bfs_get_parents (+ host printing)
+ */
+#ifndef BEEDRILL_B200_H
+#define BEEDRILL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int bd_status;
+#define BD_OK 0
+#define BD_ERR_INVALID (-1)    /* bad argument (null pointer, bad size, bad enum)    */
+#define BD_ERR_IO (-2)         /* file cannot be opened / read / written              */
+#define BD_ERR_FORMAT (-3)     /* el64 header or body rejected (edge_list.cc rules)  */
+#define BD_ERR_OOM (-4)        /* host or device allocation failed                    */
+#define BD_ERR_CUDA (-5)       /* a CUDA runtime call failed                          */
+#define BD_ERR_TIMEOUT (-6)    /* a bounded device-side wait ran out                  */
+#define BD_ERR_RANGE (-7)      /* vertex id out of range (hybrid_bfs.cc:155 assert)   */
+#define BD_ERR_STATE (-8)      /* call out of order (e.g. results before a run)       */
+#define BD_ERR_NODEV (-9)      /* no usable CUDA device (sm_100 required)             */
+#define BD_ERR_LIMIT (-10)     /* size beyond a documented limit                      */
+
+typedef struct bd_graph bd_graph;
+typedef struct bd_bfs bd_bfs;
+
+/* Adjacency order inside each vertex's neighbour list. */
+#define BD_ORDER_INSERTION 0 /* reference order: file order, (s->d) then (d->s) */
+#define BD_ORDER_SORTED 1    /* ascending neighbour id                          */
+
+/* Direction policies (the reference's --algorithm values map onto these). */
+#define BD_ALG_BEAMER 0    /* beamer_hybrid, remote_writes_hybrid                */
+#define BD_ALG_TOP_DOWN 1  /* migrating_threads, remote_writes, top_down         */
+#define BD_ALG_BOTTOM_UP 2 /* bottom_up                                          */
+#define BD_ALG_LEARNED 3   /* MLP direction policy, Beamer as the fallback       */
+
+#define BD_DIR_TOP_DOWN 0
+#define BD_DIR_BOTTOM_UP 1
+
+typedef struct bd_bfs_opts {
+    int32_t alg;          /* BD_ALG_*                                            */
+    int32_t min_parent;   /* 1: parent(v) = smallest neighbour one level up      */
+    int64_t alpha;        /* Beamer alpha (hybrid_bfs_main.cc:74), must be > 0   */
+    int64_t beta;         /* Beamer beta (hybrid_bfs_main.cc:75), must be > 0    */
+    int32_t block_size;   /* threads per CTA; 0 = tuned default                  */
+    int32_t large_degree; /* top-down CTA-split threshold; 0 = tuned default     */
+    int32_t chunk_edges;  /* edges per split work unit; 0 = tuned default        */
+    int32_t bu_prefix;    /* bottom-up per-thread scan before warp scan; 0 = def */
+    int64_t spin_limit;   /* grid-barrier wait bound in polls; 0 = default (~2 s) */
+    int32_t test_extra_ctas; /* TEST ONLY: barrier expects this many extra CTAs,
+                                so it can never complete and must time out      */
+    int32_t reserved;
+} bd_bfs_opts;
+
+/* One BFS step as recorded on the device. */
+typedef struct bd_step {
+    int32_t dir;          /* BD_DIR_*                                             */
+    int32_t level;        /* depth of the frontier this step expanded             */
+    int64_t frontier;     /* vertices in that frontier                            */
+    int64_t frontier_edges; /* sum of their degrees (m_f)                         */
+    int64_t unexplored_edges; /* 2m - degree sum of all visited vertices (m_u)    */
+    int64_t found;        /* vertices discovered by the step                      */
+    int64_t ns;           /* device time of the step (ns, %globaltimer)           */
+} bd_step;
+
+typedef struct bd_run_stats {
+    double ms;            /* CUDA-event time of the traversal kernel(s)           */
+    int64_t num_steps;    /* steps taken (the last one discovers nothing)         */
+    int64_t reached;      /* vertices reached, source included (n_c)              */
+    int64_t traversed_edges; /* count_num_traversed_edges(): m_c                  */
+    int64_t top_down_steps;
+    int64_t bottom_up_steps;
+} bd_run_stats;
+
+/* ---- library ------------------------------------------------------------- */
+const char *bd_status_string(bd_status s);
+const char *bd_version(void);
+/* Select the CUDA device used by handles created afterwards (default 0). */
+bd_status bd_set_device(int device);
+
+/* ---- graphs --------------------------------------------------------------- */
+bd_status bd_graph_from_el64(const char *path, int32_t adjacency_order, bd_graph **out);
+bd_status bd_graph_from_edges(int64_t num_vertices, int64_t num_edges, const int64_t *src,
+                              const int64_t *dst, int32_t adjacency_order, bd_graph **out);
+bd_status bd_graph_from_csr(int64_t num_vertices, int64_t num_arcs, const int64_t *offsets,
+                            const uint32_t *adjacency, bd_graph **out);
+/* Seeded RMAT graph built on the device: edge_factor << scale generated
+ * edges, self loops re-rolled, flipped, sorted, deduplicated, vertex ids
+ * permuted and edge order shuffled by `seed`. */
+bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, double c,
+                        double d, uint64_t seed, int32_t adjacency_order, bd_graph **out);
+/* Disjoint union of graphs: vertex ids of graph i are shifted by the vertex
+ * count of graphs 0..i-1.  vertex_base (host, count+1 entries) receives the
+ * shifts; may be NULL. */
+bd_status bd_graph_concat(bd_graph *const *graphs, int64_t count, bd_graph **out,
+                          int64_t *vertex_base);
+bd_status bd_graph_info(const bd_graph *g, int64_t *num_vertices, int64_t *num_edges);
+/* Copy the CSR to host buffers of n+1 and 2m entries. */
+bd_status bd_graph_copy_csr(const bd_graph *g, int64_t *offsets, uint32_t *adjacency);
+/* Edge list (generated / loaded order); only for graphs built from edges. */
+bd_status bd_graph_copy_edges(const bd_graph *g, int64_t *src, int64_t *dst);
+bd_status bd_graph_write_el64(const bd_graph *g, const char *path);
+/* graph::check: every edge present in both lists, no adjacent duplicates.
+ * ok receives 1 (pass) or 0. */
+bd_status bd_graph_check(const bd_graph *g, int32_t *ok);
+/* Roots as hybrid_bfs_main.cc:136-144 with lcg(seed). */
+bd_status bd_graph_pick_roots(const bd_graph *g, uint64_t seed, int64_t k, int64_t *roots);
+/* Device pointers of the CSR (borrowed, valid until bd_graph_destroy). */
+bd_status bd_graph_device_csr(const bd_graph *g, const int64_t **offsets,
+                              const uint32_t **adjacency);
+bd_status bd_graph_destroy(bd_graph *g);
+
+/* ---- BFS ------------------------------------------------------------------ */
+void bd_bfs_default_opts(bd_bfs_opts *opts);
+bd_status bd_bfs_create(bd_graph *g, const bd_bfs_opts *opts, bd_bfs **out);
+bd_status bd_bfs_clear(bd_bfs *b);
+/* Run with the handle's policy (opts.alg).  stats may be NULL. */
+bd_status bd_bfs_run(bd_bfs *b, int64_t source, bd_run_stats *stats);
+bd_status bd_bfs_run_beamer(bd_bfs *b, int64_t source, int64_t alpha, int64_t beta,
+                            bd_run_stats *stats);
+bd_status bd_bfs_run_top_down(bd_bfs *b, int64_t source, bd_run_stats *stats);
+bd_status bd_bfs_run_bottom_up(bd_bfs *b, int64_t source, bd_run_stats *stats);
+/* Several sources expanded as one BFS (level 0 = all sources).  On a graph
+ * made by bd_graph_concat with one source per part, each part gets its own
+ * BFS tree and depths. */
+bd_status bd_bfs_run_multi(bd_bfs *b, const int64_t *sources, int64_t count,
+                           bd_run_stats *stats);
+/* k single-source BFSs, one after another, with clear() before each (the
+ * trial loop of hybrid_bfs_main.cc:252-302).  ms_out[i], edges_out[i] and
+ * reached_out[i] (each may be NULL) get root i's run time, m_c and n_c.
+ * e2e_ms (may be NULL) gets the device time of the whole call, from the
+ * copy of the roots to the device to the copy of the results back. */
+bd_status bd_bfs_run_many(bd_bfs *b, const int64_t *sources, int64_t k, double *ms_out,
+                          int64_t *edges_out, int64_t *reached_out, double *e2e_ms);
+bd_status bd_bfs_get_depths(bd_bfs *b, int32_t *depth);
+bd_status bd_bfs_get_parents(bd_bfs *b, int64_t *parent);
+bd_status bd_bfs_device_ptrs(bd_bfs *b, const int32_t **depth, const int64_t **parent);
+bd_status bd_bfs_count_traversed_edges(bd_bfs *b, int64_t *out);
+bd_status bd_bfs_check(bd_bfs *b, int64_t source, int32_t *ok);
+/* Per-step records of the last run (count <= capacity copied). */
+bd_status bd_bfs_get_steps(bd_bfs *b, bd_step *steps, int64_t capacity, int64_t *count);
+bd_status bd_bfs_destroy(bd_bfs *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

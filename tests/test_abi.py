@@ -1,0 +1,63 @@
+"""The C ABI library: loads, exports every declared entry point, and fails
+loudly (a status code, no fallback) when no GPU is present.  CPU only."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import beedrill_b200 as bd
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for fn in os.listdir(inc):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(inc, fn)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(bd_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(bd.LIB_PATH)
+    syms = declared_symbols()
+    assert len(syms) > 25
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_status_strings_and_version():
+    L = bd.lib()
+    for code in range(0, -11, -1):
+        assert L.bd_status_string(code)
+    assert b"sm_100a" in L.bd_version()
+
+
+def test_no_gpu_means_error_not_fallback():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(bd.BeedrillError) as ei:
+        bd.Graph.rmat(8)
+    assert ei.value.status == -9  # BD_ERR_NODEV
+
+
+def test_algorithm_names_cover_reference_cli():
+    # hybrid_bfs_main.cc:228-245 accepts these four
+    for name in ("remote_writes", "migrating_threads", "remote_writes_hybrid", "beamer_hybrid"):
+        assert name in bd.ALGORITHMS
+    with pytest.raises(ValueError):
+        bd.HybridBFS.__init__(object.__new__(bd.HybridBFS), None, alg="bogus")
+
+
+def test_invalid_arguments_rejected_without_device():
+    L = bd.lib()
+    h = ctypes.c_void_p()
+    assert L.bd_graph_rmat(0, 16, 0.57, 0.19, 0.19, 0.05, 0, 0, ctypes.byref(h)) == -1
+    assert L.bd_graph_rmat(10, 16, 0.57, 0.19, 0.19, 0.05, 0, 7, ctypes.byref(h)) == -1
+    assert L.bd_bfs_create(None, None, ctypes.byref(h)) == -1
