@@ -811,6 +811,20 @@ struct bd_bfs {
 };
 
 namespace bd {
+
+bd_status bfs_install_policy(bd_bfs *b, const PolicyBlob *blob)
+{
+    BD_CUDA(cudaSetDevice(b->device));
+    if (!blob) {
+        cudaFree(b->policy);
+        b->policy = nullptr;
+        return BD_OK;
+    }
+    if (!b->policy) { BD_CUDA(cudaMalloc(&b->policy, sizeof(PolicyBlob))); }
+    BD_CUDA(cudaMemcpy(b->policy, blob, sizeof(PolicyBlob), cudaMemcpyHostToDevice));
+    return BD_OK;
+}
+
 namespace {
 
 BfsParams make_params(bd_bfs *b)

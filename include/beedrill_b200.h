@@ -170,6 +170,37 @@ bd_status bd_bfs_check(bd_bfs *b, int64_t source, int32_t *ok);
 bd_status bd_bfs_get_steps(bd_bfs *b, bd_step *steps, int64_t capacity, int64_t *count);
 bd_status bd_bfs_destroy(bd_bfs *b);
 
+/* ---- learned direction policy -------------------------------------------- */
+/* An fp32 MLP 8 -> 32 (ReLU) -> 32 (ReLU) -> 2 that picks the direction of
+ * every step in place of the alpha/beta rule (hybrid_bfs.cc:166-188).
+ * Parameter vector, BD_POLICY_PARAMS floats:
+ *   w1[32][8], b1[32], w2[32][32], b2[32], w3[2][32], b3[2].
+ * Features per step (raw, before standardisation with mean / inv_std):
+ *   log2(1+frontier vertices), log2(1+frontier degree sum m_f),
+ *   log2(1+unexplored degree sum m_u), level, log2(1+n), log2(1+m),
+ *   previous direction (0 top-down, 1 bottom-up),
+ *   log2(1+previous step time in microseconds).
+ * Output: logits (top-down, bottom-up).  The Beamer rule decides whenever
+ * |logit gap| < margin, and always when no policy is installed. */
+#define BD_POLICY_PARAMS 1410
+#define BD_POLICY_FEATURES 8
+/* Installs (or, with params == NULL, removes) the policy used by
+ * BD_ALG_LEARNED.  Host pointers; copied. */
+bd_status bd_bfs_set_policy(bd_bfs *b, const float *params, const float *mean,
+                            const float *inv_std, float margin);
+/* Device forward pass over n standardised feature rows (host buffers). */
+bd_status bd_policy_forward(const float *params, const float *x, int64_t n, float *logits);
+/* Weighted cross-entropy sum_i w_i CE(x_i, label_i) / sum_i w_i and its
+ * gradient (BD_POLICY_PARAMS floats), computed by the device kernels. */
+bd_status bd_policy_loss_grad(const float *params, const float *x, const int32_t *label,
+                              const float *weight, int64_t n, float *loss, float *grad);
+/* Full-batch Adam (beta1 0.9, beta2 0.999, eps 1e-8, L2 weight_decay) for
+ * `epochs` steps on the device; params is updated in place; loss_history
+ * (may be NULL) gets the loss before each step. */
+bd_status bd_policy_train(float *params, const float *x, const int32_t *label,
+                          const float *weight, int64_t n, int32_t epochs, float lr,
+                          float weight_decay, float *loss_history);
+
 #ifdef __cplusplus
 }
 #endif
