@@ -20,11 +20,13 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import POINTER, Structure, byref, c_char_p, c_double, c_int, c_int32, c_int64, c_uint32, c_uint64, c_void_p
+from ctypes import (POINTER, Structure, byref, c_char_p, c_double, c_float, c_int, c_int32, c_int64,
+                    c_uint32, c_uint64, c_void_p)
 
 import numpy as np
 
-__all__ = ["BeedrillError", "Graph", "HybridBFS", "Step", "ALGORITHMS", "lib", "LIB_PATH"]
+__all__ = ["BeedrillError", "Graph", "HybridBFS", "Step", "ALGORITHMS", "lib", "LIB_PATH",
+           "policy_forward", "policy_loss_grad", "policy_train"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libbeedrill_b200.so")
@@ -96,6 +98,7 @@ def lib() -> ctypes.CDLL:
         raise ImportError(f"{LIB_PATH} is missing: run `make` (or __graft_entry__.build())")
     L = ctypes.CDLL(LIB_PATH)
     i64p, u32p, i32p = POINTER(c_int64), POINTER(c_uint32), POINTER(c_int32)
+    f32p = POINTER(c_float)
     vpp = POINTER(c_void_p)
     sig = {
         "bd_status_string": (c_char_p, [c_int]),
@@ -132,6 +135,11 @@ def lib() -> ctypes.CDLL:
         "bd_bfs_check": (c_int, [c_void_p, c_int64, i32p]),
         "bd_bfs_get_steps": (c_int, [c_void_p, POINTER(Step), c_int64, i64p]),
         "bd_bfs_destroy": (c_int, [c_void_p]),
+        "bd_bfs_set_policy": (c_int, [c_void_p, f32p, f32p, f32p, c_float]),
+        "bd_policy_forward": (c_int, [f32p, f32p, c_int64, f32p]),
+        "bd_policy_loss_grad": (c_int, [f32p, f32p, i32p, f32p, c_int64, f32p, f32p]),
+        "bd_policy_train": (c_int, [f32p, f32p, i32p, f32p, c_int64, c_int32, c_float, c_float,
+                                    f32p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -385,6 +393,20 @@ class HybridBFS:
                 p = int(parent[p])
             print(line)
 
+    def set_policy(self, params, mean, inv_std, margin: float = 0.0) -> None:
+        """Install the learned direction policy used by alg="learned"
+        (params=None removes it; Beamer then decides)."""
+        if params is None:
+            _check(lib().bd_bfs_set_policy(self._h, None, None, None, 0.0), "set_policy")
+            return
+        p = np.ascontiguousarray(params, np.float32)
+        mu = np.ascontiguousarray(mean, np.float32)
+        isd = np.ascontiguousarray(inv_std, np.float32)
+        if p.size != 1410 or mu.size != 8 or isd.size != 8:
+            raise ValueError("policy shapes: 1410 params, 8 means, 8 inverse std devs")
+        _check(lib().bd_bfs_set_policy(self._h, _ptr(p, c_float), _ptr(mu, c_float),
+                                       _ptr(isd, c_float), margin), "set_policy")
+
     def close(self) -> None:
         if self._h is not None and self._h.value:
             lib().bd_bfs_destroy(self._h)
@@ -395,3 +417,46 @@ class HybridBFS:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# Learned-policy kernels (beedrill_b200/csrc/bd_policy.cu)
+# ---------------------------------------------------------------------------
+
+def policy_forward(params, x) -> np.ndarray:
+    """Device forward pass: logits (n, 2) of standardised features (n, 8)."""
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(x, np.float32).reshape(-1, 8)
+    out = np.empty((len(x), 2), np.float32)
+    _check(lib().bd_policy_forward(_ptr(p, c_float), _ptr(x, c_float), len(x), _ptr(out, c_float)),
+           "policy_forward")
+    return out
+
+
+def policy_loss_grad(params, x, label, weight):
+    """Device weighted cross-entropy and its gradient (1410 floats)."""
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(x, np.float32).reshape(-1, 8)
+    y = np.ascontiguousarray(label, np.int32)
+    w = np.ascontiguousarray(weight, np.float32)
+    loss = c_float()
+    grad = np.empty(1410, np.float32)
+    _check(lib().bd_policy_loss_grad(_ptr(p, c_float), _ptr(x, c_float), _ptr(y, c_int32),
+                                     _ptr(w, c_float), len(y), byref(loss), _ptr(grad, c_float)),
+           "policy_loss_grad")
+    return float(loss.value), grad
+
+
+def policy_train(params, x, label, weight, epochs: int, lr: float, weight_decay: float = 0.0):
+    """Full-batch Adam on the device; updates params in place and returns
+    the loss history."""
+    if not (isinstance(params, np.ndarray) and params.dtype == np.float32 and params.flags.c_contiguous):
+        raise TypeError("params must be a C-contiguous float32 array (updated in place)")
+    x = np.ascontiguousarray(x, np.float32).reshape(-1, 8)
+    y = np.ascontiguousarray(label, np.int32)
+    w = np.ascontiguousarray(weight, np.float32)
+    hist = np.empty(epochs, np.float32)
+    _check(lib().bd_policy_train(_ptr(params, c_float), _ptr(x, c_float), _ptr(y, c_int32),
+                                 _ptr(w, c_float), len(y), epochs, lr, weight_decay,
+                                 _ptr(hist, c_float)), "policy_train")
+    return hist

@@ -1271,3 +1271,4 @@ bd_status bd_bfs_destroy(bd_bfs *b)
 }
 
 }  // extern "C"
+

@@ -233,12 +233,6 @@ def regret(tables, dirs_fn) -> dict:
             "regret_ms": (cost - best) * 1e-6, "regret_frac": (cost - best) / best}
 
 
-def train(X, y, w, epochs=3000, lr=3e-3, weight_decay=1e-4, seed=0):
-    """Standardises the features and trains on the device; returns a Policy
-    (margin 0) and the loss history."""
-    from oracle_free_init import he_init  # noqa: F401  (placeholder, replaced below)
-
-
 def he_init(seed: int = 0) -> np.ndarray:
     rng = np.random.default_rng(seed)
     w1 = rng.normal(0, np.sqrt(2.0 / 8), (32, 8))
@@ -249,6 +243,8 @@ def he_init(seed: int = 0) -> np.ndarray:
 
 
 def fit(X, y, w, epochs=3000, lr=3e-3, weight_decay=1e-4, seed=0):
+    """Standardises the features and trains on the device; returns a Policy
+    (margin 0) and the loss history."""
     mean = X.mean(0).astype(np.float32)
     std = X.std(0).astype(np.float32)
     inv_std = np.where(std > 1e-6, 1.0 / np.maximum(std, 1e-6), 0.0).astype(np.float32)

@@ -1,0 +1,112 @@
+"""The learned direction policy.
+
+CPU: the float64 oracle's analytic gradient agrees with finite differences
+(this pins the oracle; the reference has no learned component to compare
+with).  GPU: the hand-written forward / backward / Adam kernels agree with the
+oracle; a BFS under the learned policy returns exactly the plain BFS's
+depths; and the trained network's regret on held-out graphs is below the
+Beamer rule's.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import policy_oracle as PO
+
+# fp32 device arithmetic against the float64 oracle
+RTOL = 2e-3
+ATOL = 2e-5
+
+
+def _problem(n=700, seed=0):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(0, 1, (n, 8))
+    y = (x[:, 0] + 0.5 * x[:, 2] - x[:, 6] > 0).astype(np.int64)
+    w = rng.uniform(0.1, 3.0, n)
+    theta = PO.init_params(seed + 1)
+    return theta, x, y, w
+
+
+def test_oracle_gradient_matches_finite_differences():
+    theta, x, y, w = _problem(60, 3)
+    _, g = PO.loss_grad(theta, x, y, w)
+    idx = list(range(0, PO.NUM_PARAMS, 37)) + [PO.NUM_PARAMS - 1, PO.NUM_PARAMS - 2]
+    fd = PO.finite_difference(theta, x, y, w, 1e-6, idx)
+    for i in idx:
+        assert abs(fd[i] - g[i]) <= 1e-6 + 1e-5 * abs(g[i]), i
+
+
+def test_oracle_adam_decreases_loss():
+    theta, x, y, w = _problem(200, 4)
+    _, losses = PO.adam(theta, lambda t: PO.loss_grad(t, x, y, w), 200, lr=1e-2)
+    assert losses[-1] < 0.5 * losses[0]
+
+
+@pytest.mark.gpu
+def test_device_forward_matches_oracle():
+    bd = pytest.importorskip("beedrill_b200")
+    theta, x, y, w = _problem()
+    z_ref, _ = PO.forward(theta, x)
+    z = bd.policy_forward(theta.astype(np.float32), x.astype(np.float32))
+    np.testing.assert_allclose(z, z_ref, rtol=RTOL, atol=1e-4)
+
+
+@pytest.mark.gpu
+def test_device_gradient_matches_oracle():
+    bd = pytest.importorskip("beedrill_b200")
+    theta, x, y, w = _problem()
+    loss_ref, g_ref = PO.loss_grad(theta, x, y, w)
+    loss, g = bd.policy_loss_grad(theta.astype(np.float32), x.astype(np.float32), y, w)
+    assert abs(loss - loss_ref) <= RTOL * abs(loss_ref)
+    scale = np.abs(g_ref).max()
+    np.testing.assert_allclose(g, g_ref, rtol=RTOL, atol=ATOL * max(scale, 1.0))
+
+
+@pytest.mark.gpu
+def test_device_adam_tracks_oracle():
+    bd = pytest.importorskip("beedrill_b200")
+    theta, x, y, w = _problem(300, 5)
+    steps, lr = 40, 5e-3
+    ref_theta, ref_losses = PO.adam(theta, lambda t: PO.loss_grad(t, x, y, w), steps, lr=lr)
+    p = theta.astype(np.float32).copy()
+    hist = bd.policy_train(p, x.astype(np.float32), y, w, steps, lr, 0.0)
+    np.testing.assert_allclose(hist, ref_losses, rtol=1e-2, atol=1e-4)
+    np.testing.assert_allclose(p, ref_theta, rtol=5e-2, atol=5e-3)
+
+
+@pytest.mark.gpu
+def test_learned_policy_does_not_change_results():
+    bd = pytest.importorskip("beedrill_b200")
+    from oracle import oracle as O
+    g = bd.Graph.rmat(15, seed=31)
+    off, adj = g.csr()
+    bfs = bd.HybridBFS(g, alg="learned")
+    # an arbitrary (untrained) network: decisions change, results must not
+    theta = PO.init_params(9).astype(np.float32)
+    bfs.set_policy(theta, np.zeros(8, np.float32), np.full(8, 0.3, np.float32), 0.0)
+    for root in g.pick_roots(2, 4):
+        root = int(root)
+        bfs.clear()
+        bfs.run(root)
+        assert np.array_equal(bfs.depths(), O.bfs_depth(off, adj, root))
+        assert O.check(off, adj, root, bfs.parents())
+
+
+@pytest.mark.gpu
+def test_trained_policy_beats_beamer_on_held_out_graphs():
+    bd = pytest.importorskip("beedrill_b200")
+    from beedrill_b200 import policy as P
+    if not os.path.exists(P.DEFAULT_PATH):
+        pytest.skip("no trained policy committed")
+    pol = P.Policy.load()
+    tables = []
+    for seed, scale, a in [(9101, 20, 0.57), (9102, 21, 0.50), (9103, 19, 0.62)]:
+        d = 0.05
+        g = bd.Graph.rmat(scale, 16, a, (1 - a - d) / 2, (1 - a - d) / 2, d, seed)
+        tables += P.measure_tables(g, g.pick_roots(seed, 4), repeats=2, with_beamer=False)
+        g.close()
+    rb = P.regret(tables, P.beamer_dirs)
+    rl = P.regret(tables, lambda t: P.policy_dirs(pol, t))
+    # the gain over the rule it replaces, on graphs it was not trained on
+    assert rl["cost_ms"] <= rb["cost_ms"], (rl, rb)
