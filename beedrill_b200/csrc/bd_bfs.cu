@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "bd_bfs_device.cuh"
@@ -1272,3 +1273,157 @@ bd_status bd_bfs_destroy(bd_bfs *b)
 
 }  // extern "C"
 
+// ---------------------------------------------------------------------------
+// Allocation-free entry point (bd_bfs_run_noalloc).
+//
+// For callers that must not allocate device memory while they run a BFS:
+// a service whose device memory is fully carved up in advance by its own
+// pool allocator (a cudaMalloc there fails or fragments the pool), or code
+// that cannot afford the device-wide synchronisation cudaMalloc / cudaFree
+// may cause.  The caller passes the CSR and the output arrays; every
+// temporary (control block, the two visited bitmaps, the frontier queues)
+// lives in one file-scope device array of fixed size, so graphs are limited
+// to BD_NOALLOC_MAX_VERTICES vertices.  Each GPU that loads this library
+// holds that array (about 4.9 MB) until the process exits.
+// ---------------------------------------------------------------------------
+namespace bd {
+namespace {
+
+constexpr int64_t kNaMaxVertices = BD_NOALLOC_MAX_VERTICES;
+constexpr int64_t kNaWords = kNaMaxVertices / 32;
+constexpr int64_t kNaLarge = 1 << 15;  // slots for large-degree frontier vertices
+constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kNaOffCtrl = 0;
+constexpr size_t kNaOffSource = align256(kNaOffCtrl + sizeof(Ctrl));
+constexpr size_t kNaOffVis = align256(kNaOffSource + sizeof(int64_t));
+constexpr size_t kNaOffQs = align256(kNaOffVis + 2 * sizeof(uint32_t) * kNaWords);
+constexpr size_t kNaOffQl = align256(kNaOffQs + 2 * sizeof(uint32_t) * kNaMaxVertices);
+constexpr size_t kNaOffQlb = align256(kNaOffQl + 2 * sizeof(uint32_t) * kNaLarge);
+constexpr size_t kNaBytes = align256(kNaOffQlb + 2 * sizeof(unsigned long long) * kNaLarge);
+
+// The scratch array.  Host code must not use this name as an address: it
+// gets the device address from cudaGetSymbolAddress (noalloc_scratch_base).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mutex;
+unsigned char *g_na_base[kNaMaxDevices] = {};
+int g_na_grid[kNaMaxDevices] = {};
+
+// Once per device, with that device current: the device address of the
+// scratch array and the co-resident grid size of the persistent kernel.
+bd_status noalloc_setup(int dev, unsigned char **base, int *grid)
+{
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_base[dev]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) { return cuda_fail(e, "cudaGetSymbolAddress", __FILE__, __LINE__); }
+        int per_sm = 0, sms = 0;
+        KernelChoice kc = pick_kernel(512);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)kc.fn, kc.block, 0);
+        if (e == cudaSuccess) { e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev); }
+        if (e != cudaSuccess) { return cuda_fail(e, "occupancy", __FILE__, __LINE__); }
+        if (per_sm < 1) { return BD_ERR_CUDA; }
+        g_na_grid[dev] = per_sm * sms;
+        g_na_base[dev] = static_cast<unsigned char *>(ptr);
+    }
+    *base = g_na_base[dev];
+    *grid = g_na_grid[dev];
+    return BD_OK;
+}
+
+// depth = -1; vis[0] = degree-zero and padding bits; the source id.
+__global__ void noalloc_prepare_kernel(const int64_t *off, int64_t n, int32_t *depth,
+                                       uint32_t *vis0, int64_t source, int64_t *source_slot)
+{
+    const int64_t words = (n + 31) / 32;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (int64_t v = t; v < n; v += stride) { depth[v] = -1; }
+    for (int64_t w = t; w < words; w += stride) {
+        uint32_t b = 0;
+        for (int k = 0; k < 32; ++k) {
+            const int64_t v = w * 32 + k;
+            if (v >= n || off[v + 1] == off[v]) { b |= 1u << k; }
+        }
+        vis0[w] = b;
+    }
+    if (t == 0) { *source_slot = source; }
+}
+
+}  // namespace
+}  // namespace bd
+
+extern "C" bd_status bd_bfs_run_noalloc(const int64_t *d_offsets, const uint32_t *d_adjacency,
+                                        int64_t num_vertices, int64_t num_arcs, int64_t source,
+                                        int64_t alpha, int64_t beta, int32_t *d_depth,
+                                        int64_t *d_parent, void *stream,
+                                        int64_t *traversed_edges)
+{
+    using namespace bd;
+    if (!d_offsets || (!d_adjacency && num_arcs) || !d_depth || !d_parent || num_vertices <= 0 ||
+        num_arcs < 0 || alpha <= 0 || beta <= 0) {
+        return BD_ERR_INVALID;
+    }
+    if (num_vertices > kNaMaxVertices || num_arcs > ((int64_t)1 << 34)) { return BD_ERR_LIMIT; }
+    if (source < 0 || source >= num_vertices) { return BD_ERR_RANGE; }
+    int dev = 0, major = 0;
+    BD_CUDA(cudaGetDevice(&dev));
+    BD_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major != 10 || dev >= kNaMaxDevices) { return BD_ERR_NODEV; }
+    unsigned char *base = nullptr;
+    int grid = 0;
+    BD_TRY(noalloc_setup(dev, &base, &grid));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    BfsParams p{};
+    p.off = d_offsets;
+    p.adj = d_adjacency;
+    p.n = num_vertices;
+    p.m = num_arcs / 2;
+    p.depth = d_depth;
+    p.parent = d_parent;
+    p.words = bitmap_words(num_vertices);
+    Ctrl *ctrl = reinterpret_cast<Ctrl *>(base + kNaOffCtrl);
+    int64_t *source_slot = reinterpret_cast<int64_t *>(base + kNaOffSource);
+    for (int i = 0; i < 2; ++i) {
+        p.vis[i] = reinterpret_cast<uint32_t *>(base + kNaOffVis) + i * kNaWords;
+        p.qs[i] = reinterpret_cast<uint32_t *>(base + kNaOffQs) + i * kNaMaxVertices;
+        p.ql[i] = reinterpret_cast<uint32_t *>(base + kNaOffQl) + i * kNaLarge;
+        p.qlb[i] = reinterpret_cast<unsigned long long *>(base + kNaOffQlb) + i * kNaLarge;
+    }
+    p.ctrl = ctrl;
+    p.rec = nullptr;
+    p.rec_cap = 0;
+    p.alg = BD_ALG_BEAMER;
+    p.alpha = alpha;
+    p.beta = beta;
+    // Large-degree slots: at most num_arcs / large_deg vertices qualify.
+    p.large_deg = (uint32_t)std::max<int64_t>(1024, num_arcs / kNaLarge + 1);
+    p.chunk = 1024;
+    p.bu_prefix = 32;
+    p.spin_limit = kDefaultSpin;
+    p.expected_ctas = (unsigned)grid;
+    p.policy = nullptr;
+
+    // The control block, source slot and vis[0] are rewritten here; the
+    // queues and vis[1] are written before they are read within a run.
+    noalloc_prepare_kernel<<<grid_for(std::max<int64_t>(num_vertices, 1)), 256, 0, s>>>(
+        d_offsets, num_vertices, d_depth, p.vis[0], source, source_slot);
+    BD_CUDA(cudaGetLastError());
+    init_sources_kernel<<<1, 32, 0, s>>>(p, source_slot, 1, 0);
+    BD_CUDA(cudaGetLastError());
+    KernelChoice kc = pick_kernel(512);
+    void *args[] = {&p};
+    BD_CUDA(cudaLaunchCooperativeKernel((const void *)kc.fn, dim3(grid), dim3(kc.block), args, 0, s));
+    finalize_parents_kernel<<<grid_for(num_vertices), 256, 0, s>>>(d_offsets, num_vertices, d_depth,
+                                                                   d_parent);
+    BD_CUDA(cudaGetLastError());
+    Ctrl host{};
+    BD_CUDA(cudaMemcpyAsync(&host, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+    BD_CUDA(cudaStreamSynchronize(s));
+    if (host.error) { return (bd_status)host.error; }
+    if (traversed_edges) { *traversed_edges = host.visited_degsum / 2; }
+    return BD_OK;
+}

@@ -170,6 +170,36 @@ bd_status bd_bfs_check(bd_bfs *b, int64_t source, int32_t *ok);
 bd_status bd_bfs_get_steps(bd_bfs *b, bd_step *steps, int64_t capacity, int64_t *count);
 bd_status bd_bfs_destroy(bd_bfs *b);
 
+/* Allocation-free BFS.  No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory on this call path: a
+ * process whose device memory is reserved up front by its own pool allocator
+ * (a cudaMalloc there fails or fragments the pool), or code that cannot
+ * afford the device-wide synchronisation cudaMalloc / cudaFree may cause.
+ * One Beamer BFS (alpha, beta) from `source` over a CSR already in device
+ * memory (d_offsets: num_vertices+1 int64, d_adjacency: num_arcs uint32);
+ * writes d_depth (int32, -1 unreached) and d_parent (reference encoding)
+ * in caller-owned device memory, on `stream` (a cudaStream_t, NULL for the
+ * default stream), and returns after the stream has finished.
+ * traversed_edges (host, may be NULL) gets count_num_traversed_edges().
+ *
+ * All temporaries live in one fixed device array inside the library, so:
+ *   - num_vertices must not exceed BD_NOALLOC_MAX_VERTICES (else
+ *     BD_ERR_LIMIT, nothing launched);
+ *   - the first call on a device looks the array up on that device
+ *     (cudaGetSymbolAddress); make that first call before any stream
+ *     capture;
+ *   - every call shares the array: calls that overlap on the GPU (other
+ *     streams, other host threads) race and corrupt each other.  Serialise
+ *     them.
+ * Nothing is allocated or freed; the call uses the device current on the
+ * calling thread. */
+#define BD_NOALLOC_MAX_VERTICES 524288
+bd_status bd_bfs_run_noalloc(const int64_t *d_offsets, const uint32_t *d_adjacency,
+                             int64_t num_vertices, int64_t num_arcs, int64_t source,
+                             int64_t alpha, int64_t beta, int32_t *d_depth, int64_t *d_parent,
+                             void *stream, int64_t *traversed_edges);
+
 /* ---- learned direction policy -------------------------------------------- */
 /* An fp32 MLP 8 -> 32 (ReLU) -> 32 (ReLU) -> 2 that picks the direction of
  * every step in place of the alpha/beta rule (hybrid_bfs.cc:166-188).
