@@ -25,7 +25,8 @@ from ctypes import (POINTER, Structure, byref, c_char_p, c_double, c_float, c_in
 
 import numpy as np
 
-__all__ = ["BeedrillError", "Graph", "HybridBFS", "Step", "ALGORITHMS", "lib", "LIB_PATH",
+__all__ = ["BeedrillError", "Graph", "HybridBFS", "BatchedBFS", "Step", "ALGORITHMS", "lib", "LIB_PATH",
+           "tuned_options",
            "policy_forward", "policy_loss_grad", "policy_train"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -37,7 +38,7 @@ STATUS_NAMES = {
     -5: "BD_ERR_CUDA", -6: "BD_ERR_TIMEOUT", -7: "BD_ERR_RANGE", -8: "BD_ERR_STATE",
     -9: "BD_ERR_NODEV", -10: "BD_ERR_LIMIT",
 }
-ORDER_INSERTION, ORDER_SORTED = 0, 1
+ORDER_INSERTION, ORDER_SORTED, ORDER_DEGREE = 0, 1, 2
 ALG_BEAMER, ALG_TOP_DOWN, ALG_BOTTOM_UP, ALG_LEARNED = 0, 1, 2, 3
 
 # The reference's --algorithm values (hybrid_bfs_main.cc:228-245) plus the
@@ -65,7 +66,7 @@ class BfsOpts(Structure):
         ("alg", c_int32), ("min_parent", c_int32), ("alpha", c_int64), ("beta", c_int64),
         ("block_size", c_int32), ("large_degree", c_int32), ("chunk_edges", c_int32),
         ("bu_prefix", c_int32), ("spin_limit", c_int64), ("test_extra_ctas", c_int32),
-        ("reserved", c_int32),
+        ("bu_words", c_int32), ("bu_sparse_words", c_int32), ("reserved", c_int32),
     ]
 
 
@@ -79,6 +80,14 @@ class Step(Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class MsBfsOpts(Structure):
+    _fields_ = [
+        ("alpha", c_int64), ("force_dir", c_int32), ("block_size", c_int32),
+        ("large_degree", c_int32), ("chunk_edges", c_int32), ("pull_prefix", c_int32),
+        ("use_graph", c_int32), ("spin_limit", c_int64),
+    ]
+
+
 class RunStats(Structure):
     _fields_ = [
         ("ms", c_double), ("num_steps", c_int64), ("reached", c_int64),
@@ -87,6 +96,17 @@ class RunStats(Structure):
 
 
 _lib = None
+TUNING_PATH = os.path.join(HERE, "tuning", "b200.json")
+
+
+def tuned_options(kind: str) -> dict:
+    """Launch parameters picked by beedrill_b200.autotune for `kind`
+    ("single" or "batched"), or {} when no tuning file exists."""
+    if not os.path.exists(TUNING_PATH):
+        return {}
+    import json
+    with open(TUNING_PATH) as f:
+        return dict(json.load(f).get(kind, {}))
 
 
 def lib() -> ctypes.CDLL:
@@ -110,6 +130,7 @@ def lib() -> ctypes.CDLL:
         "bd_graph_rmat": (c_int, [c_int32, c_int64, c_double, c_double, c_double, c_double,
                                   c_uint64, c_int32, vpp]),
         "bd_graph_concat": (c_int, [vpp, c_int64, vpp, i64p]),
+        "bd_graph_grid": (c_int, [c_int64, c_int64, c_double, c_uint64, c_int32, vpp]),
         "bd_graph_info": (c_int, [c_void_p, i64p, i64p]),
         "bd_graph_copy_csr": (c_int, [c_void_p, i64p, u32p]),
         "bd_graph_copy_edges": (c_int, [c_void_p, i64p, i64p]),
@@ -135,7 +156,15 @@ def lib() -> ctypes.CDLL:
         "bd_bfs_check": (c_int, [c_void_p, c_int64, i32p]),
         "bd_bfs_get_steps": (c_int, [c_void_p, POINTER(Step), c_int64, i64p]),
         "bd_bfs_destroy": (c_int, [c_void_p]),
-        "bd_bfs_set_policy": (c_int, [c_void_p, f32p, f32p, f32p, c_float]),
+        "bd_bfs_set_policy": (c_int, [c_void_p, f32p, f32p, f32p, f32p, f32p, c_float]),
+        "bd_msbfs_default_opts": (None, [POINTER(MsBfsOpts)]),
+        "bd_msbfs_create": (c_int, [c_void_p, c_int32, POINTER(MsBfsOpts), vpp]),
+        "bd_msbfs_run": (c_int, [c_void_p, i64p, c_int32, POINTER(RunStats)]),
+        "bd_msbfs_get_depths": (c_int, [c_void_p, c_int32, i32p]),
+        "bd_msbfs_get_parents": (c_int, [c_void_p, c_int32, i64p]),
+        "bd_msbfs_count_traversed_edges": (c_int, [c_void_p, c_int32, i64p, i64p]),
+        "bd_msbfs_get_steps": (c_int, [c_void_p, POINTER(Step), c_int64, i64p]),
+        "bd_msbfs_destroy": (c_int, [c_void_p]),
         "bd_policy_forward": (c_int, [f32p, f32p, c_int64, f32p]),
         "bd_policy_loss_grad": (c_int, [f32p, f32p, i32p, f32p, c_int64, f32p, f32p]),
         "bd_policy_train": (c_int, [f32p, f32p, i32p, f32p, c_int64, c_int32, c_float, c_float,
@@ -208,6 +237,14 @@ class Graph:
         return cls(h)
 
     @classmethod
+    def grid(cls, rows: int, cols: int, delete_frac: float = 0.01, seed: int = 0,
+             order: int = ORDER_INSERTION) -> "Graph":
+        h = c_void_p()
+        _check(lib().bd_graph_grid(rows, cols, delete_frac, seed, order, byref(h)),
+               f"grid({rows}x{cols})")
+        return cls(h)
+
+    @classmethod
     def concat(cls, graphs) -> tuple["Graph", np.ndarray]:
         arr = (c_void_p * len(graphs))(*[g._h.value for g in graphs])
         base = np.zeros(len(graphs) + 1, np.int64)
@@ -273,9 +310,18 @@ class HybridBFS:
     def __init__(self, graph: Graph, alg: str = "beamer_hybrid", alpha: int = 15,
                  beta: int = 18, min_parent: bool = False, block_size: int = 0,
                  large_degree: int = 0, chunk_edges: int = 0, bu_prefix: int = 0,
-                 spin_limit: int = 0, test_extra_ctas: int = 0):
+                 spin_limit: int = 0, test_extra_ctas: int = 0, bu_words: int = 0,
+                 bu_sparse_words: int = 0, tuned: bool = True):
         if alg not in ALGORITHMS:
             raise ValueError(f"Algorithm '{alg}' not implemented!")
+        if tuned:
+            t = tuned_options("single")
+            block_size = block_size or t.get("block_size", 0)
+            large_degree = large_degree or t.get("large_degree", 0)
+            chunk_edges = chunk_edges or t.get("chunk_edges", 0)
+            bu_prefix = bu_prefix or t.get("bu_prefix", 0)
+            bu_words = bu_words or t.get("bu_words", 0)
+            bu_sparse_words = bu_sparse_words or t.get("bu_sparse_words", 0)
         self.graph = graph  # keeps the graph alive
         o = BfsOpts()
         lib().bd_bfs_default_opts(byref(o))
@@ -284,6 +330,8 @@ class HybridBFS:
         o.min_parent = int(bool(min_parent))
         o.block_size, o.large_degree, o.chunk_edges = block_size, large_degree, chunk_edges
         o.bu_prefix, o.spin_limit, o.test_extra_ctas = bu_prefix, spin_limit, test_extra_ctas
+        o.bu_words = bu_words
+        o.bu_sparse_words = bu_sparse_words
         self.alg = alg
         self.alpha, self.beta = alpha, beta
         self._h = c_void_p()
@@ -393,23 +441,119 @@ class HybridBFS:
                 p = int(parent[p])
             print(line)
 
-    def set_policy(self, params, mean, inv_std, margin: float = 0.0) -> None:
+    def set_policy(self, params, mean, inv_std, margin: float = 0.0, lo=None, hi=None) -> None:
         """Install the learned direction policy used by alg="learned"
-        (params=None removes it; Beamer then decides)."""
+        (params=None removes it; Beamer then decides).  lo / hi bound the raw
+        features the policy is trusted on (None: no bound)."""
         if params is None:
-            _check(lib().bd_bfs_set_policy(self._h, None, None, None, 0.0), "set_policy")
+            _check(lib().bd_bfs_set_policy(self._h, None, None, None, None, None, 0.0),
+                   "set_policy")
             return
+        lo_p = hi_p = None
+        if lo is not None:
+            lo_a = np.ascontiguousarray(lo, np.float32)
+            hi_a = np.ascontiguousarray(hi, np.float32)
+            lo_p, hi_p = _ptr(lo_a, c_float), _ptr(hi_a, c_float)
         p = np.ascontiguousarray(params, np.float32)
         mu = np.ascontiguousarray(mean, np.float32)
         isd = np.ascontiguousarray(inv_std, np.float32)
         if p.size != 1410 or mu.size != 8 or isd.size != 8:
             raise ValueError("policy shapes: 1410 params, 8 means, 8 inverse std devs")
         _check(lib().bd_bfs_set_policy(self._h, _ptr(p, c_float), _ptr(mu, c_float),
-                                       _ptr(isd, c_float), margin), "set_policy")
+                                       _ptr(isd, c_float), lo_p, hi_p, margin), "set_policy")
 
     def close(self) -> None:
         if self._h is not None and self._h.value:
             lib().bd_bfs_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchedBFS:
+    """Many BFSs per pass over the graph: groups of up to 64 roots, one bit
+    lane per root, all groups of a call replayed as one captured CUDA graph.
+    Per root the results equal HybridBFS's (depths, parents, m_c)."""
+
+    def __init__(self, graph: Graph, max_roots: int = 64, alpha: int = 0, force_dir: int = -1,
+                 use_graph: bool = True, block_size: int = 0, large_degree: int = 0,
+                 chunk_edges: int = 0, pull_prefix: int = 0, spin_limit: int = 0,
+                 tuned: bool = True):
+        if tuned:
+            t = tuned_options("batched")
+            alpha = alpha or t.get("alpha", 0)
+            block_size = block_size or t.get("block_size", 0)
+            large_degree = large_degree or t.get("large_degree", 0)
+            chunk_edges = chunk_edges or t.get("chunk_edges", 0)
+            pull_prefix = pull_prefix or t.get("pull_prefix", 0)
+        self.graph = graph
+        o = MsBfsOpts()
+        lib().bd_msbfs_default_opts(byref(o))
+        if alpha:
+            o.alpha = alpha
+        o.force_dir = force_dir
+        o.use_graph = int(bool(use_graph))
+        o.block_size, o.large_degree, o.chunk_edges = block_size, large_degree, chunk_edges
+        o.pull_prefix, o.spin_limit = pull_prefix, spin_limit
+        self.max_roots = max_roots
+        self._h = c_void_p()
+        _check(lib().bd_msbfs_create(graph._h, max_roots, byref(o), byref(self._h)), "msbfs")
+        self.last_stats = RunStats()
+
+    def run(self, sources) -> RunStats:
+        src = np.ascontiguousarray(sources, np.int64)
+        _check(lib().bd_msbfs_run(self._h, _ptr(src, c_int64), len(src), byref(self.last_stats)),
+               "msbfs run")
+        self.count = len(src)
+        return self.last_stats
+
+    def depths(self, i: int) -> np.ndarray:
+        d = np.empty(self.graph.num_vertices(), np.int32)
+        _check(lib().bd_msbfs_get_depths(self._h, i, _ptr(d, c_int32)), "msbfs depths")
+        return d
+
+    def parents(self, i: int) -> np.ndarray:
+        p = np.empty(self.graph.num_vertices(), np.int64)
+        _check(lib().bd_msbfs_get_parents(self._h, i, _ptr(p, c_int64)), "msbfs parents")
+        return p
+
+    def count_num_traversed_edges(self, i: int) -> int:
+        e = c_int64()
+        _check(lib().bd_msbfs_count_traversed_edges(self._h, i, byref(e), None), "msbfs count")
+        return e.value
+
+    def reached(self, i: int) -> int:
+        r = c_int64()
+        _check(lib().bd_msbfs_count_traversed_edges(self._h, i, None, byref(r)), "msbfs count")
+        return r.value
+
+    def counts(self):
+        """(m_c, n_c) arrays over the roots of the last run."""
+        m = np.empty(self.count, np.int64)
+        n = np.empty(self.count, np.int64)
+        for i in range(self.count):
+            e, r = c_int64(), c_int64()
+            _check(lib().bd_msbfs_count_traversed_edges(self._h, i, byref(e), byref(r)), "count")
+            m[i], n[i] = e.value, r.value
+        return m, n
+
+    def steps(self) -> list[dict]:
+        count = c_int64()
+        _check(lib().bd_msbfs_get_steps(self._h, None, 0, byref(count)), "steps")
+        buf = (Step * max(count.value, 1))()
+        _check(lib().bd_msbfs_get_steps(self._h, buf, count.value, byref(count)), "steps")
+        return [buf[i].as_dict() for i in range(count.value)]
+
+    def directions(self) -> str:
+        return "".join("B" if s["dir"] else "T" for s in self.steps())
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            lib().bd_msbfs_destroy(self._h)
         self._h = None
 
     def __del__(self):

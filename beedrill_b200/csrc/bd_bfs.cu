@@ -94,6 +94,7 @@ struct StepView {
     int vis_cur;
     int q_cur;
     int step;
+    int bu_sparse;
     long long f_small;
     long long f_large;
     long long f_chunks;
@@ -104,6 +105,7 @@ __device__ __forceinline__ StepView read_view(const Ctrl *c)
     const volatile Ctrl *vc = c;
     StepView v;
     v.dir = vc->dir;
+    v.bu_sparse = vc->bu_sparse;
     v.level = vc->level;
     v.vis_cur = vc->vis_cur;
     v.q_cur = vc->q_cur;
@@ -114,58 +116,66 @@ __device__ __forceinline__ StepView read_view(const Ctrl *c)
     return v;
 }
 
-// Warp-collective: appends the lanes' newly discovered vertices (has) to the
-// next frontier, binned by degree.  Small vertices get one slot each in qs;
-// large ones get a slot in ql plus a contiguous range of chunk ids.
-__device__ __forceinline__ void warp_append(const BfsParams &p, Acc *acc, int qout, bool has,
-                                            uint32_t v, int64_t deg, Local &loc)
-{
-    if (has) {
-        loc.found += 1;
-        loc.degsum += (unsigned long long)deg;
-    }
-    const int lane = lane_id();
-    const bool large = has && deg >= (int64_t)p.large_deg;
-    const unsigned sm = __ballot_sync(kFull, has && !large);
-    if (sm) {
-        const int leader = __ffs(sm) - 1;
-        unsigned long long base = 0;
-        if (lane == leader) { base = atomicAdd(&acc->small_cnt, (unsigned long long)__popc(sm)); }
-        base = __shfl_sync(kFull, base, leader);
-        if (has && !large) { p.qs[qout][base + __popc(sm & lanemask_lt())] = v; }
-    }
-    const unsigned lm = __ballot_sync(kFull, large);
-    if (lm) {
-        const unsigned long long nch =
-            large ? (unsigned long long)((deg + p.chunk - 1) / p.chunk) : 0ull;
-        const unsigned long long incl = warp_incl_scan(nch);
-        const unsigned long long total = __shfl_sync(kFull, incl, 31);
-        const int leader = __ffs(lm) - 1;
-        unsigned long long old = 0;
-        if (lane == leader) {
-            old = atomicAdd(&acc->large_packed,
-                            ((unsigned long long)__popc(lm) << kLargeShift) | total);
-        }
-        old = __shfl_sync(kFull, old, leader);
-        if (large) {
-            const unsigned long long pos = (old >> kLargeShift) + __popc(lm & lanemask_lt());
-            p.ql[qout][pos] = v;
-            p.qlb[qout][pos] = (old & kChunkMask) + incl - nch;
-        }
-    }
-}
+// Visited-bit lookups.  A plain (L1-cacheable) load is correct here: the
+// bitmap a bottom-up step reads is not written during that step, and every
+// CTA passes the grid barrier's acquire before the step, after which weak
+// loads observe all writes made before the barrier (PTX memory model).
+__device__ __forceinline__ uint32_t ld_bits(const uint32_t *p) { return *p; }
 
-// Top-down claim (hybrid_bfs.cc:83-96): visited-bit filter, then atomicCAS
-// on the depth word decides the single winner, which writes the parent.
-__device__ __forceinline__ bool td_claim(const BfsParams &p, uint32_t *vis, uint32_t v,
-                                         uint32_t u, int new_level)
+// Warp-collective append of up to K discoveries per lane with one atomic
+// for all the small-degree ones.
+template <int K>
+__device__ __forceinline__ void warp_append_k(const BfsParams &p, Acc *acc, int qout,
+                                              const bool (&has)[K], const uint32_t (&v)[K],
+                                              const int64_t (&deg)[K], Local &loc)
 {
-    const uint32_t w = __ldcg(&vis[v >> 5]);
-    if ((w >> (v & 31)) & 1u) { return false; }
-    if (atomicCAS(&p.depth[v], -1, new_level) != -1) { return false; }
-    p.parent[v] = (int64_t)u;
-    atomicOr(&vis[v >> 5], 1u << (v & 31));
-    return true;
+    const int lane = lane_id();
+    unsigned sm[K];
+    bool large[K];
+    unsigned total = 0, any_large = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (has[k]) {
+            loc.found += 1;
+            loc.degsum += (unsigned long long)deg[k];
+        }
+        large[k] = has[k] && deg[k] >= (int64_t)p.large_deg;
+        sm[k] = __ballot_sync(kFull, has[k] && !large[k]);
+        total += __popc(sm[k]);
+        any_large |= __ballot_sync(kFull, large[k]);
+    }
+    if (total) {
+        unsigned long long base = 0;
+        if (lane == 0) { base = atomicAdd(&acc->small_cnt, (unsigned long long)total); }
+        base = __shfl_sync(kFull, base, 0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (has[k] && !large[k]) { p.qs[qout][base + __popc(sm[k] & lanemask_lt())] = v[k]; }
+            base += __popc(sm[k]);
+        }
+    }
+    if (any_large) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const unsigned lm = __ballot_sync(kFull, large[k]);
+            if (!lm) { continue; }
+            const unsigned long long nch =
+                large[k] ? (unsigned long long)((deg[k] + p.chunk - 1) / p.chunk) : 0ull;
+            const unsigned long long incl = warp_incl_scan(nch);
+            const unsigned long long tot = __shfl_sync(kFull, incl, 31);
+            unsigned long long old = 0;
+            if (lane == 0) {
+                old = atomicAdd(&acc->large_packed,
+                                ((unsigned long long)__popc(lm) << kLargeShift) | tot);
+            }
+            old = __shfl_sync(kFull, old, 0);
+            if (large[k]) {
+                const unsigned long long pos = (old >> kLargeShift) + __popc(lm & lanemask_lt());
+                p.ql[qout][pos] = v[k];
+                p.qlb[qout][pos] = (old & kChunkMask) + incl - nch;
+            }
+        }
+    }
 }
 
 __device__ __forceinline__ int64_t degree_of(const BfsParams &p, uint32_t v)
@@ -175,6 +185,39 @@ __device__ __forceinline__ int64_t degree_of(const BfsParams &p, uint32_t v)
 
 constexpr int kILP = 4;
 
+// Top-down claims of a batch of kILP neighbours per lane (hybrid_bfs.cc:83-96):
+// visited-bit filter, then atomicCAS on the depth word decides the single
+// winner, which writes the parent, sets the visited bit and joins the next
+// frontier.  Every stage issues its kILP memory operations back to back.
+__device__ __forceinline__ void td_claim_batch(const BfsParams &p, Acc *acc, uint32_t *vis,
+                                               int qout, int new_level, const bool (&ok)[kILP],
+                                               const uint32_t (&v)[kILP],
+                                               const uint32_t (&src)[kILP], Local &loc)
+{
+    uint32_t w[kILP];
+#pragma unroll
+    for (int i = 0; i < kILP; ++i) { w[i] = ok[i] ? __ldcg(&vis[v[i] >> 5]) : 0xFFFFFFFFu; }
+    int old[kILP];
+#pragma unroll
+    for (int i = 0; i < kILP; ++i) {
+        const bool cand = ok[i] && !((w[i] >> (v[i] & 31)) & 1u);
+        old[i] = cand ? atomicCAS(&p.depth[v[i]], -1, new_level) : 0;
+    }
+    bool won[kILP];
+    int64_t deg[kILP];
+#pragma unroll
+    for (int i = 0; i < kILP; ++i) {
+        won[i] = ok[i] && !((w[i] >> (v[i] & 31)) & 1u) && old[i] == -1;
+        deg[i] = 0;
+        if (won[i]) {
+            p.parent[v[i]] = (int64_t)src[i];
+            atomicOr(&vis[v[i] >> 5], 1u << (v[i] & 31));
+            deg[i] = degree_of(p, v[i]);
+        }
+    }
+    warp_append_k<kILP>(p, acc, qout, won, v, deg, loc);
+}
+
 // Processes arcs [b, e) of vertex u with all 32 lanes (coalesced reads).
 __device__ __forceinline__ void td_edges_warp(const BfsParams &p, Acc *acc, uint32_t *vis,
                                               int qout, int new_level, uint32_t u, int64_t b,
@@ -182,20 +225,16 @@ __device__ __forceinline__ void td_edges_warp(const BfsParams &p, Acc *acc, uint
 {
     const int lane = lane_id();
     for (int64_t base = b; base < e; base += 32 * kILP) {
-        uint32_t v[kILP];
+        uint32_t v[kILP], src[kILP];
         bool ok[kILP];
 #pragma unroll
         for (int i = 0; i < kILP; ++i) {
             const int64_t k = base + i * 32 + lane;
             ok[i] = k < e;
             v[i] = ok[i] ? __ldg(&p.adj[k]) : 0u;
+            src[i] = u;
         }
-#pragma unroll
-        for (int i = 0; i < kILP; ++i) {
-            bool c = ok[i] && td_claim(p, vis, v[i], u, new_level);
-            int64_t deg = c ? degree_of(p, v[i]) : 0;
-            warp_append(p, acc, qout, c, v[i], deg, loc);
-        }
+        td_claim_batch(p, acc, vis, qout, new_level, ok, v, src, loc);
     }
 }
 
@@ -233,20 +272,38 @@ __device__ void td_step(const BfsParams &p, const StepView &sv, SharedState<BLOC
     Acc *acc = &p.ctrl->acc[sv.step & 1];
     const int new_level = sv.level + 1;
 
-    // Phase A: chunks of large-degree frontier vertices.
+    // Phase A: chunks of large-degree frontier vertices.  Warp gw takes a
+    // contiguous range of chunk ids, so every warp gets the same number of
+    // edges (within one chunk); one binary search finds the range's first
+    // vertex, then the walk moves forward.
     const long long nl = sv.f_large;
-    for (long long c = gw; c < sv.f_chunks; c += nw) {
-        long long lo = 0, hi = nl - 1;  // last i with qlb[i] <= c
-        while (lo < hi) {
-            long long mid = (lo + hi + 1) >> 1;
-            if ((long long)__ldcg(&p.qlb[qin][mid]) <= c) { lo = mid; } else { hi = mid - 1; }
+    const long long nch = sv.f_chunks;
+    if (nch > 0) {
+        const long long per = (nch + nw - 1) / nw;
+        const long long c0 = gw * per;
+        const long long c1 = min(nch, c0 + per);
+        if (c0 < c1) {
+            long long lo = 0, hi = nl - 1;  // last i with qlb[i] <= c0
+            while (lo < hi) {
+                long long mid = (lo + hi + 1) >> 1;
+                if ((long long)__ldcg(&p.qlb[qin][mid]) <= c0) { lo = mid; } else { hi = mid - 1; }
+            }
+            long long i = lo;
+            long long ibase = (long long)__ldcg(&p.qlb[qin][i]);
+            long long inext = i + 1 < nl ? (long long)__ldcg(&p.qlb[qin][i + 1]) : nch;
+            for (long long c = c0; c < c1; ++c) {
+                while (c >= inext) {
+                    ++i;
+                    ibase = inext;
+                    inext = i + 1 < nl ? (long long)__ldcg(&p.qlb[qin][i + 1]) : nch;
+                }
+                const uint32_t u = __ldcg(&p.ql[qin][i]);
+                const int64_t ub = __ldg(&p.off[u]), ue = __ldg(&p.off[u + 1]);
+                const int64_t b = ub + (c - ibase) * (int64_t)p.chunk;
+                const int64_t e = min(ue, b + (int64_t)p.chunk);
+                td_edges_warp(p, acc, vis, qout, new_level, u, b, e, loc);
+            }
         }
-        const uint32_t u = __ldcg(&p.ql[qin][lo]);
-        const long long j = c - (long long)__ldcg(&p.qlb[qin][lo]);
-        const int64_t ub = __ldg(&p.off[u]), ue = __ldg(&p.off[u + 1]);
-        const int64_t b = ub + j * (int64_t)p.chunk;
-        const int64_t e = min(ue, b + (int64_t)p.chunk);
-        td_edges_warp(p, acc, vis, qout, new_level, u, b, e, loc);
     }
 
     // Phase B: small-degree frontier vertices, 32 per warp; their arcs are
@@ -288,25 +345,23 @@ __device__ void td_step(const BfsParams &p, const StepView &sv, SharedState<BLOC
                     v[i] = __ldg(&p.adj[ws.beg[lo] + (e - excl)]);
                 }
             }
-#pragma unroll
-            for (int i = 0; i < kILP; ++i) {
-                bool c = ok[i] && td_claim(p, vis, v[i], src[i], new_level);
-                int64_t d = c ? degree_of(p, v[i]) : 0;
-                warp_append(p, acc, qout, c, v[i], d, loc);
-            }
+            td_claim_batch(p, acc, vis, qout, new_level, ok, v, src, loc);
         }
         __syncwarp();
     }
 }
 
-// Bottom-up step (hybrid_bfs.cc:111-143): each warp owns one bitmap word
-// (32 vertices).  Unvisited lanes scan their own neighbour lists (first
-// bu_prefix arcs, 4 loads in flight); lists longer than that are finished by
-// the whole warp, 32 arcs per ballot, stopping at the first hit.  Reads only
-// the frozen bitmap vis[cur]; writes whole words of vis[cur^1].
-template <int BLOCK>
+// Bottom-up step (hybrid_bfs.cc:111-143).  A warp works on K consecutive
+// bitmap words (32 K vertices) at a time, so K independent load chains are
+// in flight per lane.  Unvisited lanes scan their own neighbour lists (the
+// first bu_prefix arcs, P arcs per word per round), stopping at the first
+// visited neighbour; lists longer than that are finished by the whole warp,
+// 32 arcs per ballot (warp-ballot early exit).  Reads only the frozen bitmap
+// vis[cur]; writes whole words of vis[cur^1].
+template <int BLOCK, int K>
 __device__ void bu_step(const BfsParams &p, const StepView &sv, Local &loc)
 {
+    constexpr int P = K >= 4 ? 2 : 4;
     const int lane = lane_id();
     const int warp = threadIdx.x >> 5;
     const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
@@ -317,71 +372,248 @@ __device__ void bu_step(const BfsParams &p, const StepView &sv, Local &loc)
     Acc *acc = &p.ctrl->acc[sv.step & 1];
     const int new_level = sv.level + 1;
 
-    for (long long w = gw; w < p.words; w += nw) {
-        const uint32_t word = __ldcg(&vin[w]);
-        if (word == kFull) {
-            if (lane == 0) { vout[w] = word; }
+    for (long long w0 = gw * K; w0 < p.words; w0 += nw * K) {
+        uint32_t word[K];
+        unsigned open = 0;  // words with work
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            word[k] = (w0 + k < p.words) ? __ldcg(&vin[w0 + k]) : kFull;
+            if (word[k] != kFull) { open |= 1u << k; }
+        }
+        if (!open) {
+            if (lane < K && w0 + lane < p.words) { vout[w0 + lane] = kFull; }
             continue;
         }
-        const uint32_t v = (uint32_t)(w * 32 + lane);
-        const bool unvisited = !((word >> lane) & 1u);
-        bool found = false;
-        uint32_t par = 0;
-        int64_t beg = 0, end = 0, next = 0;
-        if (unvisited) {
-            beg = __ldg(&p.off[v]);
-            end = __ldg(&p.off[v + 1]);
-            const int64_t lim = min(end, beg + (int64_t)p.bu_prefix);
-            int64_t k = beg;
-            for (; k < lim && !found; k += 4) {
-                uint32_t x[4];
-                uint32_t bits[4];
+        uint32_t v[K], par[K];
+        bool found[K], unv[K];
+        int64_t beg[K], end[K], next[K];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) { x[i] = (k + i < lim) ? __ldg(&p.adj[k + i]) : 0u; }
+        for (int k = 0; k < K; ++k) {
+            v[k] = (uint32_t)((w0 + k) * 32 + lane);
+            unv[k] = !((word[k] >> lane) & 1u);
+            found[k] = false;
+            par[k] = 0;
+            beg[k] = end[k] = next[k] = 0;
+            if (unv[k]) {
+                beg[k] = __ldg(&p.off[v[k]]);
+                end[k] = __ldg(&p.off[v[k] + 1]);
+            }
+        }
+        // per-lane scan of the first bu_prefix arcs, P arcs per word per round
+        for (int r = 0; r < p.bu_prefix; r += P) {
+            uint32_t x[K][P];
+            bool in[K][P];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) { bits[i] = (k + i < lim) ? __ldcg(&vin[x[i] >> 5]) : 0u; }
+            for (int k = 0; k < K; ++k) {
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    if (!found && ((bits[i] >> (x[i] & 31)) & 1u)) {
-                        found = true;
-                        par = x[i];
+                for (int j = 0; j < P; ++j) {
+                    const int64_t e = beg[k] + r + j;
+                    in[k][j] = unv[k] && !found[k] && e < end[k];
+                    x[k][j] = in[k][j] ? __ldg(&p.adj[e]) : 0u;
+                }
+            }
+            uint32_t bits[K][P];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+#pragma unroll
+                for (int j = 0; j < P; ++j) { bits[k][j] = in[k][j] ? ld_bits(&vin[x[k][j] >> 5]) : 0u; }
+            }
+            bool more = false;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+#pragma unroll
+                for (int j = 0; j < P; ++j) {
+                    if (in[k][j] && !found[k] && ((bits[k][j] >> (x[k][j] & 31)) & 1u)) {
+                        found[k] = true;
+                        par[k] = x[k][j];
+                    }
+                }
+                more |= unv[k] && !found[k] && beg[k] + r + P < end[k];
+            }
+            if (!__any_sync(kFull, more)) { break; }
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int64_t lim = min(end[k], beg[k] + (int64_t)((p.bu_prefix + P - 1) / P * P));
+            next[k] = found[k] ? end[k] : lim;
+            unsigned pending = __ballot_sync(kFull, unv[k] && !found[k] && next[k] < end[k]);
+            while (pending) {
+                const int owner = __ffs(pending) - 1;
+                pending &= pending - 1;
+                const int64_t b = __shfl_sync(kFull, next[k], owner);
+                const int64_t e = __shfl_sync(kFull, end[k], owner);
+                for (int64_t base = b; base < e; base += 32) {
+                    const int64_t kk = base + lane;
+                    bool hit = false;
+                    uint32_t xx = 0;
+                    if (kk < e) {
+                        xx = __ldg(&p.adj[kk]);
+                        hit = (ld_bits(&vin[xx >> 5]) >> (xx & 31)) & 1u;
+                    }
+                    const unsigned hm = __ballot_sync(kFull, hit);
+                    if (hm) {
+                        const uint32_t hx = __shfl_sync(kFull, xx, __ffs(hm) - 1);
+                        if (lane == owner) {
+                            found[k] = true;
+                            par[k] = hx;
+                        }
+                        break;
                     }
                 }
             }
-            next = found ? end : lim;
+            const unsigned fm = __ballot_sync(kFull, found[k]);
+            if (lane == 0 && w0 + k < p.words) { vout[w0 + k] = word[k] | fm; }
+            if (found[k]) {
+                p.depth[v[k]] = new_level;
+                p.parent[v[k]] = (int64_t)par[k];
+            }
         }
-        unsigned pending = __ballot_sync(kFull, unvisited && !found && next < end);
-        while (pending) {
-            const int owner = __ffs(pending) - 1;
-            pending &= pending - 1;
-            const int64_t b = __shfl_sync(kFull, next, owner);
-            const int64_t e = __shfl_sync(kFull, end, owner);
-            for (int64_t base = b; base < e; base += 32) {
-                const int64_t k = base + lane;
-                bool hit = false;
-                uint32_t x = 0;
-                if (k < e) {
-                    x = __ldg(&p.adj[k]);
-                    hit = (__ldcg(&vin[x >> 5]) >> (x & 31)) & 1u;
+        int64_t deg[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) { deg[k] = end[k] - beg[k]; }
+        warp_append_k<K>(p, acc, qout, found, v, deg, loc);
+    }
+}
+
+// Bottom-up step, lane-owned words (hybrid_bfs.cc:111-143).  Each lane owns
+// one bitmap word (32 vertices) and walks its unvisited vertices on its own:
+// a lane that finds a parent moves straight to its next vertex instead of
+// waiting for the warp's slowest list.  P arcs are probed per iteration.
+// Lists longer than kLongList are left to the whole warp (ballot scan) after
+// the per-lane walk.  Reads only the frozen bitmap vis[cur]; writes whole
+// words of vis[cur^1].
+constexpr int64_t kLongList = 256;
+
+template <int BLOCK>
+__device__ void bu_step_lanes(const BfsParams &p, const StepView &sv, Local &loc)
+{
+    constexpr int P = 4;
+    const int lane = lane_id();
+    const int warp = threadIdx.x >> 5;
+    const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
+    const long long nw = (long long)gridDim.x * (BLOCK / 32);
+    const uint32_t *vin = p.vis[sv.vis_cur];
+    uint32_t *vout = p.vis[sv.vis_cur ^ 1];
+    const int qout = sv.q_cur ^ 1;
+    Acc *acc = &p.ctrl->acc[sv.step & 1];
+    const int new_level = sv.level + 1;
+
+    for (long long base = gw * 32; base < p.words; base += nw * 32) {
+        const long long w = base + lane;
+        const bool mine = w < p.words;
+        const uint32_t word = mine ? __ldcg(&vin[w]) : kFull;
+        uint32_t todo = ~word;     // unvisited vertices of this lane's word
+        uint32_t found = 0;        // ... that found a parent
+        uint32_t longs = 0;        // ... with lists left to the warp
+        int64_t e = 0, end = 0;
+        int cur = -1;
+        unsigned long long degsum = 0;
+        while (__any_sync(kFull, todo != 0 || cur >= 0)) {
+            if (cur < 0 && todo) {
+                cur = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const uint32_t v = (uint32_t)(w * 32 + cur);
+                e = __ldg(&p.off[v]);
+                end = __ldg(&p.off[v + 1]);
+                if (end - e > kLongList) {
+                    longs |= 1u << cur;
+                    cur = -1;
                 }
-                const unsigned hm = __ballot_sync(kFull, hit);
-                if (hm) {
-                    const uint32_t hx = __shfl_sync(kFull, x, __ffs(hm) - 1);
-                    if (lane == owner) {
-                        found = true;
-                        par = hx;
-                    }
-                    break;
+            }
+            if (cur >= 0) {
+                uint32_t x[P], bits[P];
+#pragma unroll
+                for (int j = 0; j < P; ++j) { x[j] = (e + j < end) ? __ldg(&p.adj[e + j]) : 0u; }
+#pragma unroll
+                for (int j = 0; j < P; ++j) { bits[j] = (e + j < end) ? ld_bits(&vin[x[j] >> 5]) : 0u; }
+                int hit = -1;
+#pragma unroll
+                for (int j = P - 1; j >= 0; --j) {
+                    if ((e + j < end) && ((bits[j] >> (x[j] & 31)) & 1u)) { hit = j; }
+                }
+                if (hit >= 0) {
+                    const uint32_t v = (uint32_t)(w * 32 + cur);
+                    found |= 1u << cur;
+                    p.depth[v] = new_level;
+                    p.parent[v] = (int64_t)x[hit];
+                    degsum += (unsigned long long)(end - __ldg(&p.off[v]));
+                    cur = -1;
+                } else {
+                    e += P;
+                    if (e >= end) { cur = -1; }
                 }
             }
         }
-        const unsigned fm = __ballot_sync(kFull, found);
-        if (lane == 0) { vout[w] = word | fm; }
-        if (found) {
-            p.depth[v] = new_level;
-            p.parent[v] = (int64_t)par;
+        // long lists: the whole warp, one vertex at a time, 32 arcs a ballot
+        unsigned owners = __ballot_sync(kFull, longs != 0);
+        while (owners) {
+            const int owner = __ffs(owners) - 1;
+            uint32_t ol = __shfl_sync(kFull, longs, owner);
+            const long long ow = __shfl_sync(kFull, w, owner);
+            while (ol) {
+                const int bit = __ffs(ol) - 1;
+                ol &= ol - 1;
+                const uint32_t v = (uint32_t)(ow * 32 + bit);
+                const int64_t b = __ldg(&p.off[v]), en = __ldg(&p.off[v + 1]);
+                for (int64_t kb = b; kb < en; kb += 32) {
+                    const int64_t k = kb + lane;
+                    bool hit = false;
+                    uint32_t xx = 0;
+                    if (k < en) {
+                        xx = __ldg(&p.adj[k]);
+                        hit = (ld_bits(&vin[xx >> 5]) >> (xx & 31)) & 1u;
+                    }
+                    const unsigned hm = __ballot_sync(kFull, hit);
+                    if (hm) {
+                        const uint32_t hx = __shfl_sync(kFull, xx, __ffs(hm) - 1);
+                        if (lane == owner) {
+                            found |= 1u << bit;
+                            p.depth[v] = new_level;
+                            p.parent[v] = (int64_t)hx;
+                            degsum += (unsigned long long)(en - b);
+                        }
+                        break;
+                    }
+                }
+            }
+            owners &= owners - 1;
         }
-        warp_append(p, acc, qout, found, v, end - beg, loc);
+        if (mine) { vout[w] = word | found; }
+        // append this lane's discoveries: one atomic per warp for the small
+        // ones, one per large vertex (rare)
+        uint32_t small = 0, large = 0;
+        for (uint32_t f = found; f; f &= f - 1) {
+            const int bit = __ffs(f) - 1;
+            const uint32_t v = (uint32_t)(w * 32 + bit);
+            if (__ldg(&p.off[v + 1]) - __ldg(&p.off[v]) >= (int64_t)p.large_deg) {
+                large |= 1u << bit;
+            } else {
+                small |= 1u << bit;
+            }
+        }
+        const unsigned cnt = __popc(small);
+        const unsigned incl = warp_incl_scan(cnt);
+        const unsigned total = __shfl_sync(kFull, incl, 31);
+        if (total) {
+            unsigned long long start = 0;
+            if (lane == 0) { start = atomicAdd(&acc->small_cnt, (unsigned long long)total); }
+            start = __shfl_sync(kFull, start, 0) + (incl - cnt);
+            for (uint32_t f = small; f; f &= f - 1) {
+                p.qs[qout][start++] = (uint32_t)(w * 32 + (__ffs(f) - 1));
+            }
+        }
+        for (uint32_t f = large; f; f &= f - 1) {
+            const uint32_t v = (uint32_t)(w * 32 + (__ffs(f) - 1));
+            const int64_t d = __ldg(&p.off[v + 1]) - __ldg(&p.off[v]);
+            const unsigned long long nch = (unsigned long long)((d + p.chunk - 1) / p.chunk);
+            const unsigned long long old =
+                atomicAdd(&acc->large_packed, (1ull << kLargeShift) | nch);
+            const unsigned long long pos = old >> kLargeShift;
+            p.ql[qout][pos] = v;
+            p.qlb[qout][pos] = old & kChunkMask;
+        }
+        loc.found += __popc(found);
+        loc.degsum += degsum;
     }
 }
 
@@ -459,7 +691,14 @@ __device__ void choose_next(Ctrl *c, const BfsParams &p, SharedState<BLOCK> *sh)
     }
     if (!sh) { return; }
     __syncthreads();
-    const bool learned = p.alg == BD_ALG_LEARNED && p.policy && sh->beamer_dir != kDirDone;
+    bool learned = p.alg == BD_ALG_LEARNED && p.policy && sh->beamer_dir != kDirDone;
+    if (learned) {
+        // out of the trusted feature range: the rule decides
+#pragma unroll
+        for (int i = 0; i < kPolicyIn; ++i) {
+            if (!(sh->feat[i] >= p.policy->lo[i] && sh->feat[i] <= p.policy->hi[i])) { learned = false; }
+        }
+    }
     if (learned && tid < 32) {
         const PolicyBlob *w = p.policy;
         const int j = tid;
@@ -531,6 +770,9 @@ __device__ void finish_step(Ctrl *c, const BfsParams &p)
     }
     c->visited_degsum += degsum;
     c->reached += found;
+    // once fewer than half of the live vertices are unvisited, bottom-up
+    // work per bitmap word is sparse: switch to the lane-owned layout
+    c->bu_sparse = 2 * (p.n_live - c->reached) < p.n_live;
     c->f_count = found;
     c->f_degsum = degsum;
     c->f_small = nsmall;
@@ -618,7 +860,20 @@ __device__ void reduce_and_publish(const BfsParams &p, const StepView &sv, Share
     loc.degsum = 0;
 }
 
-template <int BLOCK, int MINB>
+// K bitmap words per warp step: 1, 2, 4 (warp-shared words) or 32 (one word
+// per lane).
+template <int BLOCK, int K>
+__device__ __forceinline__ void bu_layout(const BfsParams &p, const StepView &sv, Local &loc)
+{
+    if constexpr (K == 32) {
+        bu_step_lanes<BLOCK>(p, sv, loc);
+    } else {
+        bu_step<BLOCK, K>(p, sv, loc);
+    }
+}
+
+// KD: bottom-up layout while most live vertices are unvisited; KS: after.
+template <int BLOCK, int MINB, int KD, int KS>
 __global__ void __launch_bounds__(BLOCK, MINB) bfs_persistent_kernel(BfsParams p)
 {
     __shared__ SharedState<BLOCK> sh;
@@ -636,7 +891,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) bfs_persistent_kernel(BfsParams p
         if (sv.dir == kDirTD) {
             td_step<BLOCK>(p, sv, sh, loc);
         } else {
-            bu_step<BLOCK>(p, sv, loc);
+            if (sv.bu_sparse) {
+                bu_layout<BLOCK, KS>(p, sv, loc);
+            } else {
+                bu_layout<BLOCK, KD>(p, sv, loc);
+            }
         }
         reduce_and_publish<BLOCK>(p, sv, sh, loc);
         barrier_decide<BLOCK>(p, sh);
@@ -768,13 +1027,17 @@ struct KernelChoice {
     int block;
 };
 
-KernelChoice pick_kernel(int block)
+KernelChoice pick_kernel(int block, int kd = 4, int ks = 4)
 {
-    switch (block) {
-        case 256: return {bfs_persistent_kernel<256, 4>, 256};
-        case 1024: return {bfs_persistent_kernel<1024, 1>, 1024};
-        default: return {bfs_persistent_kernel<512, 2>, 512};
-    }
+#define BD_KC(B, M, D, S) \
+    if (block == B && kd == D && ks == S) { return {bfs_persistent_kernel<B, M, D, S>, B}; }
+#define BD_KC_B(B, M)                                                                  \
+    BD_KC(B, M, 1, 1) BD_KC(B, M, 2, 2) BD_KC(B, M, 4, 4) BD_KC(B, M, 32, 32)          \
+    BD_KC(B, M, 2, 32) BD_KC(B, M, 4, 32)
+    BD_KC_B(256, 4) BD_KC_B(512, 2) BD_KC_B(1024, 1)
+#undef BD_KC_B
+#undef BD_KC
+    return {nullptr, 0};
 }
 
 }  // namespace
@@ -840,6 +1103,7 @@ BfsParams make_params(bd_bfs *b)
     p.vis[0] = b->vis[0];
     p.vis[1] = b->vis[1];
     p.words = bitmap_words(b->g->n);
+    p.n_live = b->g->n_live;
     for (int i = 0; i < 2; ++i) {
         p.qs[i] = b->qs[i];
         p.ql[i] = b->ql[i];
@@ -1001,8 +1265,11 @@ bd_status bd_bfs_create(bd_graph *g, const bd_bfs_opts *opts, bd_bfs **out)
     }
     if (o.block_size == 0) { o.block_size = 512; }
     if (o.block_size != 256 && o.block_size != 512 && o.block_size != 1024) { return BD_ERR_INVALID; }
-    if (o.large_degree <= 0) { o.large_degree = 1024; }
-    if (o.chunk_edges <= 0) { o.chunk_edges = 1024; }
+    if (o.bu_words == 0) { o.bu_words = 4; }
+    if (o.bu_sparse_words == 0) { o.bu_sparse_words = o.bu_words == 1 ? 1 : 32; }
+    if (o.large_degree <= 0) { o.large_degree = 32; }
+    if (o.large_degree > (1 << 20)) { return BD_ERR_INVALID; }
+    if (o.chunk_edges <= 0) { o.chunk_edges = 256; }
     if (o.bu_prefix <= 0) { o.bu_prefix = 32; }
     if (o.spin_limit <= 0) { o.spin_limit = kDefaultSpin; }
     if (o.test_extra_ctas < 0) { return BD_ERR_INVALID; }
@@ -1030,7 +1297,8 @@ bd_status bd_bfs_create(bd_graph *g, const bd_bfs_opts *opts, bd_bfs **out)
              cudaMalloc(&b->qlb[i], sizeof(unsigned long long) * b->cap_large) == cudaSuccess;
     }
     if (!ok) { return fail(BD_ERR_OOM); }
-    KernelChoice kc = pick_kernel(o.block_size);
+    KernelChoice kc = pick_kernel(o.block_size, o.bu_words, o.bu_sparse_words);
+    if (!kc.fn) { return fail(BD_ERR_INVALID); }
     b->kernel = kc.fn;
     b->block = kc.block;
     int per_sm = 0, sms = 0;
@@ -1385,6 +1653,7 @@ extern "C" bd_status bd_bfs_run_noalloc(const int64_t *d_offsets, const uint32_t
     p.depth = d_depth;
     p.parent = d_parent;
     p.words = bitmap_words(num_vertices);
+    p.n_live = num_vertices;
     Ctrl *ctrl = reinterpret_cast<Ctrl *>(base + kNaOffCtrl);
     int64_t *source_slot = reinterpret_cast<int64_t *>(base + kNaOffSource);
     for (int i = 0; i < 2; ++i) {

@@ -58,6 +58,8 @@ struct Ctrl {
     long long t_last;
     long long td_steps, bu_steps;
     long long policy_overrides;  // learned decisions that differed from Beamer
+    int bu_sparse;               // next bottom-up step uses the sparse layout
+    int pad0;
     Acc acc[2];
 };
 
@@ -76,6 +78,8 @@ struct PolicyBlob {
     float b3[kPolicyOut];
     float mean[kPolicyIn];   // feature standardisation
     float inv_std[kPolicyIn];
+    float lo[kPolicyIn];     // raw-feature range the policy trusts; outside
+    float hi[kPolicyIn];     // it the Beamer rule decides
     float margin;            // |logit gap| below which Beamer decides
     float pad[3];
 };
@@ -89,6 +93,7 @@ struct BfsParams {
     int64_t *parent;
     uint32_t *vis[2];
     int64_t words;
+    int64_t n_live;  // vertices of nonzero degree
     uint32_t *qs[2];
     uint32_t *ql[2];
     unsigned long long *qlb[2];

@@ -213,6 +213,49 @@ __global__ void unpack_relabel_kernel(const uint64_t *packed, int64_t m, int sca
 }
 
 // ---------------------------------------------------------------------------
+// 2-D grid with 4-neighbour edges, a seeded fraction deleted
+// ---------------------------------------------------------------------------
+constexpr uint32_t kTagGrid = 0x47524944u;  // "GRID"
+
+// Edge e: e < rows*(cols-1) is horizontal (r, c)-(r, c+1) with
+// r = e / (cols-1), c = e % (cols-1); the rest are vertical (r, c)-(r+1, c).
+// Edge e is kept when the top 53 bits of its Philox key, as a fraction of
+// 2^53, are >= delete_frac.
+__global__ void grid_keep_kernel(int64_t rows, int64_t cols, double delete_frac, uint64_t seed,
+                                 int64_t total, int *keep)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = perm_key(seed, (uint64_t)e, kTagGrid);
+        const double u = __dmul_rn(__ull2double_rn(k >> 11), 1.0 / 9007199254740992.0);
+        keep[e] = u >= delete_frac ? 1 : 0;
+    }
+}
+
+__global__ void grid_emit_kernel(int64_t rows, int64_t cols, int64_t total, const int *keep,
+                                 const int64_t *pos, int64_t *src, int64_t *dst)
+{
+    const int64_t horiz = rows * (cols - 1);
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        if (!keep[e]) { continue; }
+        int64_t a, b;
+        if (e < horiz) {
+            const int64_t r = e / (cols - 1), c = e % (cols - 1);
+            a = r * cols + c;
+            b = a + 1;
+        } else {
+            const int64_t f = e - horiz;
+            const int64_t r = f / cols, c = f % cols;
+            a = r * cols + c;
+            b = a + cols;
+        }
+        src[pos[e]] = a;
+        dst[pos[e]] = b;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // CSR construction
 // ---------------------------------------------------------------------------
 
@@ -273,6 +316,31 @@ __global__ void offsets_from_sorted_kernel(const uint32_t *sorted_src, int64_t a
         int64_t cur = i == arcs ? n : (int64_t)sorted_src[i];
         for (int64_t v = prev + 1; v <= cur; ++v) { off[v] = i; }
     }
+}
+
+// Key of arc i for the degree order: source in the high word, then the
+// complement of the neighbour's degree (higher degree sorts first).
+__global__ void degree_keys_kernel(const uint32_t *src, const uint32_t *adj, const int64_t *off,
+                                   int64_t arcs, uint64_t *key)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < arcs;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = adj[i];
+        const int64_t d = off[v + 1] - off[v];
+        const uint32_t dc = 0xFFFFFFFFu - (uint32_t)(d < 0xFFFFFFFFll ? d : 0xFFFFFFFFll);
+        key[i] = ((uint64_t)src[i] << 32) | dc;
+    }
+}
+
+__global__ void count_live_kernel(const int64_t *off, int64_t n, unsigned long long *live)
+{
+    unsigned long long c = 0;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        c += off[v + 1] != off[v];
+    }
+    for (int d = 16; d > 0; d >>= 1) { c += __shfl_xor_sync(0xFFFFFFFFu, c, d); }
+    if ((threadIdx.x & 31) == 0 && c) { atomicAdd(live, c); }
 }
 
 __global__ void isolated_bitmap_kernel(const int64_t *off, int64_t n, uint32_t *bits)
@@ -490,7 +558,15 @@ bd_status graph_finish(bd_graph *g, cudaStream_t s)
     BD_CUDA(cudaMalloc(&g->d_isolated, sizeof(uint32_t) * (words ? words : 1)));
     isolated_bitmap_kernel<<<grid_for(words), kThreads, 0, s>>>(g->d_off, g->n, g->d_isolated);
     BD_CUDA(cudaGetLastError());
+    DevBuf<unsigned long long> live;
+    if (live.alloc(1) != cudaSuccess) { return BD_ERR_OOM; }
+    BD_CUDA(cudaMemsetAsync(live.p, 0, sizeof(unsigned long long), s));
+    count_live_kernel<<<grid_for(g->n), kThreads, 0, s>>>(g->d_off, g->n, live.p);
+    BD_CUDA(cudaGetLastError());
+    unsigned long long nl = 0;
+    BD_CUDA(cudaMemcpyAsync(&nl, live.p, sizeof(nl), cudaMemcpyDeviceToHost, s));
     BD_CUDA(cudaStreamSynchronize(s));
+    g->n_live = (int64_t)nl;
     return BD_OK;
 }
 
@@ -551,6 +627,29 @@ bd_status graph_from_device_edges(int64_t n, int64_t m, int64_t *d_src, int64_t 
     int flag = 0;
     if (read_flag(bad.p, &flag) != BD_OK) { return fail(BD_ERR_CUDA); }
     if (flag) { return fail(BD_ERR_RANGE); }
+    if (order == BD_ORDER_DEGREE) {
+        // Re-sort every list by neighbour degree, highest first; the stable
+        // sort keeps insertion order among equal degrees.
+        DevBuf<uint64_t> k_in, k_out;
+        DevBuf<uint32_t> v_out;
+        if (k_in.alloc(arcs) != cudaSuccess || k_out.alloc(arcs) != cudaSuccess ||
+            v_out.alloc(arcs) != cudaSuccess) {
+            return fail(BD_ERR_OOM);
+        }
+        degree_keys_kernel<<<grid_for(arcs), kThreads, 0, s>>>(sorted_src.p, g->d_adj, g->d_off,
+                                                               arcs, k_in.p);
+        const int end_bit = 32 + bits_for(n);
+        cudaError_t e = cub_run([&](void *tmp, size_t &bytes) {
+            return cub::DeviceRadixSort::SortPairs(tmp, bytes, k_in.p, k_out.p, g->d_adj, v_out.p,
+                                                   arcs, 0, end_bit, s);
+        }, s);
+        if (e != cudaSuccess) { return fail(cuda_fail(e, "SortPairs(degree)", __FILE__, __LINE__)); }
+        if (cudaMemcpyAsync(g->d_adj, v_out.p, sizeof(uint32_t) * arcs, cudaMemcpyDeviceToDevice,
+                            s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            return fail(BD_ERR_CUDA);
+        }
+    }
     bd_status st = graph_finish(g, s);
     if (st != BD_OK) { return fail(st); }
     *out = g;
@@ -569,7 +668,7 @@ bd_status bd_graph_from_edges(int64_t num_vertices, int64_t num_edges, const int
     if (!out || (!src && num_edges) || (!dst && num_edges) || num_vertices <= 0 || num_edges < 0) {
         return BD_ERR_INVALID;
     }
-    if (adjacency_order != BD_ORDER_INSERTION && adjacency_order != BD_ORDER_SORTED) {
+    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_DEGREE) {
         return BD_ERR_INVALID;
     }
     if (num_vertices > (int64_t)UINT32_MAX) { return BD_ERR_LIMIT; }
@@ -596,7 +695,7 @@ bd_status bd_graph_from_edges(int64_t num_vertices, int64_t num_edges, const int
 bd_status bd_graph_from_el64(const char *path, int32_t adjacency_order, bd_graph **out)
 {
     if (!path || !out) { return BD_ERR_INVALID; }
-    if (adjacency_order != BD_ORDER_INSERTION && adjacency_order != BD_ORDER_SORTED) {
+    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_DEGREE) {
         return BD_ERR_INVALID;
     }
     FILE *fp = fopen(path, "rb");
@@ -716,7 +815,7 @@ bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, 
     if (!(a >= 0 && b >= 0 && c >= 0 && d >= 0 && a <= 1 && b <= 1 && c <= 1 && d <= 1)) {
         return BD_ERR_INVALID;
     }
-    if (adjacency_order != BD_ORDER_INSERTION && adjacency_order != BD_ORDER_SORTED) {
+    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_DEGREE) {
         return BD_ERR_INVALID;
     }
     BD_TRY(ensure_device());
@@ -783,6 +882,63 @@ bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, 
     ekeys_sorted.reset();
     vkeys.reset();
     vkeys_sorted.reset();
+    return graph_from_device_edges(n, m, d_src, d_dst, adjacency_order, out);
+}
+
+bd_status bd_graph_grid(int64_t rows, int64_t cols, double delete_frac, uint64_t seed,
+                        int32_t adjacency_order, bd_graph **out)
+{
+    if (!out || rows < 1 || cols < 1 || !(delete_frac >= 0.0 && delete_frac <= 1.0)) {
+        return BD_ERR_INVALID;
+    }
+    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_DEGREE) {
+        return BD_ERR_INVALID;
+    }
+    if (rows * cols > (int64_t)UINT32_MAX) { return BD_ERR_LIMIT; }
+    BD_TRY(ensure_device());
+    const int64_t n = rows * cols;
+    const int64_t total = rows * (cols - 1) + (rows - 1) * cols;
+    DevBuf<int> keep;
+    DevBuf<int64_t> pos, count;
+    if (keep.alloc(total) != cudaSuccess || pos.alloc(total + 1) != cudaSuccess ||
+        count.alloc(1) != cudaSuccess) {
+        return BD_ERR_OOM;
+    }
+    cudaStream_t s = 0;
+    if (total > 0) {
+        grid_keep_kernel<<<grid_for(total), kThreads, 0, s>>>(rows, cols, delete_frac, seed, total,
+                                                               keep.p);
+        BD_CUDA(cudaGetLastError());
+        BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
+            return cub::DeviceScan::ExclusiveSum(tmp, bytes, keep.p, pos.p, total, s);
+        }, s));
+    }
+    int64_t m = 0;
+    if (total > 0) {
+        int last_keep = 0;
+        int64_t last_pos = 0;
+        BD_CUDA(cudaMemcpy(&last_keep, keep.p + total - 1, sizeof(int), cudaMemcpyDeviceToHost));
+        BD_CUDA(cudaMemcpy(&last_pos, pos.p + total - 1, sizeof(int64_t), cudaMemcpyDeviceToHost));
+        m = last_pos + last_keep;
+    }
+    int64_t *d_src = nullptr, *d_dst = nullptr;
+    if (cudaMalloc(&d_src, sizeof(int64_t) * (m ? m : 1)) != cudaSuccess ||
+        cudaMalloc(&d_dst, sizeof(int64_t) * (m ? m : 1)) != cudaSuccess) {
+        cudaFree(d_src);
+        cudaFree(d_dst);
+        return BD_ERR_OOM;
+    }
+    if (total > 0) {
+        grid_emit_kernel<<<grid_for(total), kThreads, 0, s>>>(rows, cols, total, keep.p, pos.p,
+                                                               d_src, d_dst);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) { e = cudaStreamSynchronize(s); }
+    if (e != cudaSuccess) {
+        cudaFree(d_src);
+        cudaFree(d_dst);
+        return cuda_fail(e, "grid_emit_kernel", __FILE__, __LINE__);
+    }
     return graph_from_device_edges(n, m, d_src, d_dst, adjacency_order, out);
 }
 

@@ -42,6 +42,7 @@ struct bd_graph {
     int64_t n = 0;          // vertices
     int64_t m = 0;          // undirected edges (arcs / 2)
     int64_t arcs = 0;       // entries of the adjacency array
+    int64_t n_live = 0;     // vertices of nonzero degree
     int32_t order = BD_ORDER_INSERTION;
     int64_t *d_off = nullptr;     // [n + 1]
     uint32_t *d_adj = nullptr;    // [arcs]

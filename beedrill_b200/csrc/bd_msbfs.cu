@@ -1,0 +1,936 @@
+// bd_msbfs.cu -- batched traversal: up to 64 BFSs at once, one bit lane of a
+// uint64 per root ("multi-source BFS"), in one persistent cooperative launch.
+//
+// The reference runs its trials one root at a time (hybrid_bfs_main.cc:252-302);
+// every root re-reads the whole graph.  Here R <= 64 roots share each pass
+// over the adjacency: vertex v carries seen[v] (lanes that reached it
+// before the current level) and F[v] (lanes whose frontier holds it), and a
+// level updates all lanes with 64-bit ORs.  Results per lane are exactly
+// those of a single-source BFS from that lane's root: depths equal, parents
+// one level up (each (vertex, lane) gets the first neighbour that delivered
+// the lane's bit).
+//
+// Steps, chosen per level on the device (Beamer-style rule over the batch):
+//   push  frontier vertices OR their lanes into their neighbours' next
+//         word (atomicOr; the returned old word identifies the one writer
+//         that delivered each new lane, which becomes that lane's parent);
+//   pull  each vertex not yet reached by every lane ORs its neighbours'
+//         frontier words until it has all the lanes it still needs.
+//
+// Layout in HBM (n vertices, R lanes):
+//   seen    uint64[n]      lanes that reached v at an earlier level
+//   F[3]    uint64[n]      frontier words, three buffers: step s reads
+//                          F[s%3], writes F[(s+1)%3], clears F[(s+2)%3]
+//   Q[3]                   the vertex lists of those frontiers (degree bins)
+//   depth   int32[n][R]    vertex-major, so a vertex's lanes share sectors
+//   parent  uint32[n][R]   vertex-major; widened to the reference's int64
+//                          encoding when copied out
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "bd_device_util.cuh"
+#include "bd_internal.h"
+
+namespace bd {
+namespace {
+
+using namespace dev;
+using ull = unsigned long long;
+
+constexpr int kPush = 0, kPull = 1, kMsDone = 2;
+constexpr int kLargeShift = 38;
+constexpr ull kChunkMask = (1ull << kLargeShift) - 1;
+constexpr int64_t kMsRecCap = 1 << 14;
+constexpr long long kMsDefaultSpin = 4000000;
+
+struct MsAcc {
+    ull vertices;    // vertices entering the next frontier
+    ull degsum;      // their degree sum
+    ull lanes;       // new (vertex, lane) pairs
+    ull small_cnt;
+    ull large_packed;
+    ull done_degsum; // degree sum of vertices that just got every lane
+};
+
+struct MsCtrl {
+    unsigned bar_count, bar_gen;
+    int error, dir, level, step;
+    long long f_count, f_degsum, f_small, f_large, f_chunks;
+    long long p_small, p_large;  // lists of the frontier read by the previous step
+    long long arcs_left;         // 2m - degree sum of vertices reached by all lanes
+    long long lanes_total;
+    long long t_last, push_steps, pull_steps;
+    MsAcc acc[2];
+};
+
+struct MsParams {
+    const int64_t *off;
+    const uint32_t *adj;
+    const uint32_t *isolated;
+    int64_t n, m;
+    ull *seen;
+    ull *F[3];
+    uint32_t *qs[3];
+    uint32_t *ql[3];
+    ull *qlb[3];
+    int32_t *depth;
+    uint32_t *parent;
+    int R;
+    ull all;
+    MsCtrl *ctrl;
+    bd_step *rec;
+    int64_t rec_cap;
+    int64_t alpha;
+    uint32_t large_deg, chunk;
+    int prefix;
+    long long spin_limit;
+    unsigned expected_ctas;
+    int force_dir;  // -1 rule, kPush, kPull
+};
+
+struct MsLocal {
+    ull vertices, degsum, lanes, done_degsum;
+};
+
+__device__ __forceinline__ int64_t ms_degree(const MsParams &p, uint32_t v)
+{
+    return __ldg(&p.off[v + 1]) - __ldg(&p.off[v]);
+}
+
+// Warp-collective append of new frontier vertices, binned by degree
+// (same scheme as the single-source kernel).
+__device__ __forceinline__ void ms_append(const MsParams &p, MsAcc *acc, int qn, bool has,
+                                          uint32_t v, int64_t deg, MsLocal &loc)
+{
+    if (has) {
+        loc.vertices += 1;
+        loc.degsum += (ull)deg;
+    }
+    const int lane = lane_id();
+    const bool large = has && deg >= (int64_t)p.large_deg;
+    const unsigned sm = __ballot_sync(kFullMask, has && !large);
+    if (sm) {
+        const int leader = __ffs(sm) - 1;
+        ull base = 0;
+        if (lane == leader) { base = atomicAdd(&acc->small_cnt, (ull)__popc(sm)); }
+        base = __shfl_sync(kFullMask, base, leader);
+        if (has && !large) { p.qs[qn][base + __popc(sm & lanemask_lt())] = v; }
+    }
+    const unsigned lm = __ballot_sync(kFullMask, large);
+    if (lm) {
+        const ull nch = large ? (ull)((deg + p.chunk - 1) / p.chunk) : 0ull;
+        const ull incl = warp_incl_scan(nch);
+        const ull total = __shfl_sync(kFullMask, incl, 31);
+        const int leader = __ffs(lm) - 1;
+        ull old = 0;
+        if (lane == leader) {
+            old = atomicAdd(&acc->large_packed, ((ull)__popc(lm) << kLargeShift) | total);
+        }
+        old = __shfl_sync(kFullMask, old, leader);
+        if (large) {
+            const ull pos = (old >> kLargeShift) + __popc(lm & lanemask_lt());
+            p.ql[qn][pos] = v;
+            p.qlb[qn][pos] = (old & kChunkMask) + incl - nch;
+        }
+    }
+}
+
+__device__ __forceinline__ void write_lanes(const MsParams &p, uint32_t v, ull lanes, int level,
+                                            uint32_t parent)
+{
+    while (lanes) {
+        const int r = __ffsll((long long)lanes) - 1;
+        lanes &= lanes - 1;
+        p.depth[(int64_t)v * p.R + r] = level;
+        p.parent[(int64_t)v * p.R + r] = parent;
+    }
+}
+
+struct MsView {
+    int dir, level, step;
+    long long f_small, f_large, f_chunks, p_small, p_large;
+};
+
+__device__ __forceinline__ MsView ms_view(const MsCtrl *c)
+{
+    const volatile MsCtrl *vc = c;
+    MsView v;
+    v.dir = vc->dir;
+    v.level = vc->level;
+    v.step = vc->step;
+    v.f_small = vc->f_small;
+    v.f_large = vc->f_large;
+    v.f_chunks = vc->f_chunks;
+    v.p_small = vc->p_small;
+    v.p_large = vc->p_large;
+    return v;
+}
+
+// Zeroes the frontier words of the frontier read by the previous step.
+__device__ void ms_clear_old(const MsParams &p, const MsView &sv)
+{
+    const int old = (sv.step + 2) % 3;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nt = (long long)gridDim.x * blockDim.x;
+    for (long long i = t; i < sv.p_small; i += nt) { p.F[old][p.qs[old][i]] = 0ull; }
+    for (long long i = t; i < sv.p_large; i += nt) { p.F[old][p.ql[old][i]] = 0ull; }
+}
+
+// push: lanes of frontier vertex u flow into neighbours [b, e).
+__device__ __forceinline__ void push_edges(const MsParams &p, MsAcc *acc, int cur, int nxt,
+                                           int new_level, uint32_t u, ull bits, int64_t b,
+                                           int64_t e, MsLocal &loc)
+{
+    const int lane = lane_id();
+    for (int64_t base = b; base < e; base += 32) {
+        const int64_t k = base + lane;
+        bool appended = false;
+        uint32_t v = 0;
+        int64_t deg = 0;
+        if (k < e) {
+            v = __ldg(&p.adj[k]);
+            const ull vis = __ldcg(&p.seen[v]) | __ldcg(&p.F[cur][v]);
+            const ull give = bits & ~vis;
+            if (give) {
+                const ull old = atomicOr(&p.F[nxt][v], give);
+                const ull fresh = give & ~old;
+                if (fresh) {
+                    write_lanes(p, v, fresh, new_level, u);
+                    loc.lanes += __popcll(fresh);
+                    if (((vis | old | fresh) & p.all) == p.all) { loc.done_degsum += ms_degree(p, v); }
+                }
+                if (old == 0ull) {
+                    appended = true;
+                    deg = ms_degree(p, v);
+                }
+            }
+        }
+        ms_append(p, acc, nxt, appended, v, deg, loc);
+    }
+}
+
+template <int BLOCK>
+__device__ void ms_push_step(const MsParams &p, const MsView &sv, MsLocal &loc)
+{
+    const int lane = lane_id();
+    const int warp = threadIdx.x >> 5;
+    const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
+    const long long nw = (long long)gridDim.x * (BLOCK / 32);
+    const int cur = sv.step % 3, nxt = (sv.step + 1) % 3;
+    MsAcc *acc = &p.ctrl->acc[sv.step & 1];
+    const int new_level = sv.level + 1;
+    // large frontier vertices: chunk c of vertex ql[i]
+    for (long long c = gw; c < sv.f_chunks; c += nw) {
+        long long lo = 0, hi = sv.f_large - 1;
+        while (lo < hi) {
+            long long mid = (lo + hi + 1) >> 1;
+            if ((long long)__ldcg(&p.qlb[cur][mid]) <= c) { lo = mid; } else { hi = mid - 1; }
+        }
+        const uint32_t u = __ldcg(&p.ql[cur][lo]);
+        const long long j = c - (long long)__ldcg(&p.qlb[cur][lo]);
+        const ull bits = __ldcg(&p.F[cur][u]);
+        if (j == 0 && lane == 0) { p.seen[u] |= bits; }
+        const int64_t ub = __ldg(&p.off[u]), ue = __ldg(&p.off[u + 1]);
+        const int64_t b = ub + j * (int64_t)p.chunk;
+        push_edges(p, acc, cur, nxt, new_level, u, bits, b, min(ue, b + (int64_t)p.chunk), loc);
+    }
+    // small frontier vertices: one warp walks one vertex at a time
+    for (long long i = gw; i < sv.f_small; i += nw) {
+        const uint32_t u = __ldcg(&p.qs[cur][i]);
+        const ull bits = __ldcg(&p.F[cur][u]);
+        if (lane == 0) { p.seen[u] |= bits; }
+        push_edges(p, acc, cur, nxt, new_level, u, bits, __ldg(&p.off[u]), __ldg(&p.off[u + 1]), loc);
+    }
+}
+
+// pull: warp per 32 vertices; short lists per lane, long lists by the warp.
+template <int BLOCK>
+__device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
+{
+    const int lane = lane_id();
+    const int warp = threadIdx.x >> 5;
+    const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
+    const long long nw = (long long)gridDim.x * (BLOCK / 32);
+    const int cur = sv.step % 3, nxt = (sv.step + 1) % 3;
+    MsAcc *acc = &p.ctrl->acc[sv.step & 1];
+    const int new_level = sv.level + 1;
+    const long long words = (p.n + 31) / 32;
+    for (long long w = gw; w < words; w += nw) {
+        const uint32_t iso = __ldg(&p.isolated[w]);
+        if (iso == kFullMask) { continue; }
+        const uint32_t v = (uint32_t)(w * 32 + lane);
+        const bool live = !((iso >> lane) & 1u);
+        ull need = 0, got = 0;
+        int64_t beg = 0, end = 0, next = 0;
+        if (live) {
+            const ull f = __ldcg(&p.F[cur][v]);
+            ull s = __ldcg(&p.seen[v]);
+            if (f) {
+                s |= f;
+                p.seen[v] = s;
+            }
+            need = p.all & ~s;
+            if (need) {
+                beg = __ldg(&p.off[v]);
+                end = __ldg(&p.off[v + 1]);
+                const int64_t lim = min(end, beg + (int64_t)p.prefix);
+                int64_t k = beg;
+                for (; k < lim && got != need; ++k) {
+                    const uint32_t u = __ldg(&p.adj[k]);
+                    const ull fu = __ldcg(&p.F[cur][u]) & need & ~got;
+                    if (fu) {
+                        got |= fu;
+                        write_lanes(p, v, fu, new_level, u);
+                    }
+                }
+                next = (got == need) ? end : k;
+            }
+        }
+        unsigned pending = __ballot_sync(kFullMask, need != 0 && got != need && next < end);
+        while (pending) {
+            const int owner = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const int64_t b = __shfl_sync(kFullMask, next, owner);
+            const int64_t e = __shfl_sync(kFullMask, end, owner);
+            const ull nd = __shfl_sync(kFullMask, need, owner);
+            ull have = __shfl_sync(kFullMask, got, owner);
+            const uint32_t vo = __shfl_sync(kFullMask, v, owner);
+            for (int64_t base = b; base < e && have != nd; base += 32) {
+                const int64_t k = base + lane;
+                ull fu = 0;
+                uint32_t u = 0;
+                if (k < e) {
+                    u = __ldg(&p.adj[k]);
+                    fu = __ldcg(&p.F[cur][u]) & nd & ~have;
+                }
+                // lanes of lower warp lanes win: each lane keeps the bits no
+                // earlier neighbour in this batch already delivered
+                const ull mine = fu & ~warp_excl_or(fu);
+                if (mine) { write_lanes(p, vo, mine, new_level, u); }
+                have |= warp_or(fu);
+            }
+            if (lane == owner) { got = have; }
+        }
+        const bool gained = got != 0;
+        if (gained) {
+            p.F[nxt][v] = got;
+            loc.lanes += __popcll(got);
+            if (((p.all & ~need) | got) == p.all) { loc.done_degsum += (ull)(end - beg); }
+        }
+        ms_append(p, acc, nxt, gained, v, end - beg, loc);
+    }
+}
+
+template <int BLOCK>
+struct MsShared {
+    ull red[4][BLOCK / 32];
+    int is_last;
+    unsigned gen;
+    int exit_flag;
+};
+
+__device__ void ms_choose(MsCtrl *c, const MsParams &p)
+{
+    if (c->f_count == 0) {
+        c->dir = kMsDone;
+    } else if (p.force_dir >= 0) {
+        c->dir = p.force_dir;
+    } else {
+        // pull once the frontier's edges are a sizeable share of the edges
+        // still able to deliver a lane (Beamer's alpha test over the batch)
+        c->dir = (c->f_degsum * p.alpha > c->arcs_left) ? kPull : kPush;
+    }
+}
+
+__device__ void ms_finish_step(MsCtrl *c, const MsParams &p)
+{
+    const int s = c->step;
+    volatile MsAcc *a = &c->acc[s & 1];
+    const long long now = globaltimer();
+    const long long found = (long long)a->vertices;
+    if (s < p.rec_cap) {
+        bd_step r;
+        r.dir = c->dir;
+        r.level = c->level;
+        r.frontier = c->f_count;
+        r.frontier_edges = c->f_degsum;
+        r.unexplored_edges = c->arcs_left;
+        r.found = (long long)a->lanes;
+        r.ns = now - c->t_last;
+        p.rec[s] = r;
+    }
+    c->lanes_total += (long long)a->lanes;
+    c->arcs_left -= (long long)a->done_degsum;
+    c->p_small = c->f_small;
+    c->p_large = c->f_large;
+    c->f_count = found;
+    c->f_degsum = (long long)a->degsum;
+    c->f_small = (long long)a->small_cnt;
+    c->f_large = (long long)(a->large_packed >> kLargeShift);
+    c->f_chunks = (long long)(a->large_packed & kChunkMask);
+    if (c->dir == kPush) { c->push_steps += 1; } else { c->pull_steps += 1; }
+    c->level += 1;
+    MsAcc *z = &c->acc[(s + 1) & 1];
+    z->vertices = z->degsum = z->lanes = z->small_cnt = z->large_packed = z->done_degsum = 0;
+    c->step = s + 1;
+    c->t_last = now;
+    ms_choose(c, p);
+}
+
+template <int BLOCK>
+__device__ void ms_barrier(const MsParams &p, MsShared<BLOCK> &sh)
+{
+    MsCtrl *c = p.ctrl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = ld_acquire(&c->bar_gen);
+        __threadfence();
+        const unsigned prev = atomicAdd(&c->bar_count, 1u);
+        sh.is_last = (prev == p.expected_ctas - 1);
+        sh.gen = gen;
+        if (sh.is_last) {
+            __threadfence();
+            ms_finish_step(c, p);
+            atomicExch(&c->bar_count, 0u);
+            __threadfence();
+            st_release(&c->bar_gen, gen + 1);
+        } else {
+            long long it = 0;
+            while (ld_acquire(&c->bar_gen) == gen) {
+                if (++it > p.spin_limit) {
+                    atomicExch(&c->error, (int)BD_ERR_TIMEOUT);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int BLOCK>
+__device__ void ms_publish(const MsParams &p, const MsView &sv, MsShared<BLOCK> &sh, MsLocal &loc)
+{
+    const int lane = lane_id(), warp = threadIdx.x >> 5;
+    ull a = warp_sum(loc.vertices), b = warp_sum(loc.degsum), cc = warp_sum(loc.lanes),
+        d = warp_sum(loc.done_degsum);
+    if (lane == 0) {
+        sh.red[0][warp] = a;
+        sh.red[1][warp] = b;
+        sh.red[2][warp] = cc;
+        sh.red[3][warp] = d;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        ull t = 0;
+        for (int i = 0; i < BLOCK / 32; ++i) { t += sh.red[threadIdx.x][i]; }
+        MsAcc *acc = &p.ctrl->acc[sv.step & 1];
+        ull *dst = threadIdx.x == 0 ? &acc->vertices
+                   : threadIdx.x == 1 ? &acc->degsum
+                   : threadIdx.x == 2 ? &acc->lanes
+                                      : &acc->done_degsum;
+        if (t) { atomicAdd(dst, t); }
+    }
+    loc = MsLocal{0, 0, 0, 0};
+}
+
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) msbfs_kernel(MsParams p)
+{
+    __shared__ MsShared<BLOCK> sh;
+    MsCtrl *c = p.ctrl;
+    if (blockIdx.x == 0 && threadIdx.x == 0) { c->t_last = globaltimer(); }
+    MsLocal loc{0, 0, 0, 0};
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const volatile MsCtrl *vc = c;
+            sh.exit_flag = (vc->error != 0) || (vc->dir == kMsDone);
+        }
+        __syncthreads();
+        if (sh.exit_flag) { break; }
+        const MsView sv = ms_view(c);
+        ms_clear_old(p, sv);
+        if (sv.dir == kPush) {
+            ms_push_step<BLOCK>(p, sv, loc);
+        } else {
+            ms_pull_step<BLOCK>(p, sv, loc);
+        }
+        ms_publish<BLOCK>(p, sv, sh, loc);
+        ms_barrier<BLOCK>(p, sh);
+    }
+}
+
+// Sources: lane r starts at sources[r].  One thread (sources are few).
+__global__ void ms_init_kernel(MsParams p, const int64_t *sources, int count)
+{
+    MsCtrl *c = p.ctrl;
+    memset(c, 0, sizeof(MsCtrl));
+    long long nsmall = 0, nf = 0, degsum = 0, done = 0;
+    ull lp = 0;
+    for (int r = 0; r < count; ++r) {
+        const uint32_t s = (uint32_t)sources[r];
+        const ull bit = 1ull << r;
+        const ull before = p.F[0][s];
+        p.F[0][s] = before | bit;
+        p.seen[s] |= bit;
+        p.depth[(int64_t)s * p.R + r] = 0;
+        p.parent[(int64_t)s * p.R + r] = s;
+        const int64_t deg = p.off[s + 1] - p.off[s];
+        if (p.seen[s] == p.all) { done += deg; }
+        if (before) { continue; }
+        nf += 1;
+        degsum += deg;
+        if (deg >= (int64_t)p.large_deg) {
+            const ull pos = lp >> kLargeShift;
+            p.ql[0][pos] = s;
+            p.qlb[0][pos] = lp & kChunkMask;
+            lp += (1ull << kLargeShift) | (ull)((deg + p.chunk - 1) / p.chunk);
+        } else {
+            p.qs[0][nsmall++] = s;
+        }
+    }
+    c->f_count = nf;
+    c->f_degsum = degsum;
+    c->f_small = nsmall;
+    c->f_large = (long long)(lp >> kLargeShift);
+    c->f_chunks = (long long)(lp & kChunkMask);
+    c->arcs_left = 2 * p.m - done;
+    c->lanes_total = count;
+    ms_choose(c, p);
+}
+
+// Per-lane reached count and degree sum (count_num_traversed_edges per root).
+__global__ void ms_count_kernel(const ull *seen, const int64_t *off, int64_t n, ull all, int R,
+                                unsigned long long *out /* [2][64]: reached, degsum */)
+{
+    __shared__ unsigned long long s_cnt[64], s_deg[64];
+    __shared__ unsigned long long s_full_cnt, s_full_deg;
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) { s_cnt[i] = s_deg[i] = 0; }
+    if (threadIdx.x == 0) { s_full_cnt = s_full_deg = 0; }
+    __syncthreads();
+    ull full_cnt = 0, full_deg = 0;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        ull s = seen[v] & all;
+        if (!s) { continue; }
+        const int64_t d = off[v + 1] - off[v];
+        if (s == all) {
+            full_cnt += 1;
+            full_deg += (ull)d;
+            continue;
+        }
+        while (s) {
+            const int r = __ffsll((long long)s) - 1;
+            s &= s - 1;
+            atomicAdd(&s_cnt[r], 1ull);
+            atomicAdd(&s_deg[r], (ull)d);
+        }
+    }
+    full_cnt = warp_sum(full_cnt);
+    full_deg = warp_sum(full_deg);
+    if (lane_id() == 0) {
+        atomicAdd(&s_full_cnt, full_cnt);
+        atomicAdd(&s_full_deg, full_deg);
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        const ull c = s_cnt[r] + s_full_cnt, dg = s_deg[r] + s_full_deg;
+        if (c) { atomicAdd(&out[r], c); }
+        if (dg) { atomicAdd(&out[64 + r], dg); }
+    }
+}
+
+// Lane r's depth / parent rows, widened to the single-source output format.
+// A lane's entries are valid only where its seen bit is set; the rest read
+// as unreached, so the output rows never need clearing.
+__global__ void ms_extract_kernel(const int32_t *depth, const uint32_t *parent, const ull *seen,
+                                  const int64_t *off, int64_t n, int R, int r, int32_t *depth_out,
+                                  int64_t *parent_out)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = ((seen[v] >> r) & 1ull) ? depth[v * R + r] : -1;
+        if (depth_out) { depth_out[v] = d; }
+        if (parent_out) {
+            if (d >= 0) {
+                parent_out[v] = (int64_t)parent[v * R + r];
+            } else {
+                const int64_t g = off[v + 1] - off[v];
+                parent_out[v] = g != 0 ? -g : -1;
+            }
+        }
+    }
+}
+
+using MsKernel = void (*)(MsParams);
+
+int ms_grid_for(int64_t items)
+{
+    int64_t b = (items + 255) / 256;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 32));
+}
+
+}  // namespace
+}  // namespace bd
+
+using namespace bd;
+
+struct bd_msbfs {
+    bd_graph *g = nullptr;
+    int device = 0;
+    int R = 64;          // lanes per group (= lane stride of the output rows)
+    int groups = 1;      // result slices
+    int max_roots = 64;
+    bd_msbfs_opts opts{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ull *seen = nullptr;         // [groups][n]: a group's final words mark its valid lanes
+    ull *F[3] = {nullptr, nullptr, nullptr};
+    uint32_t *qs[3] = {nullptr, nullptr, nullptr};
+    uint32_t *ql[3] = {nullptr, nullptr, nullptr};
+    ull *qlb[3] = {nullptr, nullptr, nullptr};
+    int32_t *depth = nullptr;    // [groups][n][R]
+    uint32_t *parent = nullptr;  // [groups][n][R]
+    MsCtrl *ctrl = nullptr;
+    bd_step *rec = nullptr;
+    int64_t *d_sources = nullptr;         // [max_roots]
+    unsigned long long *d_counts = nullptr;  // [groups][128]
+    int64_t cap_large = 0;
+    int grid = 0;
+    int block = 512;
+    int count = 0;  // roots in the last run
+    bool ran = false;
+    cudaGraphExec_t graph = nullptr;
+    int graph_count = -1;
+    bool graph_ok = true;
+    MsCtrl last{};
+    std::vector<unsigned long long> counts;
+};
+
+namespace bd {
+namespace {
+
+MsKernel ms_pick(int block)
+{
+    switch (block) {
+        case 256: return msbfs_kernel<256, 4>;
+        case 1024: return msbfs_kernel<1024, 1>;
+        default: return msbfs_kernel<512, 2>;
+    }
+}
+
+MsParams ms_params(bd_msbfs *b, int group, int count)
+{
+    MsParams p{};
+    p.off = b->g->d_off;
+    p.adj = b->g->d_adj;
+    p.isolated = b->g->d_isolated;
+    p.n = b->g->n;
+    p.m = b->g->m;
+    p.seen = b->seen + group * b->g->n;
+    for (int i = 0; i < 3; ++i) {
+        p.F[i] = b->F[i];
+        p.qs[i] = b->qs[i];
+        p.ql[i] = b->ql[i];
+        p.qlb[i] = b->qlb[i];
+    }
+    const int64_t slice = b->g->n * (int64_t)b->R;
+    p.depth = b->depth + group * slice;
+    p.parent = b->parent + group * slice;
+    p.R = b->R;
+    p.all = count >= 64 ? ~0ull : ((1ull << count) - 1);
+    p.ctrl = b->ctrl;
+    p.rec = b->rec;
+    p.rec_cap = kMsRecCap;
+    p.alpha = b->opts.alpha;
+    p.large_deg = (uint32_t)b->opts.large_degree;
+    p.chunk = (uint32_t)b->opts.chunk_edges;
+    p.prefix = b->opts.pull_prefix;
+    p.spin_limit = b->opts.spin_limit;
+    p.expected_ctas = (unsigned)b->grid;
+    p.force_dir = b->opts.force_dir;
+    return p;
+}
+
+// One group: clear (its seen words, the frontier words), init, the
+// persistent kernel, the per-lane counts.
+bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
+{
+    const int64_t n = b->g->n;
+    BD_CUDA(cudaMemsetAsync(b->seen + group * n, 0, sizeof(ull) * n, b->stream));
+    for (int i = 0; i < 3; ++i) { BD_CUDA(cudaMemsetAsync(b->F[i], 0, sizeof(ull) * n, b->stream)); }
+    MsParams p = ms_params(b, group, count);
+    ms_init_kernel<<<1, 1, 0, b->stream>>>(p, b->d_sources + group * 64, count);
+    BD_CUDA(cudaGetLastError());
+    void *args[] = {&p};
+    BD_CUDA(cudaLaunchCooperativeKernel((const void *)ms_pick(b->block), dim3(b->grid),
+                                        dim3(b->block), args, 0, b->stream));
+    unsigned long long *dst = b->d_counts + 128 * group;
+    BD_CUDA(cudaMemsetAsync(dst, 0, sizeof(unsigned long long) * 128, b->stream));
+    ms_count_kernel<<<148 * 8, 256, 0, b->stream>>>(p.seen, b->g->d_off, n, p.all, count, dst);
+    BD_CUDA(cudaGetLastError());
+    return BD_OK;
+}
+
+bd_status ms_enqueue_all(bd_msbfs *b, int count)
+{
+    for (int gi = 0; gi * 64 < count; ++gi) {
+        BD_TRY(ms_enqueue_group(b, gi, std::min(64, count - gi * 64)));
+    }
+    return BD_OK;
+}
+
+// Captures the groups of a `count`-root call into one CUDA graph (once per
+// count); falls back to plain stream launches if capture is refused.
+bd_status ms_launch(bd_msbfs *b, int count)
+{
+    if (b->opts.use_graph && b->graph_ok) {
+        if (b->graph_count != count) {
+            if (b->graph) {
+                cudaGraphExecDestroy(b->graph);
+                b->graph = nullptr;
+            }
+            cudaGraph_t gr = nullptr;
+            if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                bd_status st = ms_enqueue_all(b, count);
+                cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
+                if (st == BD_OK && e == cudaSuccess &&
+                    cudaGraphInstantiate(&b->graph, gr, 0) == cudaSuccess) {
+                    b->graph_count = count;
+                } else {
+                    b->graph = nullptr;
+                    b->graph_ok = false;
+                }
+                if (gr) { cudaGraphDestroy(gr); }
+            } else {
+                b->graph_ok = false;
+            }
+            cudaGetLastError();  // a refused capture leaves no sticky error
+        }
+        if (b->graph) {
+            BD_CUDA(cudaGraphLaunch(b->graph, b->stream));
+            return BD_OK;
+        }
+    }
+    return ms_enqueue_all(b, count);
+}
+
+void ms_free(bd_msbfs *b)
+{
+    if (!b) { return; }
+    cudaSetDevice(b->device);
+    if (b->stream) { cudaStreamSynchronize(b->stream); }
+    if (b->graph) { cudaGraphExecDestroy(b->graph); }
+    cudaFree(b->seen);
+    for (int i = 0; i < 3; ++i) {
+        cudaFree(b->F[i]);
+        cudaFree(b->qs[i]);
+        cudaFree(b->ql[i]);
+        cudaFree(b->qlb[i]);
+    }
+    cudaFree(b->depth);
+    cudaFree(b->parent);
+    cudaFree(b->ctrl);
+    cudaFree(b->rec);
+    cudaFree(b->d_sources);
+    cudaFree(b->d_counts);
+    if (b->ev0) { cudaEventDestroy(b->ev0); }
+    if (b->ev1) { cudaEventDestroy(b->ev1); }
+    if (b->stream) { cudaStreamDestroy(b->stream); }
+    delete b;
+}
+
+bd_status ms_check_root(bd_msbfs *b, int32_t root_index)
+{
+    if (!b->ran) { return BD_ERR_STATE; }
+    if (root_index < 0 || root_index >= b->count) { return BD_ERR_RANGE; }
+    return BD_OK;
+}
+
+bd_status ms_extract(bd_msbfs *b, int32_t root_index, int32_t *depth, int64_t *parent)
+{
+    BD_TRY(ms_check_root(b, root_index));
+    BD_CUDA(cudaSetDevice(b->device));
+    const int64_t n = b->g->n;
+    const int group = root_index / 64, lane = root_index % 64;
+    const int64_t slice = n * (int64_t)b->R;
+    void *tmp = nullptr;
+    const size_t bytes = depth ? sizeof(int32_t) * n : sizeof(int64_t) * n;
+    BD_CUDA(cudaMalloc(&tmp, bytes));
+    ms_extract_kernel<<<ms_grid_for(n), 256, 0, b->stream>>>(
+        b->depth + group * slice, b->parent + group * slice, b->seen + group * n, b->g->d_off, n,
+        b->R, lane,
+        depth ? static_cast<int32_t *>(tmp) : nullptr, parent ? static_cast<int64_t *>(tmp) : nullptr);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(depth ? (void *)depth : (void *)parent, tmp, bytes,
+                            cudaMemcpyDeviceToHost, b->stream);
+    }
+    if (e == cudaSuccess) { e = cudaStreamSynchronize(b->stream); }
+    cudaFree(tmp);
+    if (e != cudaSuccess) { return cuda_fail(e, "msbfs extract", __FILE__, __LINE__); }
+    return BD_OK;
+}
+
+}  // namespace
+}  // namespace bd
+
+extern "C" {
+
+void bd_msbfs_default_opts(bd_msbfs_opts *o)
+{
+    if (!o) { return; }
+    memset(o, 0, sizeof(*o));
+    o->alpha = 4;
+    o->force_dir = -1;
+    o->use_graph = 1;
+}
+
+bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *opts,
+                          bd_msbfs **out)
+{
+    if (!g || !out || max_roots < 1 || max_roots > 65536) { return BD_ERR_INVALID; }
+    bd_msbfs_opts o;
+    bd_msbfs_default_opts(&o);
+    if (opts) { o = *opts; }
+    if (o.alpha <= 0 || o.force_dir < -1 || o.force_dir > 1) { return BD_ERR_INVALID; }
+    if (o.block_size == 0) { o.block_size = 512; }
+    if (o.block_size != 256 && o.block_size != 512 && o.block_size != 1024) { return BD_ERR_INVALID; }
+    if (o.large_degree <= 0) { o.large_degree = 1024; }
+    if (o.large_degree > (1 << 20)) { return BD_ERR_INVALID; }
+    if (o.chunk_edges <= 0) { o.chunk_edges = 1024; }
+    if (o.pull_prefix <= 0) { o.pull_prefix = 16; }
+    if (o.spin_limit <= 0) { o.spin_limit = kMsDefaultSpin; }
+    if (g->n > (int64_t)UINT32_MAX) { return BD_ERR_LIMIT; }
+    BD_TRY(ensure_device());
+    auto *b = new bd_msbfs();
+    b->g = g;
+    b->device = current_device();
+    b->max_roots = max_roots;
+    b->R = std::min(64, (int)max_roots);
+    b->groups = (max_roots + 63) / 64;
+    b->opts = o;
+    b->block = o.block_size;
+    const int64_t n = g->n;
+    b->cap_large = std::min<int64_t>(n, g->arcs / o.large_degree + 1);
+    auto fail = [&](bd_status st) { ms_free(b); return st; };
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+        return fail(BD_ERR_CUDA);
+    }
+    const size_t slots = (size_t)n * b->R * b->groups;
+    bool ok = cudaMalloc(&b->seen, sizeof(ull) * n * b->groups) == cudaSuccess &&
+              cudaMalloc(&b->depth, sizeof(int32_t) * slots) == cudaSuccess &&
+              cudaMalloc(&b->parent, sizeof(uint32_t) * slots) == cudaSuccess &&
+              cudaMalloc(&b->ctrl, sizeof(MsCtrl)) == cudaSuccess &&
+              cudaMalloc(&b->rec, sizeof(bd_step) * kMsRecCap) == cudaSuccess &&
+              cudaMalloc(&b->d_sources, sizeof(int64_t) * 64 * b->groups) == cudaSuccess &&
+              cudaMalloc(&b->d_counts, sizeof(unsigned long long) * 128 * b->groups) == cudaSuccess;
+    for (int i = 0; i < 3 && ok; ++i) {
+        ok = cudaMalloc(&b->F[i], sizeof(ull) * n) == cudaSuccess &&
+             cudaMalloc(&b->qs[i], sizeof(uint32_t) * n) == cudaSuccess &&
+             cudaMalloc(&b->ql[i], sizeof(uint32_t) * b->cap_large) == cudaSuccess &&
+             cudaMalloc(&b->qlb[i], sizeof(ull) * b->cap_large) == cudaSuccess;
+    }
+    if (!ok) { return fail(BD_ERR_OOM); }
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)ms_pick(b->block),
+                                                      b->block, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess ||
+        per_sm < 1) {
+        return fail(BD_ERR_CUDA);
+    }
+    b->grid = per_sm * sms;
+    *out = b;
+    return BD_OK;
+}
+
+bd_status bd_msbfs_run(bd_msbfs *b, const int64_t *sources, int32_t count, bd_run_stats *stats)
+{
+    if (!b || !sources || count < 1 || count > b->max_roots) { return BD_ERR_INVALID; }
+    for (int i = 0; i < count; ++i) {
+        if (sources[i] < 0 || sources[i] >= b->g->n) { return BD_ERR_RANGE; }
+    }
+    BD_CUDA(cudaSetDevice(b->device));
+    // group g's sources start at d_sources + 64 g
+    std::vector<int64_t> padded((size_t)64 * b->groups, 0);
+    for (int i = 0; i < count; ++i) { padded[(size_t)(i / 64) * 64 + i % 64] = sources[i]; }
+    BD_CUDA(cudaMemcpyAsync(b->d_sources, padded.data(), sizeof(int64_t) * padded.size(),
+                            cudaMemcpyHostToDevice, b->stream));
+    BD_CUDA(cudaEventRecord(b->ev0, b->stream));
+    BD_TRY(ms_launch(b, count));
+    BD_CUDA(cudaEventRecord(b->ev1, b->stream));
+    const int used = (count + 63) / 64;
+    b->counts.assign((size_t)128 * used, 0);
+    BD_CUDA(cudaMemcpyAsync(b->counts.data(), b->d_counts, sizeof(unsigned long long) * 128 * used,
+                            cudaMemcpyDeviceToHost, b->stream));
+    BD_CUDA(cudaMemcpyAsync(&b->last, b->ctrl, sizeof(MsCtrl), cudaMemcpyDeviceToHost, b->stream));
+    BD_CUDA(cudaStreamSynchronize(b->stream));
+    b->count = count;
+    b->ran = true;
+    if (b->last.error) { return (bd_status)b->last.error; }
+    if (stats) {
+        float ms = 0.f;
+        BD_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+        stats->ms = ms;
+        stats->num_steps = b->last.step;
+        int64_t edges = 0, reached = 0;
+        for (int i = 0; i < count; ++i) {
+            const size_t base = (size_t)(i / 64) * 128;
+            edges += (int64_t)(b->counts[base + 64 + i % 64] / 2);
+            reached += (int64_t)b->counts[base + i % 64];
+        }
+        stats->traversed_edges = edges;
+        stats->reached = reached;
+        stats->top_down_steps = b->last.push_steps;
+        stats->bottom_up_steps = b->last.pull_steps;
+    }
+    return BD_OK;
+}
+
+bd_status bd_msbfs_get_depths(bd_msbfs *b, int32_t root_index, int32_t *depth)
+{
+    if (!b || !depth) { return BD_ERR_INVALID; }
+    return ms_extract(b, root_index, depth, nullptr);
+}
+
+bd_status bd_msbfs_get_parents(bd_msbfs *b, int32_t root_index, int64_t *parent)
+{
+    if (!b || !parent) { return BD_ERR_INVALID; }
+    return ms_extract(b, root_index, nullptr, parent);
+}
+
+bd_status bd_msbfs_count_traversed_edges(bd_msbfs *b, int32_t root_index, int64_t *edges,
+                                         int64_t *reached)
+{
+    if (!b) { return BD_ERR_INVALID; }
+    BD_TRY(ms_check_root(b, root_index));
+    const size_t base = (size_t)(root_index / 64) * 128;
+    if (edges) { *edges = (int64_t)(b->counts[base + 64 + root_index % 64] / 2); }
+    if (reached) { *reached = (int64_t)b->counts[base + root_index % 64]; }
+    return BD_OK;
+}
+
+bd_status bd_msbfs_get_steps(bd_msbfs *b, bd_step *steps, int64_t capacity, int64_t *count)
+{
+    if (!b || !count || capacity < 0 || (!steps && capacity)) { return BD_ERR_INVALID; }
+    if (!b->ran) { return BD_ERR_STATE; }
+    const int64_t have = std::min<int64_t>(b->last.step, kMsRecCap);
+    const int64_t take = std::min(have, capacity);
+    if (take) {
+        BD_CUDA(cudaSetDevice(b->device));
+        BD_CUDA(cudaMemcpy(steps, b->rec, sizeof(bd_step) * take, cudaMemcpyDeviceToHost));
+    }
+    *count = have;
+    return BD_OK;
+}
+
+bd_status bd_msbfs_destroy(bd_msbfs *b)
+{
+    if (!b) { return BD_ERR_INVALID; }
+    ms_free(b);
+    return BD_OK;
+}
+
+}  // extern "C"

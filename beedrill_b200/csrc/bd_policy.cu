@@ -281,7 +281,7 @@ bd_status bd_policy_train(float *params, const float *x, const int32_t *label, c
 }
 
 bd_status bd_bfs_set_policy(bd_bfs *b, const float *params, const float *mean,
-                            const float *inv_std, float margin)
+                            const float *inv_std, const float *lo, const float *hi, float margin)
 {
     if (!b) { return BD_ERR_INVALID; }
     if (!params) { return bfs_install_policy(b, nullptr); }
@@ -291,6 +291,10 @@ bd_status bd_bfs_set_policy(bd_bfs *b, const float *params, const float *mean,
     memcpy(&blob, params, sizeof(float) * kP);
     memcpy(blob.mean, mean, sizeof(float) * kPolicyIn);
     memcpy(blob.inv_std, inv_std, sizeof(float) * kPolicyIn);
+    for (int i = 0; i < kPolicyIn; ++i) {
+        blob.lo[i] = lo ? lo[i] : -INFINITY;
+        blob.hi[i] = hi ? hi[i] : INFINITY;
+    }
     blob.margin = margin;
     return bfs_install_policy(b, &blob);
 }

@@ -153,6 +153,13 @@ class Policy:
     inv_std: np.ndarray
     margin: float = 0.0
     info: dict = field(default_factory=dict)
+    lo: np.ndarray | None = None  # trusted raw-feature range (None: unbounded)
+    hi: np.ndarray | None = None
+
+    def trusts(self, raw: np.ndarray) -> bool:
+        if self.lo is None:
+            return True
+        return bool(np.all(raw >= self.lo) and np.all(raw <= self.hi))
 
     def logits(self, raw: np.ndarray) -> np.ndarray:
         """Host float32 forward pass (for simulation only; the BFS uses the
@@ -169,21 +176,28 @@ class Policy:
     def save(self, path: str) -> None:
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
         with open(path, "w") as f:
-            json.dump({"params": [float(v) for v in self.params],
-                       "mean": [float(v) for v in self.mean],
-                       "inv_std": [float(v) for v in self.inv_std],
-                       "margin": float(self.margin), "info": self.info}, f)
+            d = {"params": [float(v) for v in self.params],
+                 "mean": [float(v) for v in self.mean],
+                 "inv_std": [float(v) for v in self.inv_std],
+                 "margin": float(self.margin), "info": self.info}
+            if self.lo is not None:
+                d["lo"] = [float(v) for v in self.lo]
+                d["hi"] = [float(v) for v in self.hi]
+            json.dump(d, f)
             f.write("\n")
 
     @classmethod
     def load(cls, path: str = DEFAULT_PATH) -> "Policy":
         with open(path) as f:
             d = json.load(f)
+        lo = np.array(d["lo"], np.float32) if "lo" in d else None
+        hi = np.array(d["hi"], np.float32) if "hi" in d else None
         return cls(np.array(d["params"], np.float32), np.array(d["mean"], np.float32),
-                   np.array(d["inv_std"], np.float32), float(d["margin"]), d.get("info", {}))
+                   np.array(d["inv_std"], np.float32), float(d["margin"]), d.get("info", {}),
+                   lo, hi)
 
     def install(self, bfs: "bd.HybridBFS") -> None:
-        bfs.set_policy(self.params, self.mean, self.inv_std, self.margin)
+        bfs.set_policy(self.params, self.mean, self.inv_std, self.margin, self.lo, self.hi)
 
 
 def beamer_dirs(tab: LevelTable, alpha=15, beta=18) -> str:
@@ -217,9 +231,11 @@ def policy_dirs(policy: Policy, tab: LevelTable, alpha=15, beta=18) -> str:
     out = []
     prev_dir, prev_ns = 0, 0.0
     for lv in range(tab.levels):
-        z = policy.logits(tab.features(lv, prev_dir, prev_ns))[0]
+        raw = tab.features(lv, prev_dir, prev_ns)
+        z = policy.logits(raw)[0]
         gap = float(z[1] - z[0])
-        d = ("B" if gap > 0 else "T") if abs(gap) >= policy.margin else rule[lv]
+        trusted = policy.trusts(raw) and abs(gap) >= policy.margin
+        d = ("B" if gap > 0 else "T") if trusted else rule[lv]
         out.append(d)
         prev_dir = 1 if d == "B" else 0
         prev_ns = tab.t_bu[lv] if d == "B" else tab.t_td[lv]
@@ -251,7 +267,10 @@ def fit(X, y, w, epochs=3000, lr=3e-3, weight_decay=1e-4, seed=0):
     Xs = ((X - mean) * inv_std).astype(np.float32)
     params = he_init(seed)
     hist = bd.policy_train(params, Xs, y, w, epochs, lr, weight_decay)
-    return Policy(params, mean, inv_std, 0.0), hist
+    # trusted range: the training extremes widened by 3 standard deviations
+    lo = (X.min(0) - 3 * std).astype(np.float32)
+    hi = (X.max(0) + 3 * std).astype(np.float32)
+    return Policy(params, mean, inv_std, 0.0, {}, lo, hi), hist
 
 
 def training_graph_specs(count=200, seed=2024):

@@ -56,6 +56,8 @@ typedef struct bd_bfs bd_bfs;
 /* Adjacency order inside each vertex's neighbour list. */
 #define BD_ORDER_INSERTION 0 /* reference order: file order, (s->d) then (d->s) */
 #define BD_ORDER_SORTED 1    /* ascending neighbour id                          */
+#define BD_ORDER_DEGREE 2    /* highest-degree neighbour first (ties: insertion
+                                order); bottom-up scans meet visited hubs first */
 
 /* Direction policies (the reference's --algorithm values map onto these). */
 #define BD_ALG_BEAMER 0    /* beamer_hybrid, remote_writes_hybrid                */
@@ -78,6 +80,13 @@ typedef struct bd_bfs_opts {
     int64_t spin_limit;   /* grid-barrier wait bound in polls; 0 = default (~2 s) */
     int32_t test_extra_ctas; /* TEST ONLY: barrier expects this many extra CTAs,
                                 so it can never complete and must time out      */
+    int32_t bu_words;     /* bottom-up: bitmap words in flight per warp: 1, 2, 4
+                             (the warp shares each word), 32 (each lane owns a
+                             word); 0 = tuned default                             */
+    int32_t bu_sparse_words; /* the same once fewer than half of the vertices
+                                of nonzero degree are unvisited; 0 = default.
+                                Pairs available: equal to bu_words, or
+                                (2 or 4, 32)                                     */
     int32_t reserved;
 } bd_bfs_opts;
 
@@ -118,6 +127,12 @@ bd_status bd_graph_from_csr(int64_t num_vertices, int64_t num_arcs, const int64_
  * permuted and edge order shuffled by `seed`. */
 bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, double c,
                         double d, uint64_t seed, int32_t adjacency_order, bd_graph **out);
+/* rows x cols grid, vertex r*cols+c, 4-neighbour edges (horizontal edges
+ * first, row by row, then vertical), each deleted independently with
+ * probability delete_frac by a seeded Philox draw.  The high-diameter
+ * contrast graph of the evaluation (no counterpart in the reference). */
+bd_status bd_graph_grid(int64_t rows, int64_t cols, double delete_frac, uint64_t seed,
+                        int32_t adjacency_order, bd_graph **out);
 /* Disjoint union of graphs: vertex ids of graph i are shifted by the vertex
  * count of graphs 0..i-1.  vertex_base (host, count+1 entries) receives the
  * shifts; may be NULL. */
@@ -200,6 +215,43 @@ bd_status bd_bfs_run_noalloc(const int64_t *d_offsets, const uint32_t *d_adjacen
                              int64_t alpha, int64_t beta, int32_t *d_depth, int64_t *d_parent,
                              void *stream, int64_t *traversed_edges);
 
+/* ---- batched traversal ---------------------------------------------------- */
+/* Many BFSs share each pass over the graph: roots are processed in groups of
+ * up to 64, one bit lane of a uint64 per root (multi-source BFS), one
+ * persistent launch per group; all groups of a call are replayed as one
+ * captured CUDA graph.  Per root the results equal a single-source BFS from
+ * that root (depths bit-exact, parents one level up, m_c).  No counterpart
+ * class in the reference, whose driver loops over roots one at a time
+ * (hybrid_bfs_main.cc:252-302); per-root results are read with the same
+ * encodings as bd_bfs_get_depths / bd_bfs_get_parents. */
+typedef struct bd_msbfs bd_msbfs;
+typedef struct bd_msbfs_opts {
+    int64_t alpha;         /* pull when frontier edges * alpha > edges left; > 0 */
+    int32_t force_dir;     /* -1: rule; 0: push only; 1: pull only              */
+    int32_t block_size;    /* 0 = default (512)                                 */
+    int32_t large_degree;  /* push: degree at which a vertex is split; 0 = def  */
+    int32_t chunk_edges;   /* push: edges per split work unit; 0 = default      */
+    int32_t pull_prefix;   /* pull: arcs a lane scans alone; 0 = default        */
+    int32_t use_graph;     /* 1 (default via bd_msbfs_default_opts): replay the
+                              groups of a call as one captured CUDA graph       */
+    int64_t spin_limit;    /* grid-barrier poll bound; 0 = default (~2 s)       */
+} bd_msbfs_opts;
+void bd_msbfs_default_opts(bd_msbfs_opts *opts);
+/* max_roots: capacity of one call (results of all roots stay readable). */
+bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *opts,
+                          bd_msbfs **out);
+/* BFS from each of sources[0..count); stats (may be NULL): ms = device time
+ * of all groups, traversed_edges = sum of m_c, reached = sum of n_c. */
+bd_status bd_msbfs_run(bd_msbfs *b, const int64_t *sources, int32_t count, bd_run_stats *stats);
+bd_status bd_msbfs_get_depths(bd_msbfs *b, int32_t root_index, int32_t *depth);
+bd_status bd_msbfs_get_parents(bd_msbfs *b, int32_t root_index, int64_t *parent);
+/* count_num_traversed_edges() (m_c) and reached vertices (n_c) of one root. */
+bd_status bd_msbfs_count_traversed_edges(bd_msbfs *b, int32_t root_index, int64_t *edges,
+                                         int64_t *reached);
+/* Step records of the last group of the last call (found = new lanes). */
+bd_status bd_msbfs_get_steps(bd_msbfs *b, bd_step *steps, int64_t capacity, int64_t *count);
+bd_status bd_msbfs_destroy(bd_msbfs *b);
+
 /* ---- learned direction policy -------------------------------------------- */
 /* An fp32 MLP 8 -> 32 (ReLU) -> 32 (ReLU) -> 2 that picks the direction of
  * every step in place of the alpha/beta rule (hybrid_bfs.cc:166-188).
@@ -215,9 +267,12 @@ bd_status bd_bfs_run_noalloc(const int64_t *d_offsets, const uint32_t *d_adjacen
 #define BD_POLICY_PARAMS 1410
 #define BD_POLICY_FEATURES 8
 /* Installs (or, with params == NULL, removes) the policy used by
- * BD_ALG_LEARNED.  Host pointers; copied. */
+ * BD_ALG_LEARNED.  lo / hi (8 floats each, may be NULL for no limit) bound
+ * the raw features the policy is trusted on; outside them the Beamer rule
+ * decides.  Host pointers; copied. */
 bd_status bd_bfs_set_policy(bd_bfs *b, const float *params, const float *mean,
-                            const float *inv_std, float margin);
+                            const float *inv_std, const float *lo, const float *hi,
+                            float margin);
 /* Device forward pass over n standardised feature rows (host buffers). */
 bd_status bd_policy_forward(const float *params, const float *x, int64_t n, float *logits);
 /* Weighted cross-entropy sum_i w_i CE(x_i, label_i) / sum_i w_i and its

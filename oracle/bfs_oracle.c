@@ -581,3 +581,32 @@ int64_t or_rmat_finish(int scale, int64_t num_edges, uint64_t seed,
     free(ek);
     return m;
 }
+
+/* The project's grid generator: edge e (horizontal edges row by row, then
+ * vertical) survives when the top 53 bits of its Philox key, as a fraction
+ * of 2^53, are >= delete_frac.  Returns the number of edges written. */
+int64_t or_grid_edges(int64_t rows, int64_t cols, double delete_frac, uint64_t seed,
+                      int64_t *src, int64_t *dst)
+{
+    const int64_t horiz = rows * (cols - 1);
+    const int64_t total = horiz + (rows - 1) * cols;
+    int64_t m = 0;
+    for (int64_t e = 0; e < total; ++e) {
+        uint64_t k = perm_key(seed, (uint64_t)e, 0x47524944u);
+        double u = (double)(k >> 11) * (1.0 / 9007199254740992.0);
+        if (u < delete_frac) { continue; }
+        int64_t a, b;
+        if (e < horiz) {
+            a = (e / (cols - 1)) * cols + e % (cols - 1);
+            b = a + 1;
+        } else {
+            int64_t f = e - horiz;
+            a = (f / cols) * cols + f % cols;
+            b = a + cols;
+        }
+        src[m] = a;
+        dst[m] = b;
+        ++m;
+    }
+    return m;
+}

@@ -90,6 +90,11 @@ void or_rmat_edges(int scale, int64_t num_edges, double a, double b, double c,
 int64_t or_rmat_finish(int scale, int64_t num_edges, uint64_t seed,
                        int64_t *src, int64_t *dst);
 
+/* The project's grid generator (vertex r*cols+c, 4-neighbour edges, each
+ * deleted with probability delete_frac by a seeded Philox draw). */
+int64_t or_grid_edges(int64_t rows, int64_t cols, double delete_frac, uint64_t seed,
+                      int64_t *src, int64_t *dst);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,6 +63,8 @@ def lib() -> ctypes.CDLL:
         L.or_rmat_edges.restype = None
         L.or_rmat_finish.argtypes = [c_int, c_int64, c_uint64, i64p, i64p]
         L.or_rmat_finish.restype = c_int64
+        L.or_grid_edges.argtypes = [c_int64, c_int64, c_double, c_uint64, i64p, i64p]
+        L.or_grid_edges.restype = c_int64
         _lib = L
     return _lib
 
@@ -218,6 +220,15 @@ def rmat_graph(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, d=0.05
     if m < 0:
         raise MemoryError("oracle generator allocation failed")
     return 1 << scale, src[:m].copy(), dst[:m].copy()
+
+
+def grid_graph(rows: int, cols: int, delete_frac: float = 0.01, seed: int = 0):
+    """Edge list of the project's seeded grid graph: (n, src, dst)."""
+    total = rows * (cols - 1) + (rows - 1) * cols
+    src = np.empty(max(total, 1), np.int64)
+    dst = np.empty(max(total, 1), np.int64)
+    m = lib().or_grid_edges(rows, cols, delete_frac, seed, _p(src, c_int64), _p(dst, c_int64))
+    return rows * cols, src[:m].copy(), dst[:m].copy()
 
 
 def depth_from_parents(parent: np.ndarray, source: int) -> np.ndarray:

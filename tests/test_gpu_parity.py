@@ -253,3 +253,30 @@ def test_barrier_timeout_is_reported_and_recoverable():
     bfs = bd.HybridBFS(g)
     bfs.run(root)
     assert np.array_equal(bfs.depths(), O.bfs_depth(off, adj, root))
+
+
+def test_degree_order_lists_and_results():
+    g = bd.Graph.rmat(14, seed=15, order=bd.ORDER_DEGREE)
+    ref = bd.Graph.rmat(14, seed=15)
+    off, adj = g.csr()
+    roff, radj = ref.csr()
+    assert np.array_equal(off, roff)
+    deg = np.diff(off)
+    for v in range(0, len(off) - 1, 97):
+        lst = adj[off[v]:off[v + 1]]
+        assert np.array_equal(np.sort(lst), np.sort(radj[roff[v]:roff[v + 1]]))
+        assert np.all(np.diff(deg[lst]) <= 0)
+    m = g.num_edges()
+    for alg in ("beamer_hybrid", "bottom_up", "top_down"):
+        bfs = bd.HybridBFS(g, alg=alg)
+        for root in g.pick_roots(0, 3):
+            root = int(root)
+            bfs.clear()
+            bfs.run(root)
+            _assert_run_matches(bfs, off, adj, m, root, alg)
+    ms = bd.BatchedBFS(g, 64)
+    roots = g.pick_roots(1, 64)
+    ms.run(roots)
+    for i in range(0, 64, 9):
+        assert np.array_equal(ms.depths(i), O.bfs_depth(off, adj, int(roots[i])))
+        assert O.check(off, adj, int(roots[i]), ms.parents(i))
