@@ -84,7 +84,8 @@ class MsBfsOpts(Structure):
     _fields_ = [
         ("alpha", c_int64), ("force_dir", c_int32), ("block_size", c_int32),
         ("large_degree", c_int32), ("chunk_edges", c_int32), ("pull_prefix", c_int32),
-        ("use_graph", c_int32), ("spin_limit", c_int64),
+        ("use_graph", c_int32), ("spin_limit", c_int64), ("heavy_degree", c_int32),
+        ("heavy_chunk", c_int32),
     ]
 
 
@@ -165,6 +166,7 @@ def lib() -> ctypes.CDLL:
         "bd_msbfs_count_traversed_edges": (c_int, [c_void_p, c_int32, i64p, i64p]),
         "bd_msbfs_get_steps": (c_int, [c_void_p, POINTER(Step), c_int64, i64p]),
         "bd_msbfs_destroy": (c_int, [c_void_p]),
+        "bd_msbfs_set_policy": (c_int, [c_void_p, f32p, f32p, f32p, f32p, f32p, c_float]),
         "bd_policy_forward": (c_int, [f32p, f32p, c_int64, f32p]),
         "bd_policy_loss_grad": (c_int, [f32p, f32p, i32p, f32p, c_int64, f32p, f32p]),
         "bd_policy_train": (c_int, [f32p, f32p, i32p, f32p, c_int64, c_int32, c_float, c_float,
@@ -192,6 +194,24 @@ def _check(status: int, what: str) -> None:
 
 def _ptr(a: np.ndarray, ct):
     return a.ctypes.data_as(POINTER(ct))
+
+
+def _set_policy(fn, handle, params, mean, inv_std, margin, lo, hi) -> None:
+    if params is None:
+        _check(fn(handle, None, None, None, None, None, 0.0), "set_policy")
+        return
+    lo_p = hi_p = None
+    if lo is not None:
+        lo_a = np.ascontiguousarray(lo, np.float32)
+        hi_a = np.ascontiguousarray(hi, np.float32)
+        lo_p, hi_p = _ptr(lo_a, c_float), _ptr(hi_a, c_float)
+    p = np.ascontiguousarray(params, np.float32)
+    mu = np.ascontiguousarray(mean, np.float32)
+    isd = np.ascontiguousarray(inv_std, np.float32)
+    if p.size != 1410 or mu.size != 8 or isd.size != 8:
+        raise ValueError("policy shapes: 1410 params, 8 means, 8 inverse std devs")
+    _check(fn(handle, _ptr(p, c_float), _ptr(mu, c_float), _ptr(isd, c_float), lo_p, hi_p,
+              margin), "set_policy")
 
 
 class Graph:
@@ -445,22 +465,7 @@ class HybridBFS:
         """Install the learned direction policy used by alg="learned"
         (params=None removes it; Beamer then decides).  lo / hi bound the raw
         features the policy is trusted on (None: no bound)."""
-        if params is None:
-            _check(lib().bd_bfs_set_policy(self._h, None, None, None, None, None, 0.0),
-                   "set_policy")
-            return
-        lo_p = hi_p = None
-        if lo is not None:
-            lo_a = np.ascontiguousarray(lo, np.float32)
-            hi_a = np.ascontiguousarray(hi, np.float32)
-            lo_p, hi_p = _ptr(lo_a, c_float), _ptr(hi_a, c_float)
-        p = np.ascontiguousarray(params, np.float32)
-        mu = np.ascontiguousarray(mean, np.float32)
-        isd = np.ascontiguousarray(inv_std, np.float32)
-        if p.size != 1410 or mu.size != 8 or isd.size != 8:
-            raise ValueError("policy shapes: 1410 params, 8 means, 8 inverse std devs")
-        _check(lib().bd_bfs_set_policy(self._h, _ptr(p, c_float), _ptr(mu, c_float),
-                                       _ptr(isd, c_float), lo_p, hi_p, margin), "set_policy")
+        _set_policy(lib().bd_bfs_set_policy, self._h, params, mean, inv_std, margin, lo, hi)
 
     def close(self) -> None:
         if self._h is not None and self._h.value:
@@ -482,7 +487,7 @@ class BatchedBFS:
     def __init__(self, graph: Graph, max_roots: int = 64, alpha: int = 0, force_dir: int = -1,
                  use_graph: bool = True, block_size: int = 0, large_degree: int = 0,
                  chunk_edges: int = 0, pull_prefix: int = 0, spin_limit: int = 0,
-                 tuned: bool = True):
+                 heavy_degree: int = 0, heavy_chunk: int = 0, tuned: bool = True):
         if tuned:
             t = tuned_options("batched")
             alpha = alpha or t.get("alpha", 0)
@@ -490,6 +495,8 @@ class BatchedBFS:
             large_degree = large_degree or t.get("large_degree", 0)
             chunk_edges = chunk_edges or t.get("chunk_edges", 0)
             pull_prefix = pull_prefix or t.get("pull_prefix", 0)
+            heavy_degree = heavy_degree or t.get("heavy_degree", 0)
+            heavy_chunk = heavy_chunk or t.get("heavy_chunk", 0)
         self.graph = graph
         o = MsBfsOpts()
         lib().bd_msbfs_default_opts(byref(o))
@@ -499,6 +506,7 @@ class BatchedBFS:
         o.use_graph = int(bool(use_graph))
         o.block_size, o.large_degree, o.chunk_edges = block_size, large_degree, chunk_edges
         o.pull_prefix, o.spin_limit = pull_prefix, spin_limit
+        o.heavy_degree, o.heavy_chunk = heavy_degree, heavy_chunk
         self.max_roots = max_roots
         self._h = c_void_p()
         _check(lib().bd_msbfs_create(graph._h, max_roots, byref(o), byref(self._h)), "msbfs")
@@ -550,6 +558,10 @@ class BatchedBFS:
 
     def directions(self) -> str:
         return "".join("B" if s["dir"] else "T" for s in self.steps())
+
+    def set_policy(self, params, mean, inv_std, margin: float = 0.0, lo=None, hi=None) -> None:
+        """Install the learned push/pull policy (params=None: the rule)."""
+        _set_policy(lib().bd_msbfs_set_policy, self._h, params, mean, inv_std, margin, lo, hi)
 
     def close(self) -> None:
         if self._h is not None and self._h.value:

@@ -45,6 +45,8 @@ BATCHED_SPACE = {
     "large_degree": [32, 128, 1024],
     "chunk_edges": [256, 1024],
     "pull_prefix": [8, 16, 32, 64],
+    "heavy_degree": [1024, 4096, 16384],
+    "heavy_chunk": [512, 2048, 8192],
 }
 
 
@@ -114,7 +116,7 @@ def tune(scale=22, roots=32, seed=22, order=bd.ORDER_DEGREE, log=None):
     single, s_score, s_table = coordinate_descent(
         SINGLE_SPACE, start_single, lambda p: score_single(g, rs, p), log)
     start_batched = {"block_size": 512, "alpha": 4, "large_degree": 1024, "chunk_edges": 1024,
-                     "pull_prefix": 16}
+                     "pull_prefix": 16, "heavy_degree": 4096, "heavy_chunk": 2048}
     batched, b_score, b_table = coordinate_descent(
         BATCHED_SPACE, start_batched, lambda p: score_batched(g, rs[:64], p), log)
     g.close()

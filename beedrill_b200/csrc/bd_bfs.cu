@@ -122,6 +122,27 @@ __device__ __forceinline__ StepView read_view(const Ctrl *c)
 // loads observe all writes made before the barrier (PTX memory model).
 __device__ __forceinline__ uint32_t ld_bits(const uint32_t *p) { return *p; }
 
+// Warp-collective: reserves `count` large-queue slots and `chunks` chunk ids
+// for this lane with one atomic for the whole warp.  Slots and chunk ids are
+// handed out in the same lane order, so chunk bases stay sorted by slot.
+__device__ __forceinline__ void warp_reserve_large(Acc *acc, unsigned count,
+                                                   unsigned long long chunks,
+                                                   unsigned long long &pos,
+                                                   unsigned long long &cbase)
+{
+    const unsigned ci = warp_incl_scan(count);
+    const unsigned long long hi = warp_incl_scan(chunks);
+    const unsigned ct = __shfl_sync(kFull, ci, 31);
+    const unsigned long long ht = __shfl_sync(kFull, hi, 31);
+    unsigned long long old = 0;
+    if (lane_id() == 0 && ct) {
+        old = atomicAdd(&acc->large_packed, ((unsigned long long)ct << kLargeShift) | ht);
+    }
+    old = __shfl_sync(kFull, old, 0);
+    pos = (old >> kLargeShift) + (ci - count);
+    cbase = (old & kChunkMask) + (hi - chunks);
+}
+
 // Warp-collective append of up to K discoveries per lane with one atomic
 // for all the small-degree ones.
 template <int K>
@@ -155,24 +176,24 @@ __device__ __forceinline__ void warp_append_k(const BfsParams &p, Acc *acc, int 
         }
     }
     if (any_large) {
+        unsigned count = 0;
+        unsigned long long chunks = 0;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            const unsigned lm = __ballot_sync(kFull, large[k]);
-            if (!lm) { continue; }
-            const unsigned long long nch =
-                large[k] ? (unsigned long long)((deg[k] + p.chunk - 1) / p.chunk) : 0ull;
-            const unsigned long long incl = warp_incl_scan(nch);
-            const unsigned long long tot = __shfl_sync(kFull, incl, 31);
-            unsigned long long old = 0;
-            if (lane == 0) {
-                old = atomicAdd(&acc->large_packed,
-                                ((unsigned long long)__popc(lm) << kLargeShift) | tot);
-            }
-            old = __shfl_sync(kFull, old, 0);
             if (large[k]) {
-                const unsigned long long pos = (old >> kLargeShift) + __popc(lm & lanemask_lt());
+                count += 1;
+                chunks += (unsigned long long)((deg[k] + p.chunk - 1) / p.chunk);
+            }
+        }
+        unsigned long long pos, cbase;
+        warp_reserve_large(acc, count, chunks, pos, cbase);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (large[k]) {
                 p.ql[qout][pos] = v[k];
-                p.qlb[qout][pos] = (old & kChunkMask) + incl - nch;
+                p.qlb[qout][pos] = cbase;
+                pos += 1;
+                cbase += (unsigned long long)((deg[k] + p.chunk - 1) / p.chunk);
             }
         }
     }
@@ -602,15 +623,23 @@ __device__ void bu_step_lanes(const BfsParams &p, const StepView &sv, Local &loc
                 p.qs[qout][start++] = (uint32_t)(w * 32 + (__ffs(f) - 1));
             }
         }
-        for (uint32_t f = large; f; f &= f - 1) {
-            const uint32_t v = (uint32_t)(w * 32 + (__ffs(f) - 1));
-            const int64_t d = __ldg(&p.off[v + 1]) - __ldg(&p.off[v]);
-            const unsigned long long nch = (unsigned long long)((d + p.chunk - 1) / p.chunk);
-            const unsigned long long old =
-                atomicAdd(&acc->large_packed, (1ull << kLargeShift) | nch);
-            const unsigned long long pos = old >> kLargeShift;
-            p.ql[qout][pos] = v;
-            p.qlb[qout][pos] = old & kChunkMask;
+        if (__any_sync(kFull, large != 0)) {
+            unsigned long long chunks = 0;
+            for (uint32_t f = large; f; f &= f - 1) {
+                const uint32_t v = (uint32_t)(w * 32 + (__ffs(f) - 1));
+                const int64_t d = __ldg(&p.off[v + 1]) - __ldg(&p.off[v]);
+                chunks += (unsigned long long)((d + p.chunk - 1) / p.chunk);
+            }
+            unsigned long long pos, cbase;
+            warp_reserve_large(acc, __popc(large), chunks, pos, cbase);
+            for (uint32_t f = large; f; f &= f - 1) {
+                const uint32_t v = (uint32_t)(w * 32 + (__ffs(f) - 1));
+                const int64_t d = __ldg(&p.off[v + 1]) - __ldg(&p.off[v]);
+                p.ql[qout][pos] = v;
+                p.qlb[qout][pos] = cbase;
+                pos += 1;
+                cbase += (unsigned long long)((d + p.chunk - 1) / p.chunk);
+            }
         }
         loc.found += __popc(found);
         loc.degsum += degsum;
@@ -652,8 +681,6 @@ __device__ void beamer_after_step(Ctrl *c, const BfsParams &p, int dir, long lon
     }
 }
 
-__device__ __forceinline__ float log2p1(double x) { return (float)log2(1.0 + (x > 0 ? x : 0)); }
-
 // Picks the direction of the next step.  Called by one CTA (the last to
 // reach the barrier, or the init kernel) with the frontier already in ctrl.
 template <int BLOCK>
@@ -676,55 +703,25 @@ __device__ void choose_next(Ctrl *c, const BfsParams &p, SharedState<BLOCK> *sh)
         }
         if (sh) {
             sh->beamer_dir = d;
-            const long long m_u = 2 * p.m - c->visited_degsum;
-            sh->feat[0] = log2p1((double)c->f_count);
-            sh->feat[1] = log2p1((double)c->f_degsum);
-            sh->feat[2] = log2p1((double)m_u);
-            sh->feat[3] = (float)c->level;
-            sh->feat[4] = log2p1((double)p.n);
-            sh->feat[5] = log2p1((double)p.m);
-            sh->feat[6] = (float)c->prev_dir;
-            sh->feat[7] = log2p1((double)c->prev_ns * 1e-3);
+            policy_features(sh->feat, c->f_count, c->f_degsum, 2 * p.m - c->visited_degsum,
+                            c->level, p.n, p.m, c->prev_dir, c->prev_ns);
         } else {
             c->dir = d;
         }
     }
     if (!sh) { return; }
     __syncthreads();
-    bool learned = p.alg == BD_ALG_LEARNED && p.policy && sh->beamer_dir != kDirDone;
-    if (learned) {
-        // out of the trusted feature range: the rule decides
-#pragma unroll
-        for (int i = 0; i < kPolicyIn; ++i) {
-            if (!(sh->feat[i] >= p.policy->lo[i] && sh->feat[i] <= p.policy->hi[i])) { learned = false; }
-        }
-    }
+    const bool learned = p.alg == BD_ALG_LEARNED && p.policy && sh->beamer_dir != kDirDone;
     if (learned && tid < 32) {
-        const PolicyBlob *w = p.policy;
-        const int j = tid;
-        float acc1 = w->b1[j];
-#pragma unroll
-        for (int i = 0; i < kPolicyIn; ++i) {
-            acc1 += w->w1[j][i] * ((sh->feat[i] - w->mean[i]) * w->inv_std[i]);
-        }
-        sh->h1[j] = fmaxf(acc1, 0.f);
-        __syncwarp();
-        float acc2 = w->b2[j];
-#pragma unroll 8
-        for (int i = 0; i < kPolicyH; ++i) { acc2 += w->w2[j][i] * sh->h1[i]; }
-        const float h2 = fmaxf(acc2, 0.f);
-        const float o0 = warp_sum(w->w3[0][j] * h2);
-        const float o1 = warp_sum(w->w3[1][j] * h2);
-        if (j == 0) {
-            sh->logit[0] = o0 + w->b3[0];
-            sh->logit[1] = o1 + w->b3[1];
-        }
+        const float gap = policy_gap_warp(p.policy, sh->feat, sh->h1);
+        if (tid == 0) { sh->logit[0] = gap; }
     }
     __syncthreads();
     if (tid == 0) {
         int d = sh->beamer_dir;
         if (learned) {
-            const float gap = sh->logit[1] - sh->logit[0];
+            // NaN gap: a feature outside the trusted range, the rule decides
+            const float gap = sh->logit[0];
             int pick = d;
             if (isfinite(gap) && fabsf(gap) >= p.policy->margin) {
                 pick = gap > 0.f ? kDirBU : kDirTD;

@@ -16,6 +16,7 @@
 #include <stdint.h>
 
 #include "beedrill_b200.h"
+#include "bd_policy.cuh"
 
 namespace bd {
 
@@ -61,27 +62,6 @@ struct Ctrl {
     int bu_sparse;               // next bottom-up step uses the sparse layout
     int pad0;
     Acc acc[2];
-};
-
-// Learned direction policy: 8-32-32-2 MLP, fp32, row-major weights.
-constexpr int kPolicyIn = 8;
-constexpr int kPolicyH = 32;
-constexpr int kPolicyOut = 2;
-constexpr int kPolicyParams = kPolicyH * kPolicyIn + kPolicyH + kPolicyH * kPolicyH + kPolicyH +
-                              kPolicyOut * kPolicyH + kPolicyOut;  // 1410
-struct PolicyBlob {
-    float w1[kPolicyH][kPolicyIn];
-    float b1[kPolicyH];
-    float w2[kPolicyH][kPolicyH];
-    float b2[kPolicyH];
-    float w3[kPolicyOut][kPolicyH];
-    float b3[kPolicyOut];
-    float mean[kPolicyIn];   // feature standardisation
-    float inv_std[kPolicyIn];
-    float lo[kPolicyIn];     // raw-feature range the policy trusts; outside
-    float hi[kPolicyIn];     // it the Beamer rule decides
-    float margin;            // |logit gap| below which Beamer decides
-    float pad[3];
 };
 
 struct BfsParams {

@@ -60,6 +60,10 @@ inline int64_t bitmap_words(int64_t n) { return (n + 31) / 32; }
 // int64[m]); takes ownership of d_src/d_dst.
 bd_status graph_from_device_edges(int64_t n, int64_t m, int64_t *d_src, int64_t *d_dst,
                                   int32_t order, bd_graph **out);
+struct PolicyBlob;
+// Host-side PolicyBlob from the ABI's arrays (bd_policy.cu).
+bd_status policy_blob(const float *params, const float *mean, const float *inv_std,
+                      const float *lo, const float *hi, float margin, PolicyBlob *blob);
 // Fills d_isolated from d_off.
 bd_status graph_finish(bd_graph *g, cudaStream_t s);
 void graph_free(bd_graph *g);

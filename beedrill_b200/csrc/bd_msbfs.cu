@@ -31,6 +31,7 @@
 
 #include "bd_device_util.cuh"
 #include "bd_internal.h"
+#include "bd_policy.cuh"
 
 namespace bd {
 namespace {
@@ -61,6 +62,8 @@ struct MsCtrl {
     long long arcs_left;         // 2m - degree sum of vertices reached by all lanes
     long long lanes_total;
     long long t_last, push_steps, pull_steps;
+    int prev_dir, pad0;
+    long long prev_ns, policy_overrides;
     MsAcc acc[2];
 };
 
@@ -71,6 +74,7 @@ struct MsParams {
     int64_t n, m;
     ull *seen;
     ull *F[3];
+    uint32_t *fb[3];  // bit v set iff F[.][v] != 0
     uint32_t *qs[3];
     uint32_t *ql[3];
     ull *qlb[3];
@@ -87,11 +91,27 @@ struct MsParams {
     long long spin_limit;
     unsigned expected_ctas;
     int force_dir;  // -1 rule, kPush, kPull
+    const PolicyBlob *policy;  // null: the rule decides
+    // vertices whose pull scan is split into chunks over all warps
+    const uint32_t *heavy;           // [n_heavy]
+    const ull *heavy_cbase;          // [n_heavy + 1] chunk prefix sums
+    int64_t n_heavy;
+    int64_t heavy_deg;               // degree above which a vertex is heavy
+    uint32_t heavy_chunk;            // arcs per chunk
 };
 
 struct MsLocal {
     ull vertices, degsum, lanes, done_degsum;
 };
+
+// Frontier word of v, read only when v's frontier bit is set: the bitmap
+// (n/8 bytes, cache-resident) spares the 8-byte gather for vertices outside
+// the frontier.  Plain loads: the buffers read in a step are not written in
+// it, and every CTA passed the grid barrier's acquire before the step.
+__device__ __forceinline__ ull frontier_word(const MsParams &p, int buf, uint32_t v)
+{
+    return ((p.fb[buf][v >> 5] >> (v & 31)) & 1u) ? p.F[buf][v] : 0ull;
+}
 
 __device__ __forceinline__ int64_t ms_degree(const MsParams &p, uint32_t v)
 {
@@ -173,8 +193,16 @@ __device__ void ms_clear_old(const MsParams &p, const MsView &sv)
     const int old = (sv.step + 2) % 3;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long nt = (long long)gridDim.x * blockDim.x;
-    for (long long i = t; i < sv.p_small; i += nt) { p.F[old][p.qs[old][i]] = 0ull; }
-    for (long long i = t; i < sv.p_large; i += nt) { p.F[old][p.ql[old][i]] = 0ull; }
+    for (long long i = t; i < sv.p_small; i += nt) {
+        const uint32_t v = p.qs[old][i];
+        p.F[old][v] = 0ull;
+        p.fb[old][v >> 5] = 0u;
+    }
+    for (long long i = t; i < sv.p_large; i += nt) {
+        const uint32_t v = p.ql[old][i];
+        p.F[old][v] = 0ull;
+        p.fb[old][v >> 5] = 0u;
+    }
 }
 
 // push: lanes of frontier vertex u flow into neighbours [b, e).
@@ -190,7 +218,7 @@ __device__ __forceinline__ void push_edges(const MsParams &p, MsAcc *acc, int cu
         int64_t deg = 0;
         if (k < e) {
             v = __ldg(&p.adj[k]);
-            const ull vis = __ldcg(&p.seen[v]) | __ldcg(&p.F[cur][v]);
+            const ull vis = __ldcg(&p.seen[v]) | frontier_word(p, cur, v);
             const ull give = bits & ~vis;
             if (give) {
                 const ull old = atomicOr(&p.F[nxt][v], give);
@@ -201,6 +229,7 @@ __device__ __forceinline__ void push_edges(const MsParams &p, MsAcc *acc, int cu
                     if (((vis | old | fresh) & p.all) == p.all) { loc.done_degsum += ms_degree(p, v); }
                 }
                 if (old == 0ull) {
+                    atomicOr(&p.fb[nxt][v >> 5], 1u << (v & 31));
                     appended = true;
                     deg = ms_degree(p, v);
                 }
@@ -245,6 +274,72 @@ __device__ void ms_push_step(const MsParams &p, const MsView &sv, MsLocal &loc)
 }
 
 // pull: warp per 32 vertices; short lists per lane, long lists by the warp.
+// pull for heavy vertices: their lists are cut into chunks dealt to all
+// warps.  A chunk ORs the lanes it finds into the vertex's next frontier
+// word; the bits the atomic returns as new are the ones this chunk
+// delivered first, so their parents come from this chunk.
+template <int BLOCK>
+__device__ void ms_pull_heavy(const MsParams &p, const MsView &sv, MsLocal &loc)
+{
+    const int lane = lane_id();
+    const int warp = threadIdx.x >> 5;
+    const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
+    const long long nw = (long long)gridDim.x * (BLOCK / 32);
+    const int cur = sv.step % 3, nxt = (sv.step + 1) % 3;
+    MsAcc *acc = &p.ctrl->acc[sv.step & 1];
+    const int new_level = sv.level + 1;
+    const long long total = p.n_heavy ? (long long)__ldg(&p.heavy_cbase[p.n_heavy]) : 0;
+    for (long long c = gw; c < total; c += nw) {
+        long long lo = 0, hi = p.n_heavy - 1;  // last i with heavy_cbase[i] <= c
+        while (lo < hi) {
+            const long long mid = (lo + hi + 1) >> 1;
+            if ((long long)__ldg(&p.heavy_cbase[mid]) <= c) { lo = mid; } else { hi = mid - 1; }
+        }
+        const uint32_t v = __ldg(&p.heavy[lo]);
+        const ull vis = __ldcg(&p.seen[v]) | __ldcg(&p.F[cur][v]);
+        const ull need = p.all & ~vis;
+        if (!need) { continue; }
+        const int64_t vb = __ldg(&p.off[v]), ve = __ldg(&p.off[v + 1]);
+        const int64_t b = vb + (c - (long long)__ldg(&p.heavy_cbase[lo])) * (int64_t)p.heavy_chunk;
+        const int64_t e = min(ve, b + (int64_t)p.heavy_chunk);
+        ull have = 0;  // lanes this chunk found or saw others deliver
+        for (int64_t base = b; base < e && (have & need) != need; base += 128) {
+            uint32_t u[4];
+            ull fu[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int64_t k = base + 32 * i + lane;
+                u[i] = k < e ? __ldg(&p.adj[k]) : 0u;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int64_t k = base + 32 * i + lane;
+                fu[i] = k < e ? frontier_word(p, cur, u[i]) & need : 0ull;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const ull f = fu[i] & ~have;
+                if (!__any_sync(kFullMask, f != 0)) { continue; }
+                const ull mine = f & ~warp_excl_or(f);
+                const ull round = warp_or(f);
+                ull old = 0;
+                if (lane == 0) { old = atomicOr(&p.F[nxt][v], round); }
+                old = __shfl_sync(kFullMask, old, 0);
+                const ull fresh = round & ~old;
+                if (mine & fresh) { write_lanes(p, v, mine & fresh, new_level, u[i]); }
+                const bool first = lane == 0 && old == 0ull;
+                if (lane == 0 && fresh) {
+                    loc.lanes += __popcll(fresh);
+                    if (((vis | old | fresh) & p.all) == p.all) { loc.done_degsum += (ull)(ve - vb); }
+                }
+                if (first) { atomicOr(&p.fb[nxt][v >> 5], 1u << (v & 31)); }
+                ms_append(p, acc, nxt, first, v, ve - vb, loc);
+                have |= round | old;
+            }
+        }
+    }
+}
+
 template <int BLOCK>
 __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
 {
@@ -274,17 +369,33 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
             if (need) {
                 beg = __ldg(&p.off[v]);
                 end = __ldg(&p.off[v + 1]);
+                if (end - beg > p.heavy_deg) {
+                    // scanned in chunks by ms_pull_heavy
+                    need = 0;
+                    beg = end = 0;
+                }
+            }
+            if (need) {
                 const int64_t lim = min(end, beg + (int64_t)p.prefix);
                 int64_t k = beg;
-                for (; k < lim && got != need; ++k) {
-                    const uint32_t u = __ldg(&p.adj[k]);
-                    const ull fu = __ldcg(&p.F[cur][u]) & need & ~got;
-                    if (fu) {
-                        got |= fu;
-                        write_lanes(p, v, fu, new_level, u);
+                // four arcs in flight per round
+                for (; k < lim && got != need; k += 4) {
+                    uint32_t u[4];
+                    ull fu[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) { u[i] = (k + i < lim) ? __ldg(&p.adj[k + i]) : 0u; }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) { fu[i] = (k + i < lim) ? frontier_word(p, cur, u[i]) : 0ull; }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const ull f = fu[i] & need & ~got;
+                        if (f) {
+                            got |= f;
+                            write_lanes(p, v, f, new_level, u[i]);
+                        }
                     }
                 }
-                next = (got == need) ? end : k;
+                next = (got == need) ? end : min(k, lim);
             }
         }
         unsigned pending = __ballot_sync(kFullMask, need != 0 && got != need && next < end);
@@ -296,23 +407,36 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
             const ull nd = __shfl_sync(kFullMask, need, owner);
             ull have = __shfl_sync(kFullMask, got, owner);
             const uint32_t vo = __shfl_sync(kFullMask, v, owner);
-            for (int64_t base = b; base < e && have != nd; base += 32) {
-                const int64_t k = base + lane;
-                ull fu = 0;
-                uint32_t u = 0;
-                if (k < e) {
-                    u = __ldg(&p.adj[k]);
-                    fu = __ldcg(&p.F[cur][u]) & nd & ~have;
+            // 128 arcs per round: four independent gathers per lane
+            for (int64_t base = b; base < e && have != nd; base += 128) {
+                uint32_t u[4];
+                ull fu[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int64_t k = base + 32 * i + lane;
+                    u[i] = k < e ? __ldg(&p.adj[k]) : 0u;
                 }
-                // lanes of lower warp lanes win: each lane keeps the bits no
-                // earlier neighbour in this batch already delivered
-                const ull mine = fu & ~warp_excl_or(fu);
-                if (mine) { write_lanes(p, vo, mine, new_level, u); }
-                have |= warp_or(fu);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int64_t k = base + 32 * i + lane;
+                    fu[i] = k < e ? frontier_word(p, cur, u[i]) & nd : 0ull;
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const ull f = fu[i] & ~have;
+                    if (!__any_sync(kFullMask, f != 0)) { continue; }
+                    // arcs earlier in the list win: each lane keeps the bits
+                    // no lower lane of this batch already delivered
+                    const ull mine = f & ~warp_excl_or(f);
+                    if (mine) { write_lanes(p, vo, mine, new_level, u[i]); }
+                    have |= warp_or(f);
+                }
             }
             if (lane == owner) { got = have; }
         }
         const bool gained = got != 0;
+        const unsigned gm = __ballot_sync(kFullMask, gained);
+        if (lane == 0 && gm) { atomicOr(&p.fb[nxt][w], gm); }
         if (gained) {
             p.F[nxt][v] = got;
             loc.lanes += __popcll(got);
@@ -328,19 +452,19 @@ struct MsShared {
     int is_last;
     unsigned gen;
     int exit_flag;
+    int rule_dir;
+    float gap;
+    float feat[kPolicyIn];
+    float h1[kPolicyH];
 };
 
-__device__ void ms_choose(MsCtrl *c, const MsParams &p)
+// The rule: pull once the frontier's edges are a sizeable share of the edges
+// still able to deliver a lane (Beamer's alpha test over the batch).
+__device__ int ms_rule(const MsCtrl *c, const MsParams &p)
 {
-    if (c->f_count == 0) {
-        c->dir = kMsDone;
-    } else if (p.force_dir >= 0) {
-        c->dir = p.force_dir;
-    } else {
-        // pull once the frontier's edges are a sizeable share of the edges
-        // still able to deliver a lane (Beamer's alpha test over the batch)
-        c->dir = (c->f_degsum * p.alpha > c->arcs_left) ? kPull : kPush;
-    }
+    if (c->f_count == 0) { return kMsDone; }
+    if (p.force_dir >= 0) { return p.force_dir; }
+    return (c->f_degsum * p.alpha > c->arcs_left) ? kPull : kPush;
 }
 
 __device__ void ms_finish_step(MsCtrl *c, const MsParams &p)
@@ -360,6 +484,8 @@ __device__ void ms_finish_step(MsCtrl *c, const MsParams &p)
         r.ns = now - c->t_last;
         p.rec[s] = r;
     }
+    c->prev_dir = c->dir;
+    c->prev_ns = now - c->t_last;
     c->lanes_total += (long long)a->lanes;
     c->arcs_left -= (long long)a->done_degsum;
     c->p_small = c->f_small;
@@ -375,7 +501,35 @@ __device__ void ms_finish_step(MsCtrl *c, const MsParams &p)
     z->vertices = z->degsum = z->lanes = z->small_cnt = z->large_packed = z->done_degsum = 0;
     c->step = s + 1;
     c->t_last = now;
-    ms_choose(c, p);
+}
+
+// Next direction by the CTA that closes a step: the rule, or the learned
+// policy (one warp) where it is installed, trusted and confident.
+template <int BLOCK>
+__device__ void ms_decide(MsCtrl *c, const MsParams &p, MsShared<BLOCK> &sh)
+{
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        sh.rule_dir = ms_rule(c, p);
+        policy_features(sh.feat, c->f_count, c->f_degsum, c->arcs_left, c->level, p.n, p.m,
+                        c->prev_dir, c->prev_ns);
+    }
+    __syncthreads();
+    const bool learned = p.policy && p.force_dir < 0 && sh.rule_dir != kMsDone;
+    if (learned && tid < 32) {
+        const float gap = policy_gap_warp(p.policy, sh.feat, sh.h1);
+        if (tid == 0) { sh.gap = gap; }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int d = sh.rule_dir;
+        if (learned && isfinite(sh.gap) && fabsf(sh.gap) >= p.policy->margin) {
+            const int pick = sh.gap > 0.f ? kPull : kPush;
+            if (pick != d) { c->policy_overrides += 1; }
+            d = pick;
+        }
+        c->dir = d;
+    }
 }
 
 template <int BLOCK>
@@ -389,21 +543,26 @@ __device__ void ms_barrier(const MsParams &p, MsShared<BLOCK> &sh)
         const unsigned prev = atomicAdd(&c->bar_count, 1u);
         sh.is_last = (prev == p.expected_ctas - 1);
         sh.gen = gen;
-        if (sh.is_last) {
-            __threadfence();
-            ms_finish_step(c, p);
+    }
+    __syncthreads();
+    if (sh.is_last) {
+        __threadfence();
+        if (threadIdx.x == 0) { ms_finish_step(c, p); }
+        __syncthreads();
+        ms_decide<BLOCK>(c, p, sh);
+        if (threadIdx.x == 0) {
             atomicExch(&c->bar_count, 0u);
             __threadfence();
-            st_release(&c->bar_gen, gen + 1);
-        } else {
-            long long it = 0;
-            while (ld_acquire(&c->bar_gen) == gen) {
-                if (++it > p.spin_limit) {
-                    atomicExch(&c->error, (int)BD_ERR_TIMEOUT);
-                    break;
-                }
-                __nanosleep(64);
+            st_release(&c->bar_gen, sh.gen + 1);
+        }
+    } else if (threadIdx.x == 0) {
+        long long it = 0;
+        while (ld_acquire(&c->bar_gen) == sh.gen) {
+            if (++it > p.spin_limit) {
+                atomicExch(&c->error, (int)BD_ERR_TIMEOUT);
+                break;
             }
+            __nanosleep(64);
         }
     }
     __syncthreads();
@@ -454,6 +613,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) msbfs_kernel(MsParams p)
         if (sv.dir == kPush) {
             ms_push_step<BLOCK>(p, sv, loc);
         } else {
+            ms_pull_heavy<BLOCK>(p, sv, loc);
             ms_pull_step<BLOCK>(p, sv, loc);
         }
         ms_publish<BLOCK>(p, sv, sh, loc);
@@ -473,6 +633,7 @@ __global__ void ms_init_kernel(MsParams p, const int64_t *sources, int count)
         const ull bit = 1ull << r;
         const ull before = p.F[0][s];
         p.F[0][s] = before | bit;
+        p.fb[0][s >> 5] |= 1u << (s & 31);
         p.seen[s] |= bit;
         p.depth[(int64_t)s * p.R + r] = 0;
         p.parent[(int64_t)s * p.R + r] = s;
@@ -497,7 +658,7 @@ __global__ void ms_init_kernel(MsParams p, const int64_t *sources, int count)
     c->f_chunks = (long long)(lp & kChunkMask);
     c->arcs_left = 2 * p.m - done;
     c->lanes_total = count;
-    ms_choose(c, p);
+    c->dir = ms_rule(c, p);
 }
 
 // Per-lane reached count and degree sum (count_num_traversed_edges per root).
@@ -587,6 +748,7 @@ struct bd_msbfs {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ull *seen = nullptr;         // [groups][n]: a group's final words mark its valid lanes
     ull *F[3] = {nullptr, nullptr, nullptr};
+    uint32_t *fb[3] = {nullptr, nullptr, nullptr};
     uint32_t *qs[3] = {nullptr, nullptr, nullptr};
     uint32_t *ql[3] = {nullptr, nullptr, nullptr};
     ull *qlb[3] = {nullptr, nullptr, nullptr};
@@ -601,6 +763,10 @@ struct bd_msbfs {
     int block = 512;
     int count = 0;  // roots in the last run
     bool ran = false;
+    PolicyBlob *policy = nullptr;  // device copy, or null
+    uint32_t *heavy = nullptr;
+    ull *heavy_cbase = nullptr;
+    int64_t n_heavy = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_count = -1;
     bool graph_ok = true;
@@ -631,6 +797,7 @@ MsParams ms_params(bd_msbfs *b, int group, int count)
     p.seen = b->seen + group * b->g->n;
     for (int i = 0; i < 3; ++i) {
         p.F[i] = b->F[i];
+        p.fb[i] = b->fb[i];
         p.qs[i] = b->qs[i];
         p.ql[i] = b->ql[i];
         p.qlb[i] = b->qlb[i];
@@ -650,6 +817,12 @@ MsParams ms_params(bd_msbfs *b, int group, int count)
     p.spin_limit = b->opts.spin_limit;
     p.expected_ctas = (unsigned)b->grid;
     p.force_dir = b->opts.force_dir;
+    p.policy = b->policy;
+    p.heavy = b->heavy;
+    p.heavy_cbase = b->heavy_cbase;
+    p.n_heavy = b->n_heavy;
+    p.heavy_deg = b->opts.heavy_degree;
+    p.heavy_chunk = (uint32_t)b->opts.heavy_chunk;
     return p;
 }
 
@@ -659,7 +832,10 @@ bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
 {
     const int64_t n = b->g->n;
     BD_CUDA(cudaMemsetAsync(b->seen + group * n, 0, sizeof(ull) * n, b->stream));
-    for (int i = 0; i < 3; ++i) { BD_CUDA(cudaMemsetAsync(b->F[i], 0, sizeof(ull) * n, b->stream)); }
+    for (int i = 0; i < 3; ++i) {
+        BD_CUDA(cudaMemsetAsync(b->F[i], 0, sizeof(ull) * n, b->stream));
+        BD_CUDA(cudaMemsetAsync(b->fb[i], 0, sizeof(uint32_t) * ((n + 31) / 32), b->stream));
+    }
     MsParams p = ms_params(b, group, count);
     ms_init_kernel<<<1, 1, 0, b->stream>>>(p, b->d_sources + group * 64, count);
     BD_CUDA(cudaGetLastError());
@@ -725,6 +901,7 @@ void ms_free(bd_msbfs *b)
     cudaFree(b->seen);
     for (int i = 0; i < 3; ++i) {
         cudaFree(b->F[i]);
+        cudaFree(b->fb[i]);
         cudaFree(b->qs[i]);
         cudaFree(b->ql[i]);
         cudaFree(b->qlb[i]);
@@ -735,6 +912,9 @@ void ms_free(bd_msbfs *b)
     cudaFree(b->rec);
     cudaFree(b->d_sources);
     cudaFree(b->d_counts);
+    cudaFree(b->policy);
+    cudaFree(b->heavy);
+    cudaFree(b->heavy_cbase);
     if (b->ev0) { cudaEventDestroy(b->ev0); }
     if (b->ev1) { cudaEventDestroy(b->ev1); }
     if (b->stream) { cudaStreamDestroy(b->stream); }
@@ -801,6 +981,8 @@ bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *o
     if (o.large_degree > (1 << 20)) { return BD_ERR_INVALID; }
     if (o.chunk_edges <= 0) { o.chunk_edges = 1024; }
     if (o.pull_prefix <= 0) { o.pull_prefix = 16; }
+    if (o.heavy_degree <= 0) { o.heavy_degree = 4096; }
+    if (o.heavy_chunk <= 0) { o.heavy_chunk = 2048; }
     if (o.spin_limit <= 0) { o.spin_limit = kMsDefaultSpin; }
     if (g->n > (int64_t)UINT32_MAX) { return BD_ERR_LIMIT; }
     BD_TRY(ensure_device());
@@ -829,6 +1011,7 @@ bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *o
               cudaMalloc(&b->d_counts, sizeof(unsigned long long) * 128 * b->groups) == cudaSuccess;
     for (int i = 0; i < 3 && ok; ++i) {
         ok = cudaMalloc(&b->F[i], sizeof(ull) * n) == cudaSuccess &&
+             cudaMalloc(&b->fb[i], sizeof(uint32_t) * ((n + 31) / 32)) == cudaSuccess &&
              cudaMalloc(&b->qs[i], sizeof(uint32_t) * n) == cudaSuccess &&
              cudaMalloc(&b->ql[i], sizeof(uint32_t) * b->cap_large) == cudaSuccess &&
              cudaMalloc(&b->qlb[i], sizeof(ull) * b->cap_large) == cudaSuccess;
@@ -842,6 +1025,32 @@ bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *o
         return fail(BD_ERR_CUDA);
     }
     b->grid = per_sm * sms;
+    // heavy vertices and their chunk prefix sums (host, once per handle)
+    {
+        std::vector<int64_t> off(n + 1);
+        if (cudaMemcpy(off.data(), g->d_off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost) !=
+            cudaSuccess) {
+            return fail(BD_ERR_CUDA);
+        }
+        std::vector<uint32_t> hv;
+        std::vector<ull> hc(1, 0);
+        for (int64_t v = 0; v < n; ++v) {
+            const int64_t d = off[v + 1] - off[v];
+            if (d > o.heavy_degree) {
+                hv.push_back((uint32_t)v);
+                hc.push_back(hc.back() + (ull)((d + o.heavy_chunk - 1) / o.heavy_chunk));
+            }
+        }
+        b->n_heavy = (int64_t)hv.size();
+        if (cudaMalloc(&b->heavy, sizeof(uint32_t) * std::max<size_t>(hv.size(), 1)) != cudaSuccess ||
+            cudaMalloc(&b->heavy_cbase, sizeof(ull) * hc.size()) != cudaSuccess ||
+            (!hv.empty() && cudaMemcpy(b->heavy, hv.data(), sizeof(uint32_t) * hv.size(),
+                                       cudaMemcpyHostToDevice) != cudaSuccess) ||
+            cudaMemcpy(b->heavy_cbase, hc.data(), sizeof(ull) * hc.size(), cudaMemcpyHostToDevice) !=
+                cudaSuccess) {
+            return fail(BD_ERR_OOM);
+        }
+    }
     *out = b;
     return BD_OK;
 }
@@ -923,6 +1132,27 @@ bd_status bd_msbfs_get_steps(bd_msbfs *b, bd_step *steps, int64_t capacity, int6
         BD_CUDA(cudaMemcpy(steps, b->rec, sizeof(bd_step) * take, cudaMemcpyDeviceToHost));
     }
     *count = have;
+    return BD_OK;
+}
+
+bd_status bd_msbfs_set_policy(bd_msbfs *b, const float *params, const float *mean,
+                              const float *inv_std, const float *lo, const float *hi, float margin)
+{
+    if (!b) { return BD_ERR_INVALID; }
+    BD_CUDA(cudaSetDevice(b->device));
+    if (!params) {
+        cudaFree(b->policy);
+        b->policy = nullptr;
+        b->graph_count = -1;  // captured launches hold the old pointer
+        return BD_OK;
+    }
+    PolicyBlob blob;
+    BD_TRY(policy_blob(params, mean, inv_std, lo, hi, margin, &blob));
+    if (!b->policy) {
+        BD_CUDA(cudaMalloc(&b->policy, sizeof(PolicyBlob)));
+        b->graph_count = -1;
+    }
+    BD_CUDA(cudaMemcpy(b->policy, &blob, sizeof(PolicyBlob), cudaMemcpyHostToDevice));
     return BD_OK;
 }
 

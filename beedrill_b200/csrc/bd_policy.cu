@@ -187,6 +187,26 @@ namespace bd {
 bd_status bfs_install_policy(bd_bfs *b, const PolicyBlob *blob);
 }
 
+namespace bd {
+
+bd_status policy_blob(const float *params, const float *mean, const float *inv_std,
+                      const float *lo, const float *hi, float margin, PolicyBlob *blob)
+{
+    if (!params || !mean || !inv_std || !(margin >= 0)) { return BD_ERR_INVALID; }
+    memset(blob, 0, sizeof *blob);
+    memcpy(blob, params, sizeof(float) * kP);
+    memcpy(blob->mean, mean, sizeof(float) * kPolicyIn);
+    memcpy(blob->inv_std, inv_std, sizeof(float) * kPolicyIn);
+    for (int i = 0; i < kPolicyIn; ++i) {
+        blob->lo[i] = lo ? lo[i] : -INFINITY;
+        blob->hi[i] = hi ? hi[i] : INFINITY;
+    }
+    blob->margin = margin;
+    return BD_OK;
+}
+
+}  // namespace bd
+
 using namespace bd;
 
 extern "C" {
@@ -285,17 +305,8 @@ bd_status bd_bfs_set_policy(bd_bfs *b, const float *params, const float *mean,
 {
     if (!b) { return BD_ERR_INVALID; }
     if (!params) { return bfs_install_policy(b, nullptr); }
-    if (!mean || !inv_std || !(margin >= 0)) { return BD_ERR_INVALID; }
     PolicyBlob blob;
-    memset(&blob, 0, sizeof blob);
-    memcpy(&blob, params, sizeof(float) * kP);
-    memcpy(blob.mean, mean, sizeof(float) * kPolicyIn);
-    memcpy(blob.inv_std, inv_std, sizeof(float) * kPolicyIn);
-    for (int i = 0; i < kPolicyIn; ++i) {
-        blob.lo[i] = lo ? lo[i] : -INFINITY;
-        blob.hi[i] = hi ? hi[i] : INFINITY;
-    }
-    blob.margin = margin;
+    BD_TRY(policy_blob(params, mean, inv_std, lo, hi, margin, &blob));
     return bfs_install_policy(b, &blob);
 }
 

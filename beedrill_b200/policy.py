@@ -37,6 +37,9 @@ NUM_PARAMS = 1410
 NUM_FEATURES = 8
 DEFAULT_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "policy",
                             "learned_policy.json")
+# push/pull policy of the batched (64-root) traversal
+BATCHED_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "policy",
+                            "learned_policy_batched.json")
 
 
 def raw_features(frontier, frontier_edges, unexplored, level, n, m, prev_dir, prev_ns):
@@ -128,6 +131,49 @@ def measure_tables(graph: "bd.Graph", roots, repeats: int = 1, with_beamer: bool
         if h is not None:
             h.close()
     return tables
+
+
+def measure_tables_batched(graph: "bd.Graph", roots, repeats: int = 1, alpha: int = 4):
+    """Forced push and forced pull runs of one batch of up to 64 roots; one
+    LevelTable whose top-down / bottom-up columns hold push / pull times,
+    `found` counts new (vertex, root) pairs and `unexplored` is the degree
+    sum of vertices some root has not reached."""
+    n, m = graph.num_vertices(), graph.num_edges()
+    runs = {}
+    for name, fd in (("push", 0), ("pull", 1)):
+        h = bd.BatchedBFS(graph, len(roots), force_dir=fd)
+        best = None
+        for _ in range(repeats):
+            h.run(roots)
+            st = h.steps()
+            t = np.array([s["ns"] for s in st], np.float64)
+            best = t if best is None else np.minimum(best, t)
+        runs[name], runs[name + "_t"] = st, best
+        h.close()
+    a, b = runs["push"], runs["pull"]
+    if len(a) != len(b) or any(x["found"] != y["found"] for x, y in zip(a, b)):
+        raise RuntimeError("forced batched runs disagree on the level structure")
+    rule = bd.BatchedBFS(graph, len(roots), alpha=alpha)
+    st = rule.run(roots)
+    tab = LevelTable(
+        n=n, m=m,
+        frontier=np.array([s["frontier"] for s in a], np.int64),
+        frontier_edges=np.array([s["frontier_edges"] for s in a], np.int64),
+        unexplored=np.array([s["unexplored_edges"] for s in a], np.int64),
+        found=np.array([s["found"] for s in a], np.int64),
+        t_td=runs["push_t"], t_bu=runs["pull_t"], beamer_dirs=rule.directions(),
+        beamer_ns=st.ms * 1e6, meta={"roots": len(roots), "alpha": alpha})
+    rule.close()
+    return tab
+
+
+def alpha_dirs(tab: LevelTable, alpha=4) -> str:
+    """The batched traversal's rule over a level table: pull when the
+    frontier's degree sum times alpha exceeds the unexplored degree sum."""
+    out = []
+    for lv in range(tab.levels):
+        out.append("B" if tab.frontier_edges[lv] * alpha > tab.unexplored[lv] else "T")
+    return "".join(out)
 
 
 def dataset(tables):
@@ -224,10 +270,11 @@ def beamer_dirs(tab: LevelTable, alpha=15, beta=18) -> str:
     return "".join(out)
 
 
-def policy_dirs(policy: Policy, tab: LevelTable, alpha=15, beta=18) -> str:
-    """Decisions the policy makes along a level table (Beamer where the
-    logit gap is below the margin)."""
-    rule = beamer_dirs(tab, alpha, beta)
+def policy_dirs(policy: Policy, tab: LevelTable, alpha=15, beta=18, rule=None) -> str:
+    """Decisions the policy makes along a level table (the rule -- Beamer by
+    default -- where the logit gap is below the margin or a feature is out
+    of the trusted range)."""
+    rule = rule if rule is not None else beamer_dirs(tab, alpha, beta)
     out = []
     prev_dir, prev_ns = 0, 0.0
     for lv in range(tab.levels):
@@ -301,15 +348,51 @@ def collect(specs, roots_per_graph=4, repeats=1, log=None):
     return tables
 
 
-def choose_margin(policy: Policy, tables, candidates=(0.0, 0.25, 0.5, 1.0, 2.0)):
+def choose_margin(policy: Policy, tables, candidates=(0.0, 0.25, 0.5, 1.0, 2.0), rule_fn=None):
     best = None
     for mgn in candidates:
         policy.margin = mgn
-        r = regret(tables, lambda t: policy_dirs(policy, t))["regret_ms"]
+        r = regret(tables, lambda t: policy_dirs(
+            policy, t, rule=rule_fn(t) if rule_fn else None))["regret_ms"]
         if best is None or r < best[1]:
             best = (mgn, r)
     policy.margin = best[0]
     return best
+
+
+def train_batched(args, log):
+    """The push/pull policy of the batched traversal, trained the same way
+    on one 64-root batch per training graph."""
+    specs = training_graph_specs(args.graphs)
+    tables = []
+    t0 = time.time()
+    for i, s in enumerate(specs):
+        g = bd.Graph.rmat(s["scale"], s["edge_factor"], s["a"], s["b"], s["c"], s["d"], s["seed"],
+                          order=bd.ORDER_DEGREE)
+        tab = measure_tables_batched(g, g.pick_roots(s["seed"], 64))
+        tab.meta.update(s)
+        tables.append(tab)
+        g.close()
+        if (i + 1) % 20 == 0:
+            log(f"collected {i + 1}/{len(specs)} graphs")
+    log(f"{len(tables)} batched level tables in {time.time() - t0:.1f} s")
+    train_t = [tb for tb in tables if (tb.meta["seed"] % 5) != 0]
+    val_t = [tb for tb in tables if (tb.meta["seed"] % 5) == 0]
+    X, y, w = dataset(train_t)
+    policy, hist = fit(X, y, w, epochs=args.epochs, lr=args.lr)
+    rule = lambda tb: alpha_dirs(tb)  # noqa: E731
+    mgn, _ = choose_margin(policy, val_t, rule_fn=rule)
+    rb = regret(val_t, rule)
+    rl = regret(val_t, lambda tb: policy_dirs(policy, tb, rule=rule(tb)))
+    policy.info = {"kind": "batched", "graphs": args.graphs, "samples": int(len(y)),
+                   "epochs": args.epochs, "lr": args.lr, "loss_first": float(hist[0]),
+                   "loss_last": float(hist[-1]), "margin": mgn,
+                   "validation": {"rule": rb, "learned": rl},
+                   "distribution": "RMAT scales 16-22, A~U[0.45,0.65], D=0.05, B=C=(1-A-D)/2, "
+                                   "ef 16, 64 roots per graph"}
+    policy.save(args.out)
+    log(f"saved {args.out}: rule regret {rb['regret_frac']:.3%}, learned {rl['regret_frac']:.3%}")
+    return 0
 
 
 def main(argv=None):
@@ -320,10 +403,16 @@ def main(argv=None):
     t.add_argument("--roots", type=int, default=4)
     t.add_argument("--epochs", type=int, default=3000)
     t.add_argument("--lr", type=float, default=3e-3)
-    t.add_argument("--out", default=DEFAULT_PATH)
+    t.add_argument("--out", default=None)
     t.add_argument("--tables-out", default=None)
+    t.add_argument("--batched", action="store_true",
+                   help="train the push/pull policy of the 64-root batched traversal")
     args = ap.parse_args(argv)
     log = lambda s: print(f"[policy {time.strftime('%H:%M:%S')}] {s}", flush=True)  # noqa: E731
+    if args.batched:
+        args.out = args.out or BATCHED_PATH
+        return train_batched(args, log)
+    args.out = args.out or DEFAULT_PATH
     specs = training_graph_specs(args.graphs)
     t0 = time.time()
     tables = collect(specs, args.roots, log=log)

@@ -242,6 +242,10 @@ def main():
         learned = bd.HybridBFS(g, alg="learned")
         P.Policy.load().install(learned)
     batched = bd.BatchedBFS(g, NUM_ROOTS)
+    batched_rule = None
+    if os.path.exists(P.BATCHED_PATH):
+        P.Policy.load(P.BATCHED_PATH).install(batched)
+        batched_rule = bd.BatchedBFS(g, NUM_ROOTS)
 
     def one_step():
         out = {}
@@ -250,11 +254,14 @@ def main():
         if learned is not None:
             ms, edges, reached, e2e = learned.run_many(roots, with_reached=True)
             out["learned"] = (ms, edges, reached, e2e)
-        t0 = time.perf_counter()
-        st = batched.run(roots)
-        wall = (time.perf_counter() - t0) * 1e3
-        m_c, n_c = batched.counts()
-        out["batched"] = (np.full(NUM_ROOTS, st.ms / NUM_ROOTS), m_c, n_c, wall)
+        for name, h in (("batched", batched), ("batched_rule", batched_rule)):
+            if h is None:
+                continue
+            t0 = time.perf_counter()
+            st = h.run(roots)
+            wall = (time.perf_counter() - t0) * 1e3
+            m_c, n_c = h.counts()
+            out[name] = (np.full(NUM_ROOTS, st.ms / NUM_ROOTS), m_c, n_c, wall)
         return out
 
     for _ in range(args.warmup):
@@ -278,7 +285,7 @@ def main():
         gteps = edges / (ms * 1e-3) / 1e9
         e2e = hmean(np.concatenate([r[name][1] / (r[name][3] / NUM_ROOTS * 1e-3) / 1e9 for r in runs]))
         step_ms = float(np.mean([r[name][0].sum() for r in runs]))
-        if name == "batched":
+        if name.startswith("batched"):
             # one shared CSR pass per 64-root launch, plus every root's
             # depth and parent outputs, spread evenly over its roots
             per_launch = 8.0 * (n + 1) + 8.0 * m + 12.0 * reached.reshape(-1, NUM_ROOTS).sum(1)
@@ -346,7 +353,8 @@ def main():
                 "h2d_bytes_per_step": 8 * NUM_ROOTS,
                 "d2h_bytes_per_step": 16 * NUM_ROOTS,
                 "note": "public API call per step: root upload, clear + runs, m_c/n_c download"},
-        "gpu_launches": args.steps * (3 * NUM_ROOTS * (1 + (learned is not None)) + 3),
+        "gpu_launches": args.steps * (3 * NUM_ROOTS * (1 + (learned is not None))
+                                      + 3 * (1 + (batched_rule is not None))),
         "clocks": clocks.summary(),
     }
     if cpu_thread is not None:
@@ -365,7 +373,7 @@ def main():
         tmpdir.cleanup()
     if rank == 0:
         print(json.dumps(line))
-    for h in (plain, learned, batched):
+    for h in (plain, learned, batched, batched_rule):
         if h is not None:
             h.close()
     if world > 1:

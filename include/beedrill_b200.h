@@ -235,6 +235,9 @@ typedef struct bd_msbfs_opts {
     int32_t use_graph;     /* 1 (default via bd_msbfs_default_opts): replay the
                               groups of a call as one captured CUDA graph       */
     int64_t spin_limit;    /* grid-barrier poll bound; 0 = default (~2 s)       */
+    int32_t heavy_degree;  /* pull: lists longer than this are cut into chunks
+                              shared by all warps; 0 = default (4096)           */
+    int32_t heavy_chunk;   /* arcs per such chunk; 0 = default (2048)           */
 } bd_msbfs_opts;
 void bd_msbfs_default_opts(bd_msbfs_opts *opts);
 /* max_roots: capacity of one call (results of all roots stay readable). */
@@ -250,6 +253,12 @@ bd_status bd_msbfs_count_traversed_edges(bd_msbfs *b, int32_t root_index, int64_
                                          int64_t *reached);
 /* Step records of the last group of the last call (found = new lanes). */
 bd_status bd_msbfs_get_steps(bd_msbfs *b, bd_step *steps, int64_t capacity, int64_t *count);
+/* Installs (params != NULL) or removes the learned push/pull policy of the
+ * batched traversal (same network layout and features as bd_bfs_set_policy;
+ * unexplored degree sum = degree sum of vertices some lane has not reached). */
+bd_status bd_msbfs_set_policy(bd_msbfs *b, const float *params, const float *mean,
+                              const float *inv_std, const float *lo, const float *hi,
+                              float margin);
 bd_status bd_msbfs_destroy(bd_msbfs *b);
 
 /* ---- learned direction policy -------------------------------------------- */

@@ -35,6 +35,19 @@ def test_64_roots_every_lane_matches(force_dir):
     _check_all(ms, off, adj, roots)
 
 
+@pytest.mark.parametrize("heavy", [(64, 32), (256, 100), (1 << 30, 2048)])
+def test_heavy_vertex_chunked_pull(heavy):
+    """Pull scans of long lists cut into chunks shared by all warps (a
+    tiny threshold makes most vertices take that path)."""
+    g = bd.Graph.rmat(15, seed=45, order=bd.ORDER_DEGREE)
+    off, adj = g.csr()
+    roots = g.pick_roots(2, 64)
+    ms = bd.BatchedBFS(g, 64, force_dir=1, heavy_degree=heavy[0], heavy_chunk=heavy[1],
+                       tuned=False)
+    ms.run(roots)
+    _check_all(ms, off, adj, roots, limit=16)
+
+
 def test_partial_groups_duplicates_and_isolated_roots():
     g = bd.Graph.rmat(13, 8, seed=42)
     off, adj = g.csr()
