@@ -44,6 +44,7 @@ constexpr int kLargeShift = 38;
 constexpr ull kChunkMask = (1ull << kLargeShift) - 1;
 constexpr int64_t kMsRecCap = 1 << 14;
 constexpr long long kMsDefaultSpin = 4000000;
+constexpr unsigned kRecSlots = 16;  // delivery records per vertex
 
 struct MsAcc {
     ull vertices;    // vertices entering the next frontier
@@ -78,8 +79,10 @@ struct MsParams {
     uint32_t *qs[3];
     uint32_t *ql[3];
     ull *qlb[3];
-    int32_t *depth;
+    int32_t *depth;     // per-lane rows, used when a vertex runs out of records
     uint32_t *parent;
+    uint4 *drec;        // [n][kRecSlots] delivery records {mask lo, mask hi, provider, level}
+    uint32_t *drec_cnt; // [n] records written (may exceed kRecSlots)
     int R;
     ull all;
     MsCtrl *ctrl;
@@ -156,8 +159,10 @@ __device__ __forceinline__ void ms_append(const MsParams &p, MsAcc *acc, int qn,
     }
 }
 
-__device__ __forceinline__ void write_lanes(const MsParams &p, uint32_t v, ull lanes, int level,
-                                            uint32_t parent)
+// Lanes whose vertex has run out of delivery records: one depth and one
+// parent entry per lane in the vertex-major rows.
+__device__ __forceinline__ void write_rows(const MsParams &p, uint32_t v, ull lanes, int level,
+                                           uint32_t parent)
 {
     while (lanes) {
         const int r = __ffsll((long long)lanes) - 1;
@@ -165,6 +170,26 @@ __device__ __forceinline__ void write_lanes(const MsParams &p, uint32_t v, ull l
         p.depth[(int64_t)v * p.R + r] = level;
         p.parent[(int64_t)v * p.R + r] = parent;
     }
+}
+
+// Delivery record `slot` of v: the lanes that `parent` delivered at `level`
+// (one 16-byte store for all of them).  Past kRecSlots, per-lane rows.
+__device__ __forceinline__ void put_record(const MsParams &p, uint32_t v, unsigned slot,
+                                           ull lanes, int level, uint32_t parent)
+{
+    if (slot < kRecSlots) {
+        p.drec[(int64_t)v * kRecSlots + slot] =
+            make_uint4((uint32_t)lanes, (uint32_t)(lanes >> 32), parent, (uint32_t)level);
+    } else {
+        write_rows(p, v, lanes, level, parent);
+    }
+}
+
+// A record from one of several concurrent deliverers (push, chunked pull).
+__device__ __forceinline__ void record_shared(const MsParams &p, uint32_t v, ull lanes, int level,
+                                              uint32_t parent)
+{
+    put_record(p, v, atomicAdd(&p.drec_cnt[v], 1u), lanes, level, parent);
 }
 
 struct MsView {
@@ -224,7 +249,7 @@ __device__ __forceinline__ void push_edges(const MsParams &p, MsAcc *acc, int cu
                 const ull old = atomicOr(&p.F[nxt][v], give);
                 const ull fresh = give & ~old;
                 if (fresh) {
-                    write_lanes(p, v, fresh, new_level, u);
+                    record_shared(p, v, fresh, new_level, u);
                     loc.lanes += __popcll(fresh);
                     if (((vis | old | fresh) & p.all) == p.all) { loc.done_degsum += ms_degree(p, v); }
                 }
@@ -326,7 +351,7 @@ __device__ void ms_pull_heavy(const MsParams &p, const MsView &sv, MsLocal &loc)
                 if (lane == 0) { old = atomicOr(&p.F[nxt][v], round); }
                 old = __shfl_sync(kFullMask, old, 0);
                 const ull fresh = round & ~old;
-                if (mine & fresh) { write_lanes(p, v, mine & fresh, new_level, u[i]); }
+                if (mine & fresh) { record_shared(p, v, mine & fresh, new_level, u[i]); }
                 const bool first = lane == 0 && old == 0ull;
                 if (lane == 0 && fresh) {
                     loc.lanes += __popcll(fresh);
@@ -358,6 +383,7 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
         const bool live = !((iso >> lane) & 1u);
         ull need = 0, got = 0;
         int64_t beg = 0, end = 0, next = 0;
+        unsigned cnt = 0, cnt0 = 0;  // this vertex's delivery records
         if (live) {
             const ull f = __ldcg(&p.F[cur][v]);
             ull s = __ldcg(&p.seen[v]);
@@ -376,6 +402,7 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
                 }
             }
             if (need) {
+                cnt = cnt0 = __ldcg(&p.drec_cnt[v]);
                 const int64_t lim = min(end, beg + (int64_t)p.prefix);
                 int64_t k = beg;
                 // four arcs in flight per round
@@ -391,7 +418,7 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
                         const ull f = fu[i] & need & ~got;
                         if (f) {
                             got |= f;
-                            write_lanes(p, v, f, new_level, u[i]);
+                            put_record(p, v, cnt++, f, new_level, u[i]);
                         }
                     }
                 }
@@ -407,6 +434,7 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
             const ull nd = __shfl_sync(kFullMask, need, owner);
             ull have = __shfl_sync(kFullMask, got, owner);
             const uint32_t vo = __shfl_sync(kFullMask, v, owner);
+            unsigned c = __shfl_sync(kFullMask, cnt, owner);
             // 128 arcs per round: four independent gathers per lane
             for (int64_t base = b; base < e && have != nd; base += 128) {
                 uint32_t u[4];
@@ -428,12 +456,18 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
                     // arcs earlier in the list win: each lane keeps the bits
                     // no lower lane of this batch already delivered
                     const ull mine = f & ~warp_excl_or(f);
-                    if (mine) { write_lanes(p, vo, mine, new_level, u[i]); }
+                    const unsigned bm = __ballot_sync(kFullMask, mine != 0);
+                    if (mine) { put_record(p, vo, c + __popc(bm & lanemask_lt()), mine, new_level, u[i]); }
+                    c += __popc(bm);
                     have |= warp_or(f);
                 }
             }
-            if (lane == owner) { got = have; }
+            if (lane == owner) {
+                got = have;
+                cnt = c;
+            }
         }
+        if (cnt != cnt0) { p.drec_cnt[v] = cnt; }
         const bool gained = got != 0;
         const unsigned gm = __ballot_sync(kFullMask, gained);
         if (lane == 0 && gm) { atomicOr(&p.fb[nxt][w], gm); }
@@ -635,8 +669,7 @@ __global__ void ms_init_kernel(MsParams p, const int64_t *sources, int count)
         p.F[0][s] = before | bit;
         p.fb[0][s >> 5] |= 1u << (s & 31);
         p.seen[s] |= bit;
-        p.depth[(int64_t)s * p.R + r] = 0;
-        p.parent[(int64_t)s * p.R + r] = s;
+        put_record(p, s, p.drec_cnt[s]++, bit, 0, s);
         const int64_t deg = p.off[s + 1] - p.off[s];
         if (p.seen[s] == p.all) { done += deg; }
         if (before) { continue; }
@@ -702,20 +735,40 @@ __global__ void ms_count_kernel(const ull *seen, const int64_t *off, int64_t n, 
     }
 }
 
-// Lane r's depth / parent rows, widened to the single-source output format.
-// A lane's entries are valid only where its seen bit is set; the rest read
-// as unreached, so the output rows never need clearing.
-__global__ void ms_extract_kernel(const int32_t *depth, const uint32_t *parent, const ull *seen,
-                                  const int64_t *off, int64_t n, int R, int r, int32_t *depth_out,
-                                  int64_t *parent_out)
+// Lane r's depths and parents in the single-source output format.  Lane r
+// reached v iff seen bit r is set; its depth and parent are in the record of
+// v whose mask holds bit r, or, when v ran out of records, in the per-lane
+// rows.  Nothing else is valid, so neither the rows nor the records need
+// clearing between runs (only the record counts do).
+__global__ void ms_extract_kernel(const int32_t *depth, const uint32_t *parent, const uint4 *rec,
+                                  const uint32_t *rec_cnt, const ull *seen, const int64_t *off,
+                                  int64_t n, int R, int r, int32_t *depth_out, int64_t *parent_out)
 {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
          v += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t d = ((seen[v] >> r) & 1ull) ? depth[v * R + r] : -1;
+        int32_t d = -1;
+        uint32_t par = 0;
+        if ((seen[v] >> r) & 1ull) {
+            const unsigned cnt = min(rec_cnt[v], kRecSlots);
+            bool found = false;
+            for (unsigned i = 0; i < cnt && !found; ++i) {
+                const uint4 x = rec[v * kRecSlots + i];
+                const ull mask = ((ull)x.y << 32) | x.x;
+                if ((mask >> r) & 1ull) {
+                    d = (int32_t)x.w;
+                    par = x.z;
+                    found = true;
+                }
+            }
+            if (!found) {
+                d = depth[v * R + r];
+                par = parent[v * R + r];
+            }
+        }
         if (depth_out) { depth_out[v] = d; }
         if (parent_out) {
             if (d >= 0) {
-                parent_out[v] = (int64_t)parent[v * R + r];
+                parent_out[v] = (int64_t)par;
             } else {
                 const int64_t g = off[v + 1] - off[v];
                 parent_out[v] = g != 0 ? -g : -1;
@@ -754,6 +807,8 @@ struct bd_msbfs {
     ull *qlb[3] = {nullptr, nullptr, nullptr};
     int32_t *depth = nullptr;    // [groups][n][R]
     uint32_t *parent = nullptr;  // [groups][n][R]
+    uint4 *drec = nullptr;       // [groups][n][kRecSlots]
+    uint32_t *drec_cnt = nullptr;  // [groups][n]
     MsCtrl *ctrl = nullptr;
     bd_step *rec = nullptr;
     int64_t *d_sources = nullptr;         // [max_roots]
@@ -804,6 +859,8 @@ MsParams ms_params(bd_msbfs *b, int group, int count)
     }
     const int64_t slice = b->g->n * (int64_t)b->R;
     p.depth = b->depth + group * slice;
+    p.drec = b->drec + group * b->g->n * (int64_t)kRecSlots;
+    p.drec_cnt = b->drec_cnt + group * b->g->n;
     p.parent = b->parent + group * slice;
     p.R = b->R;
     p.all = count >= 64 ? ~0ull : ((1ull << count) - 1);
@@ -832,6 +889,7 @@ bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
 {
     const int64_t n = b->g->n;
     BD_CUDA(cudaMemsetAsync(b->seen + group * n, 0, sizeof(ull) * n, b->stream));
+    BD_CUDA(cudaMemsetAsync(b->drec_cnt + group * n, 0, sizeof(uint32_t) * n, b->stream));
     for (int i = 0; i < 3; ++i) {
         BD_CUDA(cudaMemsetAsync(b->F[i], 0, sizeof(ull) * n, b->stream));
         BD_CUDA(cudaMemsetAsync(b->fb[i], 0, sizeof(uint32_t) * ((n + 31) / 32), b->stream));
@@ -908,6 +966,8 @@ void ms_free(bd_msbfs *b)
     }
     cudaFree(b->depth);
     cudaFree(b->parent);
+    cudaFree(b->drec);
+    cudaFree(b->drec_cnt);
     cudaFree(b->ctrl);
     cudaFree(b->rec);
     cudaFree(b->d_sources);
@@ -939,7 +999,8 @@ bd_status ms_extract(bd_msbfs *b, int32_t root_index, int32_t *depth, int64_t *p
     const size_t bytes = depth ? sizeof(int32_t) * n : sizeof(int64_t) * n;
     BD_CUDA(cudaMalloc(&tmp, bytes));
     ms_extract_kernel<<<ms_grid_for(n), 256, 0, b->stream>>>(
-        b->depth + group * slice, b->parent + group * slice, b->seen + group * n, b->g->d_off, n,
+        b->depth + group * slice, b->parent + group * slice, b->drec + group * n * (int64_t)kRecSlots,
+        b->drec_cnt + group * n, b->seen + group * n, b->g->d_off, n,
         b->R, lane,
         depth ? static_cast<int32_t *>(tmp) : nullptr, parent ? static_cast<int64_t *>(tmp) : nullptr);
     cudaError_t e = cudaGetLastError();
@@ -1005,6 +1066,8 @@ bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *o
     bool ok = cudaMalloc(&b->seen, sizeof(ull) * n * b->groups) == cudaSuccess &&
               cudaMalloc(&b->depth, sizeof(int32_t) * slots) == cudaSuccess &&
               cudaMalloc(&b->parent, sizeof(uint32_t) * slots) == cudaSuccess &&
+              cudaMalloc(&b->drec, sizeof(uint4) * (size_t)n * kRecSlots * b->groups) == cudaSuccess &&
+              cudaMalloc(&b->drec_cnt, sizeof(uint32_t) * (size_t)n * b->groups) == cudaSuccess &&
               cudaMalloc(&b->ctrl, sizeof(MsCtrl)) == cudaSuccess &&
               cudaMalloc(&b->rec, sizeof(bd_step) * kMsRecCap) == cudaSuccess &&
               cudaMalloc(&b->d_sources, sizeof(int64_t) * 64 * b->groups) == cudaSuccess &&
