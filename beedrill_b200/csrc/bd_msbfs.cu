@@ -230,37 +230,121 @@ __device__ void ms_clear_old(const MsParams &p, const MsView &sv)
     }
 }
 
-// push: lanes of frontier vertex u flow into neighbours [b, e).
+// Warp-collective append of up to K new frontier vertices per lane: one
+// atomic for all the small-degree ones of the warp, one for the large ones.
+template <int K>
+__device__ __forceinline__ void ms_append_k(const MsParams &p, MsAcc *acc, int qn,
+                                            const bool (&has)[K], const uint32_t (&v)[K],
+                                            const int64_t (&deg)[K], MsLocal &loc)
+{
+    const int lane = lane_id();
+    unsigned sm[K];
+    bool large[K];
+    unsigned total = 0, any_large = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (has[k]) {
+            loc.vertices += 1;
+            loc.degsum += (ull)deg[k];
+        }
+        large[k] = has[k] && deg[k] >= (int64_t)p.large_deg;
+        sm[k] = __ballot_sync(kFullMask, has[k] && !large[k]);
+        total += __popc(sm[k]);
+        any_large |= __ballot_sync(kFullMask, large[k]);
+    }
+    if (total) {
+        ull base = 0;
+        if (lane == 0) { base = atomicAdd(&acc->small_cnt, (ull)total); }
+        base = __shfl_sync(kFullMask, base, 0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (has[k] && !large[k]) { p.qs[qn][base + __popc(sm[k] & lanemask_lt())] = v[k]; }
+            base += __popc(sm[k]);
+        }
+    }
+    if (any_large) {
+        unsigned count = 0;
+        ull chunks = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (large[k]) {
+                count += 1;
+                chunks += (ull)((deg[k] + p.chunk - 1) / p.chunk);
+            }
+        }
+        const unsigned ci = warp_incl_scan(count);
+        const ull hi = warp_incl_scan(chunks);
+        const unsigned ct = __shfl_sync(kFullMask, ci, 31);
+        const ull ht = __shfl_sync(kFullMask, hi, 31);
+        ull old = 0;
+        if (lane == 0) { old = atomicAdd(&acc->large_packed, ((ull)ct << kLargeShift) | ht); }
+        old = __shfl_sync(kFullMask, old, 0);
+        ull pos = (old >> kLargeShift) + (ci - count);
+        ull cbase = (old & kChunkMask) + (hi - chunks);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (large[k]) {
+                p.ql[qn][pos] = v[k];
+                p.qlb[qn][pos] = cbase;
+                pos += 1;
+                cbase += (ull)((deg[k] + p.chunk - 1) / p.chunk);
+            }
+        }
+    }
+}
+
+// push: lanes of frontier vertex u flow into neighbours [b, e), four arcs
+// per lane per round with each stage's loads and atomics issued back to
+// back.  The atomicOr on the neighbour's next word tells each deliverer
+// which lanes it delivered first; those lanes' depth and parent go to the
+// per-lane rows (every (vertex, lane) pair is delivered exactly once, so the
+// rows and the pull steps' records never hold the same pair).
+constexpr int kPushU = 4;
+
 __device__ __forceinline__ void push_edges(const MsParams &p, MsAcc *acc, int cur, int nxt,
                                            int new_level, uint32_t u, ull bits, int64_t b,
                                            int64_t e, MsLocal &loc)
 {
     const int lane = lane_id();
-    for (int64_t base = b; base < e; base += 32) {
-        const int64_t k = base + lane;
-        bool appended = false;
-        uint32_t v = 0;
-        int64_t deg = 0;
-        if (k < e) {
-            v = __ldg(&p.adj[k]);
-            const ull vis = __ldcg(&p.seen[v]) | frontier_word(p, cur, v);
-            const ull give = bits & ~vis;
-            if (give) {
-                const ull old = atomicOr(&p.F[nxt][v], give);
-                const ull fresh = give & ~old;
-                if (fresh) {
-                    record_shared(p, v, fresh, new_level, u);
-                    loc.lanes += __popcll(fresh);
-                    if (((vis | old | fresh) & p.all) == p.all) { loc.done_degsum += ms_degree(p, v); }
-                }
-                if (old == 0ull) {
-                    atomicOr(&p.fb[nxt][v >> 5], 1u << (v & 31));
-                    appended = true;
-                    deg = ms_degree(p, v);
-                }
-            }
+    for (int64_t base = b; base < e; base += 32 * kPushU) {
+        uint32_t v[kPushU];
+        bool in[kPushU];
+#pragma unroll
+        for (int i = 0; i < kPushU; ++i) {
+            const int64_t k = base + 32 * i + lane;
+            in[i] = k < e;
+            v[i] = in[i] ? __ldg(&p.adj[k]) : 0u;
         }
-        ms_append(p, acc, nxt, appended, v, deg, loc);
+        ull vis[kPushU];
+#pragma unroll
+        for (int i = 0; i < kPushU; ++i) {
+            vis[i] = in[i] ? (__ldcg(&p.seen[v[i]]) | frontier_word(p, cur, v[i])) : ~0ull;
+        }
+        ull old[kPushU], give[kPushU];
+#pragma unroll
+        for (int i = 0; i < kPushU; ++i) {
+            give[i] = bits & ~vis[i];
+            old[i] = give[i] ? atomicOr(&p.F[nxt][v[i]], give[i]) : ~0ull;
+        }
+        bool first[kPushU];
+        int64_t deg[kPushU];
+#pragma unroll
+        for (int i = 0; i < kPushU; ++i) {
+            const ull fresh = give[i] & ~old[i];
+            first[i] = give[i] != 0 && old[i] == 0ull;
+            deg[i] = 0;
+            if (fresh) {
+                write_rows(p, v[i], fresh, new_level, u);
+                loc.lanes += __popcll(fresh);
+            }
+            if (first[i] || (fresh && ((vis[i] | old[i] | fresh) & p.all) == p.all)) {
+                deg[i] = ms_degree(p, v[i]);
+            }
+            if (fresh && ((vis[i] | old[i] | fresh) & p.all) == p.all) { loc.done_degsum += (ull)deg[i]; }
+            if (first[i]) { atomicOr(&p.fb[nxt][v[i] >> 5], 1u << (v[i] & 31)); }
+            if (!first[i]) { deg[i] = 0; }
+        }
+        ms_append_k<kPushU>(p, acc, nxt, first, v, deg, loc);
     }
 }
 
