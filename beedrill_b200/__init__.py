@@ -165,6 +165,7 @@ def lib() -> ctypes.CDLL:
         "bd_msbfs_get_parents": (c_int, [c_void_p, c_int32, i64p]),
         "bd_msbfs_count_traversed_edges": (c_int, [c_void_p, c_int32, i64p, i64p]),
         "bd_msbfs_get_steps": (c_int, [c_void_p, POINTER(Step), c_int64, i64p]),
+        "bd_msbfs_check": (c_int, [c_void_p, c_int32, POINTER(c_int32)]),
         "bd_msbfs_destroy": (c_int, [c_void_p]),
         "bd_msbfs_set_policy": (c_int, [c_void_p, f32p, f32p, f32p, f32p, f32p, c_float]),
         "bd_policy_forward": (c_int, [f32p, f32p, c_int64, f32p]),
@@ -538,6 +539,12 @@ class BatchedBFS:
         r = c_int64()
         _check(lib().bd_msbfs_count_traversed_edges(self._h, i, None, byref(r)), "msbfs count")
         return r.value
+
+    # hybrid_bfs::check (hybrid_bfs.cc:281-379) of root i's parents
+    def check(self, i: int) -> bool:
+        ok = c_int32()
+        _check(lib().bd_msbfs_check(self._h, i, byref(ok)), "msbfs check")
+        return bool(ok.value)
 
     def counts(self):
         """(m_c, n_c) arrays over the roots of the last run."""

@@ -64,6 +64,9 @@ struct PolicyBlob;
 // Host-side PolicyBlob from the ABI's arrays (bd_policy.cu).
 bd_status policy_blob(const float *params, const float *mean, const float *inv_std,
                       const float *lo, const float *hi, float margin, PolicyBlob *blob);
+// hybrid_bfs::check on the host for a parent array in the reference's
+// encoding; *ok = 1 when it passes.
+bd_status check_parents(const bd_graph *g, int64_t source, const int64_t *parent, int32_t *ok);
 // Fills d_isolated from d_off.
 bd_status graph_finish(bd_graph *g, cudaStream_t s);
 void graph_free(bd_graph *g);

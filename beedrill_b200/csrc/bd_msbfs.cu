@@ -901,6 +901,7 @@ struct bd_msbfs {
     int grid = 0;
     int block = 512;
     int count = 0;  // roots in the last run
+    std::vector<int64_t> sources;  // roots of the last run
     bool ran = false;
     PolicyBlob *policy = nullptr;  // device copy, or null
     uint32_t *heavy = nullptr;
@@ -1224,6 +1225,7 @@ bd_status bd_msbfs_run(bd_msbfs *b, const int64_t *sources, int32_t count, bd_ru
     BD_CUDA(cudaMemcpyAsync(&b->last, b->ctrl, sizeof(MsCtrl), cudaMemcpyDeviceToHost, b->stream));
     BD_CUDA(cudaStreamSynchronize(b->stream));
     b->count = count;
+    b->sources.assign(sources, sources + count);
     b->ran = true;
     if (b->last.error) { return (bd_status)b->last.error; }
     if (stats) {
@@ -1255,6 +1257,15 @@ bd_status bd_msbfs_get_parents(bd_msbfs *b, int32_t root_index, int64_t *parent)
 {
     if (!b || !parent) { return BD_ERR_INVALID; }
     return ms_extract(b, root_index, nullptr, parent);
+}
+
+bd_status bd_msbfs_check(bd_msbfs *b, int32_t root_index, int32_t *ok)
+{
+    if (!b || !ok) { return BD_ERR_INVALID; }
+    BD_TRY(ms_check_root(b, root_index));
+    std::vector<int64_t> parent(b->g->n);
+    BD_TRY(ms_extract(b, root_index, nullptr, parent.data()));
+    return check_parents(b->g, b->sources[root_index], parent.data(), ok);
 }
 
 bd_status bd_msbfs_count_traversed_edges(bd_msbfs *b, int32_t root_index, int64_t *edges,

@@ -9,8 +9,18 @@
 //   --min_parent       deterministic parents: smallest neighbour one level up
 //   --dump_depths F    write the int32 depth array of the last trial to F
 //   --root_seed S      lcg(S) instead of lcg(0) for the root picker
+//   --policy_file F    trained direction policy for --algorithm learned
+//                      (default: ../policy/learned_policy.json, or
+//                      learned_policy_batched.json with --batched, beside
+//                      this binary's directory)
+//   --batched          run all trials' roots together (64 per group, one
+//                      captured launch); per-root lines report the batch
+//                      time divided evenly
+//   --degree_order     neighbour lists ordered by neighbour degree, highest
+//                      first (results are unchanged)
 // Algorithms: the reference's four names plus top_down, bottom_up, learned.
 #include <getopt.h>
+#include <unistd.h>
 
 #include <cmath>
 #include <cstdio>
@@ -45,6 +55,9 @@ const struct option long_options[] = {
     {"root_seed", required_argument, nullptr, 0},
     {"min_parent", no_argument, nullptr, 0},
     {"dump_depths", required_argument, nullptr, 0},
+    {"policy_file", required_argument, nullptr, 0},
+    {"batched", no_argument, nullptr, 0},
+    {"degree_order", no_argument, nullptr, 0},
     {nullptr, 0, nullptr, 0},
 };
 
@@ -71,6 +84,9 @@ void print_help(const char *argv0)
     printf("\t--root_seed S        Root picker seed (default 0, as the reference)\n");
     printf("\t--min_parent         Deterministic parents (smallest neighbour one level up)\n");
     printf("\t--dump_depths FILE   Write the depth array (int32) of the last trial\n");
+    printf("\t--policy_file FILE   Trained direction policy for --algorithm learned\n");
+    printf("\t--batched            Run all trials' roots together (64 per group)\n");
+    printf("\t--degree_order       Order neighbour lists by neighbour degree\n");
     printf("\t--version            Print version info\n");
     printf("\t--help               Print command line help\n");
 }
@@ -93,6 +109,9 @@ struct bfs_args {
     unsigned long root_seed = 0;
     bool min_parent = false;
     const char *dump_depths = nullptr;
+    const char *policy_file = nullptr;
+    bool batched = false;
+    bool degree_order = false;
 };
 
 bfs_args parse(int argc, char **argv)
@@ -125,6 +144,9 @@ bfs_args parse(int argc, char **argv)
         else if (name == "root_seed") { a.root_seed = strtoul(optarg, nullptr, 10); }
         else if (name == "min_parent") { a.min_parent = true; }
         else if (name == "dump_depths") { a.dump_depths = optarg; }
+        else if (name == "policy_file") { a.policy_file = optarg; }
+        else if (name == "batched") { a.batched = true; }
+        else if (name == "degree_order") { a.degree_order = true; }
         else if (name == "version") {
             printf("%s\n", bd_version());
             exit(0);
@@ -155,6 +177,88 @@ int alg_code(const char *name)
     return -1;
 }
 
+// The trained policy beside this binary (beedrill_b200/bin -> beedrill_b200/policy).
+std::string default_policy(bool batched)
+{
+    char exe[4096];
+    const ssize_t len = readlink("/proc/self/exe", exe, sizeof(exe) - 1);
+    std::string dir = ".";
+    if (len > 0) {
+        exe[len] = '\0';
+        dir = exe;
+        const size_t slash = dir.rfind('/');
+        dir = slash == std::string::npos ? "." : dir.substr(0, slash);
+    }
+    return dir + (batched ? "/../policy/learned_policy_batched.json" : "/../policy/learned_policy.json");
+}
+
+// Loads the policy for --algorithm learned; without a file the rule decides.
+bool find_policy(const bfs_args &args, beedrill::policy *pol)
+{
+    const std::string path = args.policy_file ? args.policy_file : default_policy(args.batched);
+    if (access(path.c_str(), R_OK) != 0) {
+        if (args.policy_file) { throw beedrill::error(BD_ERR_IO, "policy file " + path); }
+        printf("No policy file %s: the rule decides every step\n", path.c_str());
+        return false;
+    }
+    *pol = beedrill::load_policy(path);
+    return true;
+}
+
+void report(long edges, double ms, const std::string &dirs, long *edges_all, double *ms_all,
+            double *inv_sum)
+{
+    *edges_all += edges;
+    *ms_all += ms;
+    const double mteps = (1e-6 * edges) / (ms / 1000);
+    *inv_sum += 1.0 / mteps;
+    printf("Traversed %li edges in %3.4f ms, %3.2f MTEPS (steps %s)\n", edges, ms, mteps,
+           dirs.c_str());
+}
+
+bool write_depths(const char *path, const std::vector<int32_t> &d)
+{
+    FILE *fp = fopen(path, "wb");
+    const bool ok = fp && fwrite(d.data(), sizeof(int32_t), d.size(), fp) == d.size();
+    if (!ok) { printf("Cannot write %s\n", path); }
+    if (fp) { fclose(fp); }
+    return ok;
+}
+
+// --batched: every trial's root in one call of the batched traversal.
+bool run_batched(const bfs_args &args, beedrill::graph &g, int alg, const std::vector<int64_t> &roots)
+{
+    bool success = true;
+    bd_msbfs_opts opts;
+    bd_msbfs_default_opts(&opts);
+    if (alg == BD_ALG_TOP_DOWN) { opts.force_dir = 0; }
+    if (alg == BD_ALG_BOTTOM_UP) { opts.force_dir = 1; }
+    beedrill::batched_bfs bfs(g, (int32_t)roots.size(), &opts);
+    beedrill::policy pol;
+    if (alg == BD_ALG_LEARNED && find_policy(args, &pol)) { bfs.set_policy(pol); }
+    printf("Doing breadth-first search from %zu vertices in one batch\n", roots.size());
+    bfs.run(roots);
+    const double ms = bfs.last_stats().ms / (double)roots.size();
+    long edges_all = 0;
+    double ms_all = 0, inv_sum = 0;
+    for (size_t s = 0; s < roots.size(); ++s) {
+        if (args.check_results) {
+            int32_t ok = 0;
+            beedrill::throw_if(bd_msbfs_check(bfs.handle(), (int32_t)s, &ok), "check");
+            printf("Checking results...\n%s\n", ok ? "PASS" : "FAIL");
+            success = success && ok;
+        }
+        report(bfs.count_num_traversed_edges((int32_t)s), ms, "batched", &edges_all, &ms_all,
+               &inv_sum);
+    }
+    if (args.dump_depths) {
+        success = write_depths(args.dump_depths, bfs.depths((int32_t)roots.size() - 1)) && success;
+    }
+    printf("Mean performance over all trials: %3.2f MTEPS \n", (1e-6 * edges_all) / (ms_all / 1000));
+    printf("Harmonic mean over all trials: %3.2f MTEPS \n", roots.size() / inv_sum);
+    return success;
+}
+
 }  // namespace
 
 int main(int argc, char **argv)
@@ -162,7 +266,9 @@ int main(int argc, char **argv)
     bool success = true;
     bfs_args args = parse(argc, argv);
     try {
-        const int32_t order = args.sort_edge_blocks ? BD_ORDER_SORTED : BD_ORDER_INSERTION;
+        const int32_t order = args.degree_order       ? BD_ORDER_DEGREE
+                              : args.sort_edge_blocks ? BD_ORDER_SORTED
+                                                      : BD_ORDER_INSERTION;
         beedrill::graph g = args.rmat_scale > 0
                                 ? beedrill::graph::rmat(args.rmat_scale, args.edge_factor, args.seed,
                                                         0.57, 0.19, 0.19, 0.05, order)
@@ -199,6 +305,13 @@ int main(int argc, char **argv)
             exit(1);
         }
         printf("Initializing BFS data structures...\n");
+        std::vector<int64_t> roots;
+        if (args.source_vertex < 0) {
+            roots = g.pick_roots(args.root_seed, args.num_trials);
+        } else {
+            roots.assign(args.num_trials, args.source_vertex);
+        }
+        if (args.batched) { return run_batched(args, g, alg, roots) && success ? 0 : 1; }
         bd_bfs_opts opts;
         bd_bfs_default_opts(&opts);
         opts.alg = alg;
@@ -206,12 +319,12 @@ int main(int argc, char **argv)
         opts.beta = args.beta;
         opts.min_parent = args.min_parent ? 1 : 0;
         beedrill::hybrid_bfs bfs(g, &opts);
-        std::vector<int64_t> roots;
-        if (args.source_vertex < 0) { roots = g.pick_roots(args.root_seed, args.num_trials); }
+        beedrill::policy pol;
+        if (alg == BD_ALG_LEARNED && find_policy(args, &pol)) { bfs.set_policy(pol); }
         long edges_all = 0;
         double ms_all = 0, inv_sum = 0;
         for (long s = 0; s < args.num_trials; ++s) {
-            const long source = args.source_vertex >= 0 ? args.source_vertex : (long)roots[s];
+            const long source = (long)roots[s];
             bfs.clear();
             printf("Doing breadth-first search from vertex %li (sample %li of %li)\n", source, s + 1,
                    args.num_trials);
@@ -226,23 +339,11 @@ int main(int argc, char **argv)
                     success = false;
                 }
             }
-            const long edges = bfs.count_num_traversed_edges();
-            edges_all += edges;
-            ms_all += ms;
-            const double mteps = (1e-6 * edges) / (ms / 1000);
-            inv_sum += 1.0 / mteps;
             std::string dirs;
             for (const bd_step &st : bfs.steps()) { dirs += st.dir ? 'B' : 'T'; }
-            printf("Traversed %li edges in %3.4f ms, %3.2f MTEPS (steps %s)\n", edges, ms, mteps,
-                   dirs.c_str());
+            report(bfs.count_num_traversed_edges(), ms, dirs, &edges_all, &ms_all, &inv_sum);
             if (args.dump_depths && s == args.num_trials - 1) {
-                std::vector<int32_t> d = bfs.depths();
-                FILE *fp = fopen(args.dump_depths, "wb");
-                if (!fp || fwrite(d.data(), sizeof(int32_t), d.size(), fp) != d.size()) {
-                    printf("Cannot write %s\n", args.dump_depths);
-                    success = false;
-                }
-                if (fp) { fclose(fp); }
+                success = write_depths(args.dump_depths, bfs.depths()) && success;
             }
         }
         printf("Mean performance over all trials: %3.2f MTEPS \n",

@@ -182,13 +182,118 @@ def impl_reference(args):
     return 0
 
 
+WORKLOADS = {
+    # the headline: RMAT scale 24, 64 roots
+    "rmat24": {"kind": "rmat", "scale": 24, "roots": 64},
+    # plain Beamer, one root per launch, at scale 22
+    "rmat22": {"kind": "rmat", "scale": 22, "roots": 64},
+    # 256 roots in four 64-lane groups of one captured launch
+    "rmat20-256": {"kind": "rmat", "scale": 20, "roots": 256},
+    # the largest single-GPU case
+    "rmat26": {"kind": "rmat", "scale": 26, "roots": 64},
+    # high-diameter contrast: 4096 x 4096 grid, 1% of its edges deleted
+    "grid4096": {"kind": "grid", "rows": 4096, "cols": 4096, "delete": 0.01, "roots": 64},
+    # 512 independent RMAT graphs (scales 10-18, edge factors 4-32), one root each
+    "packed512": {"kind": "packed", "graphs": 512},
+}
+
+
+def packed_parts(bd, count: int, order: int):
+    """The packed-graphs workload: seeded scales 10-18 and edge factors
+    4-32, graph i generated with seed 5000 + i, root lcg(i) of graph i."""
+    rng = np.random.default_rng(512)
+    scales = rng.integers(10, 19, count)
+    factors = rng.integers(4, 33, count)
+    return [bd.Graph.rmat(int(s), int(f), seed=5000 + i, order=order)
+            for i, (s, f) in enumerate(zip(scales, factors))]
+
+
+def bench_packed(args, w, bd, order, local):
+    """512 graphs packed into one CSR: one multi-source launch over all of
+    them ("batched") against one launch per graph on its own CSR ("plain").
+    GTEPS = sum of m_c over all graphs / time of the step."""
+    t_gen = time.time()
+    parts = packed_parts(bd, w["graphs"], order)
+    g, base = bd.Graph.concat(parts)
+    gen_s = time.time() - t_gen
+    roots = np.array([int(p.pick_roots(i, 1)[0]) + int(base[i]) for i, p in enumerate(parts)],
+                     np.int64)
+    n, m = g.num_vertices(), g.num_edges()
+    multi = bd.HybridBFS(g)
+    singles = [bd.HybridBFS(p) for p in parts]
+
+    def one_step():
+        t0 = time.perf_counter()
+        multi.clear()
+        st = multi.run_multi(roots)
+        edges = multi.count_num_traversed_edges()
+        wall_multi = (time.perf_counter() - t0) * 1e3
+        ms_multi = st.ms
+        t0 = time.perf_counter()
+        ms_single, edges_single = 0.0, 0
+        for i, (h, p) in enumerate(zip(singles, parts)):
+            h.clear()
+            ms_single += h.run(int(roots[i] - base[i])).ms
+            edges_single += h.count_num_traversed_edges()
+        wall_single = (time.perf_counter() - t0) * 1e3
+        return {"batched": (ms_multi, edges, wall_multi), "plain": (ms_single, edges_single, wall_single)}
+
+    for _ in range(args.warmup):
+        one_step()
+    runs = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            runs.append(one_step())
+    modes = {}
+    for name in ("batched", "plain"):
+        ms = np.array([r[name][0] for r in runs])
+        edges = np.array([r[name][1] for r in runs])
+        wall = np.array([r[name][2] for r in runs])
+        modes[name] = {"gteps": float(edges.sum() / (ms.sum() * 1e-3) / 1e9),
+                       "e2e_gteps": float(edges.sum() / (wall.sum() * 1e-3) / 1e9),
+                       "ms_per_step": float(ms.mean()), "edges": int(edges[0])}
+    if modes["batched"]["edges"] != modes["plain"]["edges"]:
+        raise RuntimeError("packed and per-graph runs disagree on m_c")
+    head = modes["batched"]
+    peak, peak_kind = peaks()
+    # one pass over the packed CSR plus every vertex's depth and parent
+    b_alg = 8.0 * (n + 1) + 8.0 * m + 12.0 * n
+    achieved = b_alg / (head["ms_per_step"] * 1e-3) / 1e9
+    line = {
+        "metric": f"aggregate GTEPS, {w['graphs']} packed RMAT graphs (scales 10-18), one root each, 1 B200",
+        "value": head["gteps"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": args.workload, "graphs": w["graphs"], "num_vertices": n,
+                   "num_edges": m, "adjacency_order": args.order,
+                   "l2": "inputs larger than L2 (CSR %.2f GB)" % ((8 * (n + 1) + 8 * m) / 1e9),
+                   "graph_build_s": round(gen_s, 2), "parallelism": "1 GPU"},
+        "modes": {k: {kk: vv for kk, vv in v.items() if kk != "edges"} for k, v in modes.items()},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "note": "B_alg = 8(n+1) + 8m + 12n per multi-source launch"},
+        "e2e": {"value": head["e2e_gteps"], "unit": UNIT, "h2d_bytes_per_step": 8 * len(roots),
+                "d2h_bytes_per_step": 8,
+                "note": "public API calls per step: clear, run_multi (root upload), m_c download"},
+        "gpu_launches": args.steps * (3 + 3 * len(parts)),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    multi.close()
+    for h in singles:
+        h.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scale", type=int, default=SCALE)
+    ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS),
+                    help="rmat24 is the headline; the others are the remaining evaluation cases")
+    ap.add_argument("--scale", type=int, default=None, help="override the RMAT scale")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-roots", type=int, default=3)
     ap.add_argument("--order", default="degree", choices=["insertion", "sorted", "degree"],
@@ -206,23 +311,42 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     bd.lib().bd_set_device(local)
 
-    scale = args.scale
-    t_gen = time.time()
+    w = dict(WORKLOADS[args.workload])
     order = {"insertion": bd.ORDER_INSERTION, "sorted": bd.ORDER_SORTED,
              "degree": bd.ORDER_DEGREE}[args.order]
-    g = bd.Graph.rmat(scale, EDGE_FACTOR, seed=GRAPH_SEED, order=order)
+    if w["kind"] == "packed":
+        if world > 1:
+            raise SystemExit("packed512 runs on one GPU")
+        return bench_packed(args, w, bd, order, local)
+    num_roots = w["roots"]
+    t_gen = time.time()
+    if w["kind"] == "rmat":
+        scale = args.scale or w["scale"]
+        g = bd.Graph.rmat(scale, EDGE_FACTOR, seed=GRAPH_SEED if scale == SCALE else scale,
+                          order=order)
+        graph_seed = GRAPH_SEED if scale == SCALE else scale
+        desc = f"rmat-scale{scale}-ef{EDGE_FACTOR} seed {graph_seed}"
+        metric = METRIC if (scale == SCALE and num_roots == NUM_ROOTS) else \
+            f"harmonic-mean GTEPS over {num_roots} roots, RMAT scale {scale}, 1 B200"
+    else:
+        scale = None
+        graph_seed = 0
+        g = bd.Graph.grid(w["rows"], w["cols"], w["delete"], graph_seed, order=order)
+        desc = f"grid {w['rows']}x{w['cols']}, {w['delete']:.0%} of edges deleted, seed {graph_seed}"
+        metric = f"harmonic-mean GTEPS over {num_roots} roots, {desc}, 1 B200"
     gen_s = time.time() - t_gen
     n, m = g.num_vertices(), g.num_edges()
-    roots = g.pick_roots(rank, NUM_ROOTS)
+    roots = g.pick_roots(rank, num_roots)
 
     # CPU baseline: the reference's own build on a bounded sample of the same
     # workload, in the background while the GPU is measured (rank 0, N = 1).
     cpu_thread = None
     cpu_result = {}
     tmpdir = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_BIN):
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_BIN) \
+            and m <= 300_000_000:
         tmpdir = tempfile.TemporaryDirectory(dir=os.environ.get("BD_TMP", None))
-        el64 = os.path.join(tmpdir.name, f"rmat{scale}.el64")
+        el64 = os.path.join(tmpdir.name, "graph.el64")
         g.write_el64(el64)
 
         def cpu_job():
@@ -234,18 +358,21 @@ def main():
         cpu_thread = threading.Thread(target=cpu_job, daemon=True)
         cpu_thread.start()
 
-    # the three ways of running the 64 roots
+    # the ways of running the roots: one launch per root under the Beamer
+    # rule and under the learned policy; all roots batched (64 per group)
+    # under the learned push/pull policy and under the plain rule
     plain = bd.HybridBFS(g, alg="beamer_hybrid")
     learned = None
     from beedrill_b200 import policy as P
     if os.path.exists(P.DEFAULT_PATH):
         learned = bd.HybridBFS(g, alg="learned")
         P.Policy.load().install(learned)
-    batched = bd.BatchedBFS(g, NUM_ROOTS)
+    batched = bd.BatchedBFS(g, num_roots)
     batched_rule = None
     if os.path.exists(P.BATCHED_PATH):
         P.Policy.load(P.BATCHED_PATH).install(batched)
-        batched_rule = bd.BatchedBFS(g, NUM_ROOTS)
+        batched_rule = bd.BatchedBFS(g, num_roots)
+    groups = (num_roots + 63) // 64
 
     def one_step():
         out = {}
@@ -259,9 +386,9 @@ def main():
                 continue
             t0 = time.perf_counter()
             st = h.run(roots)
-            wall = (time.perf_counter() - t0) * 1e3
             m_c, n_c = h.counts()
-            out[name] = (np.full(NUM_ROOTS, st.ms / NUM_ROOTS), m_c, n_c, wall)
+            wall = (time.perf_counter() - t0) * 1e3
+            out[name] = (np.full(num_roots, st.ms / num_roots), m_c, n_c, wall)
         return out
 
     for _ in range(args.warmup):
@@ -283,13 +410,18 @@ def main():
         edges = np.concatenate([r[name][1] for r in runs])
         reached = np.concatenate([r[name][2] for r in runs])
         gteps = edges / (ms * 1e-3) / 1e9
-        e2e = hmean(np.concatenate([r[name][1] / (r[name][3] / NUM_ROOTS * 1e-3) / 1e9 for r in runs]))
+        e2e = hmean(np.concatenate([r[name][1] / (r[name][3] / num_roots * 1e-3) / 1e9 for r in runs]))
         step_ms = float(np.mean([r[name][0].sum() for r in runs]))
         if name.startswith("batched"):
-            # one shared CSR pass per 64-root launch, plus every root's
-            # depth and parent outputs, spread evenly over its roots
-            per_launch = 8.0 * (n + 1) + 8.0 * m + 12.0 * reached.reshape(-1, NUM_ROOTS).sum(1)
-            b_alg = np.repeat(per_launch / NUM_ROOTS, NUM_ROOTS)
+            # one shared CSR pass per 64-root group, plus every root's depth
+            # and parent outputs, spread evenly over the group's roots
+            per_root = np.zeros(len(reached))
+            for s in range(0, len(reached), num_roots):
+                for g0 in range(0, num_roots, 64):
+                    lo, hi = s + g0, s + min(g0 + 64, num_roots)
+                    b = 8.0 * (n + 1) + 8.0 * m + 12.0 * reached[lo:hi].sum()
+                    per_root[lo:hi] = b / (hi - lo)
+            b_alg = per_root
         else:
             b_alg = 8.0 * (n + 1) + 8.0 * edges + 12.0 * reached
         return {"gteps": hmean(gteps), "e2e": e2e, "step_ms": step_ms, "ms": ms, "edges": edges,
@@ -313,26 +445,26 @@ def main():
     else:
         value, e2e_value = value_rank, e2e_rank
 
-    # roofline of the dominant kernel of the headline mode, B_alg per root
-    # = 8(n+1) + 4*(2 m_c) + 12 n_c (the batched launch shares one CSR pass
-    # among 64 roots; its B_alg is counted per root as for single runs)
+    # roofline of the dominant kernel of the headline mode: B_alg per root
+    # = 8(n+1) + 4*(2 m_c) + 12 n_c for one-root launches; a batched group
+    # shares one CSR pass among its 64 roots
     achieved = float(head["b_alg"].sum() / (head["ms"].sum() * 1e-3) / 1e9)
     peak, peak_kind = peaks()
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(f"rmat{scale}-{best}", {}).get("bytes_per_launch")
+            traffic = json.load(f).get(f"{args.workload}-{best}", {}).get("bytes_per_launch")
     ms = head["ms"]
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {
-            "workload": f"rmat-scale{scale}-ef{EDGE_FACTOR} seed {GRAPH_SEED}, {NUM_ROOTS} roots per step",
+            "workload": f"{desc}, {num_roots} roots per step",
             "mode": best,
-            "scale": scale, "edge_factor": EDGE_FACTOR, "graph_seed": GRAPH_SEED,
-            "num_vertices": n, "num_edges": m, "roots": NUM_ROOTS, "root_seed": rank,
+            "scale": scale, "edge_factor": EDGE_FACTOR if scale else None, "graph_seed": graph_seed,
+            "num_vertices": n, "num_edges": m, "roots": num_roots, "root_seed": rank,
             "l2": "inputs larger than L2 (CSR %.2f GB)" % ((8 * (n + 1) + 8 * m) / 1e9),
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
             "graph_build_s": round(gen_s, 2),
@@ -347,14 +479,14 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind,
-                     "note": ("B_alg per 64-root launch = 8(n+1) + 8m + 12 sum n_c" if best == "batched"
+                     "note": ("B_alg per 64-root group = 8(n+1) + 8m + 12 sum n_c" if best.startswith("batched")
                               else "B_alg = 8(n+1) + 8 m_c + 12 n_c per root") + " over the run time"},
         "e2e": {"value": e2e_value, "unit": UNIT,
-                "h2d_bytes_per_step": 8 * NUM_ROOTS,
-                "d2h_bytes_per_step": 16 * NUM_ROOTS,
+                "h2d_bytes_per_step": 8 * num_roots,
+                "d2h_bytes_per_step": 16 * num_roots,
                 "note": "public API call per step: root upload, clear + runs, m_c/n_c download"},
-        "gpu_launches": args.steps * (3 * NUM_ROOTS * (1 + (learned is not None))
-                                      + 3 * (1 + (batched_rule is not None))),
+        "gpu_launches": args.steps * (3 * num_roots * (1 + (learned is not None))
+                                      + 3 * groups * (1 + (batched_rule is not None))),
         "clocks": clocks.summary(),
     }
     if cpu_thread is not None:

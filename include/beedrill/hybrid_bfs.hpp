@@ -11,6 +11,8 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -30,6 +32,67 @@ public:
 inline void throw_if(bd_status s, const char *what)
 {
     if (s != BD_OK) { throw error(s, what); }
+}
+
+// A trained direction policy as the trainer (beedrill_b200/policy.py) writes
+// it: a JSON object with the float arrays "params" (BD_POLICY_PARAMS),
+// "mean", "inv_std", optionally "lo" and "hi" (BD_POLICY_FEATURES each), and
+// the number "margin".  No counterpart in the reference.
+struct policy {
+    std::vector<float> params, mean, inv_std, lo, hi;
+    float margin = 0.f;
+};
+
+namespace detail {
+// The numbers of the JSON array stored under "key" (empty if absent).
+inline std::vector<float> json_array(const std::string &text, const char *key)
+{
+    std::vector<float> out;
+    const std::string k = std::string("\"") + key + "\"";
+    size_t at = text.find(k);
+    if (at == std::string::npos) { return out; }
+    at = text.find_first_not_of(" \t\r\n:", at + k.size());
+    if (at == std::string::npos || text[at] != '[') { return out; }
+    const char *p = text.c_str() + at + 1;
+    while (*p && *p != ']') {
+        char *end = nullptr;
+        const double v = strtod(p, &end);
+        if (end == p) { throw error(BD_ERR_FORMAT, std::string("policy array ") + key); }
+        out.push_back((float)v);
+        p = end;
+        while (*p == ',' || *p == ' ' || *p == '\n' || *p == '\r' || *p == '\t') { ++p; }
+    }
+    return out;
+}
+}  // namespace detail
+
+inline policy load_policy(const std::string &path)
+{
+    FILE *fp = fopen(path.c_str(), "rb");
+    if (!fp) { throw error(BD_ERR_IO, "policy file " + path); }
+    std::string text;
+    char buf[65536];
+    size_t got;
+    while ((got = fread(buf, 1, sizeof(buf), fp)) > 0) { text.append(buf, got); }
+    fclose(fp);
+    policy pol;
+    pol.params = detail::json_array(text, "params");
+    pol.mean = detail::json_array(text, "mean");
+    pol.inv_std = detail::json_array(text, "inv_std");
+    pol.lo = detail::json_array(text, "lo");
+    pol.hi = detail::json_array(text, "hi");
+    const size_t at = text.find("\"margin\"");
+    if (at != std::string::npos) {
+        const size_t colon = text.find(':', at);
+        if (colon != std::string::npos) { pol.margin = strtof(text.c_str() + colon + 1, nullptr); }
+    }
+    const bool bounded = !pol.lo.empty() || !pol.hi.empty();
+    if (pol.params.size() != BD_POLICY_PARAMS || pol.mean.size() != BD_POLICY_FEATURES ||
+        pol.inv_std.size() != BD_POLICY_FEATURES ||
+        (bounded && (pol.lo.size() != BD_POLICY_FEATURES || pol.hi.size() != BD_POLICY_FEATURES))) {
+        throw error(BD_ERR_FORMAT, "policy file " + path);
+    }
+    return pol;
 }
 
 // The graph (graph_base.h): a CSR in HBM.
@@ -145,6 +208,14 @@ public:
     }
     // Runs the policy the handle was created with (beamer / learned / ...).
     void run(long source) { throw_if(bd_bfs_run(h_, source, &stats_), "run"); }
+    // The network BD_ALG_LEARNED consults (Beamer decides without one).
+    void set_policy(const policy &p)
+    {
+        throw_if(bd_bfs_set_policy(h_, p.params.data(), p.mean.data(), p.inv_std.data(),
+                                   p.lo.empty() ? nullptr : p.lo.data(),
+                                   p.hi.empty() ? nullptr : p.hi.data(), p.margin),
+                 "set_policy");
+    }
 
     bool check(long source)
     {
@@ -202,6 +273,68 @@ public:
 private:
     graph &g_;
     bd_bfs *h_ = nullptr;
+    bd_run_stats stats_{};
+};
+
+// Many roots per pass over the graph (64 per group, all groups of a call as
+// one captured CUDA graph).  Per root, the results read like hybrid_bfs's.
+// No counterpart in the reference, whose driver runs its roots one by one
+// (hybrid_bfs_main.cc:252-302).
+class batched_bfs {
+public:
+    batched_bfs(graph &g, int32_t max_roots, const bd_msbfs_opts *opts = nullptr) : g_(g)
+    {
+        throw_if(bd_msbfs_create(g.handle(), max_roots, opts, &h_), "batched_bfs");
+    }
+    batched_bfs(const batched_bfs &) = delete;
+    batched_bfs &operator=(const batched_bfs &) = delete;
+    ~batched_bfs()
+    {
+        if (h_) { bd_msbfs_destroy(h_); }
+    }
+    void run(const std::vector<int64_t> &sources)
+    {
+        throw_if(bd_msbfs_run(h_, sources.data(), (int32_t)sources.size(), &stats_), "run");
+    }
+    void set_policy(const policy &p)
+    {
+        throw_if(bd_msbfs_set_policy(h_, p.params.data(), p.mean.data(), p.inv_std.data(),
+                                     p.lo.empty() ? nullptr : p.lo.data(),
+                                     p.hi.empty() ? nullptr : p.hi.data(), p.margin),
+                 "set_policy");
+    }
+    long count_num_traversed_edges(int32_t i)
+    {
+        int64_t m = 0;
+        throw_if(bd_msbfs_count_traversed_edges(h_, i, &m, nullptr), "count_num_traversed_edges");
+        return (long)m;
+    }
+    std::vector<int32_t> depths(int32_t i)
+    {
+        std::vector<int32_t> d(g_.num_vertices());
+        throw_if(bd_msbfs_get_depths(h_, i, d.data()), "depths");
+        return d;
+    }
+    std::vector<int64_t> parents(int32_t i)
+    {
+        std::vector<int64_t> p(g_.num_vertices());
+        throw_if(bd_msbfs_get_parents(h_, i, p.data()), "parents");
+        return p;
+    }
+    std::vector<bd_step> steps()
+    {
+        int64_t count = 0;
+        throw_if(bd_msbfs_get_steps(h_, nullptr, 0, &count), "steps");
+        std::vector<bd_step> s(count);
+        throw_if(bd_msbfs_get_steps(h_, s.data(), count, &count), "steps");
+        return s;
+    }
+    const bd_run_stats &last_stats() const { return stats_; }
+    bd_msbfs *handle() const { return h_; }
+
+private:
+    graph &g_;
+    bd_msbfs *h_ = nullptr;
     bd_run_stats stats_{};
 };
 

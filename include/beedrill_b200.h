@@ -251,6 +251,8 @@ bd_status bd_msbfs_get_parents(bd_msbfs *b, int32_t root_index, int64_t *parent)
 /* count_num_traversed_edges() (m_c) and reached vertices (n_c) of one root. */
 bd_status bd_msbfs_count_traversed_edges(bd_msbfs *b, int32_t root_index, int64_t *edges,
                                          int64_t *reached);
+/* hybrid_bfs::check (hybrid_bfs.cc:281-379) of one root's parents. */
+bd_status bd_msbfs_check(bd_msbfs *b, int32_t root_index, int32_t *ok);
 /* Step records of the last group of the last call (found = new lanes). */
 bd_status bd_msbfs_get_steps(bd_msbfs *b, bd_step *steps, int64_t capacity, int64_t *count);
 /* Installs (params != NULL) or removes the learned push/pull policy of the

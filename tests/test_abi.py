@@ -61,3 +61,39 @@ def test_invalid_arguments_rejected_without_device():
     assert L.bd_graph_rmat(0, 16, 0.57, 0.19, 0.19, 0.05, 0, 0, ctypes.byref(h)) == -1
     assert L.bd_graph_rmat(10, 16, 0.57, 0.19, 0.19, 0.05, 0, 7, ctypes.byref(h)) == -1
     assert L.bd_bfs_create(None, None, ctypes.byref(h)) == -1
+
+
+def test_cpp_facade_reads_the_trained_policies(tmp_path):
+    """The C++ facade's JSON reader (used by the CLI's --algorithm learned)
+    gets the same numbers the Python trainer wrote."""
+    import json
+    import subprocess
+    src = tmp_path / "load.cc"
+    src.write_text(
+        '#include "beedrill/hybrid_bfs.hpp"\n'
+        'int main(int argc, char **argv) {\n'
+        '  beedrill::policy p = beedrill::load_policy(argv[1]);\n'
+        '  double s = 0; for (float v : p.params) s += v;\n'
+        '  printf("%zu %zu %zu %zu %.6g %.9g %.9g\\n", p.params.size(), p.mean.size(), p.lo.size(),\n'
+        '         p.hi.size(), p.margin, s, p.inv_std[3]);\n'
+        '  try { beedrill::load_policy(argv[2]); } catch (const beedrill::error &e) {\n'
+        '    printf("%d\\n", (int)e.status); }\n'
+        '  return 0; }\n')
+    exe = tmp_path / "load"
+    lib_dir = os.path.dirname(bd.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", lib_dir, "-lbeedrill_b200", f"-Wl,-rpath,{lib_dir}"], check=True)
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"params": [1, 2, 3], "mean": [0]}')
+    for name in ("learned_policy.json", "learned_policy_batched.json"):
+        path = os.path.join(ROOT, "beedrill_b200", "policy", name)
+        if not os.path.exists(path):
+            continue
+        out = subprocess.run([str(exe), path, str(bad)], check=True, stdout=subprocess.PIPE,
+                             text=True).stdout.split()
+        d = json.load(open(path))
+        assert out[:4] == ["1410", "8", "8", "8"]
+        assert abs(float(out[4]) - d["margin"]) <= 1e-6 * max(1.0, abs(d["margin"]))
+        assert abs(float(out[5]) - sum(d["params"])) <= 1e-3 * max(1.0, sum(abs(v) for v in d["params"]))
+        assert abs(float(out[6]) - d["inv_std"][3]) <= 1e-6 * abs(d["inv_std"][3])
+        assert out[7] == "-3"  # BD_ERR_FORMAT
