@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "bd_bfs_device.cuh"
+#include "bd_device_util.cuh"
 #include "bd_internal.h"
 
 namespace bd {
@@ -30,56 +31,7 @@ namespace {
 constexpr int64_t kRecCap = 1 << 15;
 constexpr long long kDefaultSpin = 4000000;  // ~2 s of polling
 
-// ---------------------------------------------------------------------------
-// small device helpers
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
-{
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_release(unsigned *p, unsigned v)
-{
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-__device__ __forceinline__ long long globaltimer()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return (long long)t;
-}
-
-__device__ __forceinline__ unsigned lanemask_lt()
-{
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
-__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
-
-template <typename T>
-__device__ __forceinline__ T warp_incl_scan(T x)
-{
-    const int lane = lane_id();
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        T y = __shfl_up_sync(kFull, x, d);
-        if (lane >= d) { x += y; }
-    }
-    return x;
-}
-
-template <typename T>
-__device__ __forceinline__ T warp_sum(T x)
-{
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) { x += __shfl_xor_sync(kFull, x, d); }
-    return x;
-}
+using namespace dev;
 
 // Per-thread accumulators of one step, reduced once per CTA at its end.
 struct Local {
@@ -87,7 +39,7 @@ struct Local {
     unsigned long long degsum;
 };
 
-// The view every CTA takes of the control block at the start of a step.
+// What a step needs of the traversal state, in registers.
 struct StepView {
     int dir;
     int level;
@@ -100,19 +52,18 @@ struct StepView {
     long long f_chunks;
 };
 
-__device__ __forceinline__ StepView read_view(const Ctrl *c)
+__device__ __forceinline__ StepView view_of(const LevelState &s)
 {
-    const volatile Ctrl *vc = c;
     StepView v;
-    v.dir = vc->dir;
-    v.bu_sparse = vc->bu_sparse;
-    v.level = vc->level;
-    v.vis_cur = vc->vis_cur;
-    v.q_cur = vc->q_cur;
-    v.step = vc->step;
-    v.f_small = vc->f_small;
-    v.f_large = vc->f_large;
-    v.f_chunks = vc->f_chunks;
+    v.dir = s.dir;
+    v.bu_sparse = s.bu_sparse;
+    v.level = s.level;
+    v.vis_cur = s.vis_cur;
+    v.q_cur = s.q_cur;
+    v.step = s.step;
+    v.f_small = s.f_small;
+    v.f_large = s.f_large;
+    v.f_chunks = s.f_chunks;
     return v;
 }
 
@@ -270,14 +221,12 @@ struct SharedState {
     WarpScratch warp[BLOCK / 32];
     unsigned long long red_found[BLOCK / 32];
     unsigned long long red_deg[BLOCK / 32];
-    int is_last;
-    unsigned gen;
-    int exit_flag;
+    LevelState st;       // this CTA's copy of the traversal state
+    PolicyBlob pol;      // the learned policy's weights, staged once
     float feat[kPolicyIn];
     float h1[kPolicyH];
-    float h2[kPolicyH];
-    float logit[kPolicyOut];
-    int beamer_dir;
+    float gap;
+    int rule_dir;
 };
 
 template <int BLOCK>
@@ -290,7 +239,7 @@ __device__ void td_step(const BfsParams &p, const StepView &sv, SharedState<BLOC
     const long long nw = (long long)gridDim.x * (BLOCK / 32);
     const int qin = sv.q_cur, qout = sv.q_cur ^ 1;
     uint32_t *vis = p.vis[sv.vis_cur];
-    Acc *acc = &p.ctrl->acc[sv.step & 1];
+    Acc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
 
     // Phase A: chunks of large-degree frontier vertices.  Warp gw takes a
@@ -390,7 +339,7 @@ __device__ void bu_step(const BfsParams &p, const StepView &sv, Local &loc)
     const uint32_t *vin = p.vis[sv.vis_cur];
     uint32_t *vout = p.vis[sv.vis_cur ^ 1];
     const int qout = sv.q_cur ^ 1;
-    Acc *acc = &p.ctrl->acc[sv.step & 1];
+    Acc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
 
     for (long long w0 = gw * K; w0 < p.words; w0 += nw * K) {
@@ -516,7 +465,7 @@ __device__ void bu_step_lanes(const BfsParams &p, const StepView &sv, Local &loc
     const uint32_t *vin = p.vis[sv.vis_cur];
     uint32_t *vout = p.vis[sv.vis_cur ^ 1];
     const int qout = sv.q_cur ^ 1;
-    Acc *acc = &p.ctrl->acc[sv.step & 1];
+    Acc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
 
     for (long long base = gw * 32; base < p.words; base += nw * 32) {
@@ -647,201 +596,151 @@ __device__ void bu_step_lanes(const BfsParams &p, const StepView &sv, Local &loc
 }
 
 // Beamer's rule (hybrid_bfs.cc:152-191) for the step about to run, given the
-// frontier in ctrl.  Updates the Beamer state like the reference loop does
-// when it commits to that direction.
-__device__ int beamer_choose(Ctrl *c, const BfsParams &p, bool commit)
+// frontier in the state.  Updates the Beamer state like the reference loop
+// does when it commits to that direction.
+__device__ int beamer_choose(LevelState &c, const BfsParams &p, bool commit)
 {
-    if (c->in_bu) { return kDirBU; }
-    if (c->scout > c->etc / p.alpha) {
+    if (c.in_bu) { return kDirBU; }
+    if (c.scout > c.etc / p.alpha) {
         if (commit) {
-            c->in_bu = 1;
-            c->awake = c->f_count;  // queue_.combined_size()
+            c.in_bu = 1;
+            c.awake = c.f_count;  // queue_.combined_size()
         }
         return kDirBU;
     }
-    if (commit) { c->etc -= c->scout; }
+    if (commit) { c.etc -= c.scout; }
     return kDirTD;
 }
 
 // After a step of direction `dir` found `found` vertices of degree sum
 // `degsum`: the reference's bookkeeping (scout after top-down, the awake
 // test of the bottom-up do-while, scout = 1 on leaving it).
-__device__ void beamer_after_step(Ctrl *c, const BfsParams &p, int dir, long long found,
+__device__ void beamer_after_step(LevelState &c, const BfsParams &p, int dir, long long found,
                                   long long degsum)
 {
     if (dir == kDirTD) {
-        c->scout = degsum;
-    } else if (c->in_bu) {
-        c->old_awake = c->awake;
-        c->awake = found;
-        if (!(c->awake >= c->old_awake || c->awake > p.n / p.beta)) {
-            c->in_bu = 0;
-            c->scout = 1;
+        c.scout = degsum;
+    } else if (c.in_bu) {
+        c.old_awake = c.awake;
+        c.awake = found;
+        if (!(c.awake >= c.old_awake || c.awake > p.n / p.beta)) {
+            c.in_bu = 0;
+            c.scout = 1;
         }
     }
 }
 
-// Picks the direction of the next step.  Called by one CTA (the last to
-// reach the barrier, or the init kernel) with the frontier already in ctrl.
-template <int BLOCK>
-__device__ void choose_next(Ctrl *c, const BfsParams &p, SharedState<BLOCK> *sh)
+// Whether the learned policy is consulted for the step after state c.
+__device__ __forceinline__ bool policy_applies(const LevelState &c, const BfsParams &p)
 {
-    const int tid = threadIdx.x;
-    // thread 0: the rule-based choice, and the learned-policy features
-    if (tid == 0) {
-        int d;
-        if (c->f_count == 0) {
-            d = kDirDone;
-        } else if (p.alg == BD_ALG_TOP_DOWN) {
-            d = kDirTD;
-        } else if (p.alg == BD_ALG_BOTTOM_UP) {
-            d = kDirBU;
-        } else if (p.alg == BD_ALG_LEARNED && p.policy) {
-            d = beamer_choose(c, p, false);
-        } else {
-            d = beamer_choose(c, p, true);
-        }
-        if (sh) {
-            sh->beamer_dir = d;
-            policy_features(sh->feat, c->f_count, c->f_degsum, 2 * p.m - c->visited_degsum,
-                            c->level, p.n, p.m, c->prev_dir, c->prev_ns);
-        } else {
-            c->dir = d;
-        }
-    }
-    if (!sh) { return; }
-    __syncthreads();
-    const bool learned = p.alg == BD_ALG_LEARNED && p.policy && sh->beamer_dir != kDirDone;
-    if (learned && tid < 32) {
-        const float gap = policy_gap_warp(p.policy, sh->feat, sh->h1);
-        if (tid == 0) { sh->logit[0] = gap; }
-    }
-    __syncthreads();
-    if (tid == 0) {
-        int d = sh->beamer_dir;
-        if (learned) {
-            // NaN gap: a feature outside the trusted range, the rule decides
-            const float gap = sh->logit[0];
-            int pick = d;
-            if (isfinite(gap) && fabsf(gap) >= p.policy->margin) {
-                pick = gap > 0.f ? kDirBU : kDirTD;
-            }
-            if (pick != d) { c->policy_overrides += 1; }
-            d = pick;
-            // keep the rule's state consistent with the step actually taken
-            if (d == kDirTD) {
-                c->in_bu = 0;
-                c->etc -= c->scout;
-            } else if (!c->in_bu) {
-                c->in_bu = 1;
-                c->awake = c->f_count;
-            }
-        }
-        c->dir = d;
-    }
-    __syncthreads();
+    return p.alg == BD_ALG_LEARNED && p.policy != nullptr && c.f_count != 0;
 }
 
-// Bookkeeping after a step; run by thread 0 of the deciding CTA.
-__device__ void finish_step(Ctrl *c, const BfsParams &p)
+// The rule's direction for the next step (committed into the Beamer state
+// unless the learned policy will decide), and the policy's raw features.
+// One thread.
+__device__ int rule_direction(LevelState &c, const BfsParams &p, float *feat)
 {
-    const int s = c->step;
-    volatile Acc *a = &c->acc[s & 1];
-    const long long found = (long long)a->found;
-    const long long degsum = (long long)a->degsum;
-    const long long nsmall = (long long)a->small_cnt;
-    const unsigned long long lp = a->large_packed;
-    const long long now = globaltimer();
-    const long long ns = now - c->t_last;
-    const int dir = c->dir;
-    if (s < p.rec_cap) {
-        bd_step r;
-        r.dir = dir;
-        r.level = c->level;
-        r.frontier = c->f_count;
-        r.frontier_edges = c->f_degsum;
-        r.unexplored_edges = 2 * p.m - c->visited_degsum;
-        r.found = found;
-        r.ns = ns;
-        p.rec[s] = r;
+    if (c.f_count == 0) { return kDirDone; }
+    if (p.alg == BD_ALG_TOP_DOWN) { return kDirTD; }
+    if (p.alg == BD_ALG_BOTTOM_UP) { return kDirBU; }
+    const bool learned = policy_applies(c, p);
+    const int d = beamer_choose(c, p, !learned);
+    if (learned) {
+        policy_features(feat, c.f_count, c.f_degsum, 2 * p.m - c.visited_degsum, c.level, p.n, p.m,
+                        c.prev_dir, c.prev_ns);
     }
-    c->visited_degsum += degsum;
-    c->reached += found;
+    return d;
+}
+
+// The learned policy's pick over the rule's (NaN gap: a feature outside the
+// trusted range, the rule decides); keeps the rule's state consistent with
+// the step actually taken.  One thread.
+__device__ int apply_policy(LevelState &c, const PolicyBlob *w, int rule, float gap)
+{
+    int d = rule;
+    if (isfinite(gap) && fabsf(gap) >= w->margin) { d = gap > 0.f ? kDirBU : kDirTD; }
+    if (d != rule) { c.policy_overrides += 1; }
+    if (d == kDirTD) {
+        c.in_bu = 0;
+        c.etc -= c.scout;
+    } else if (!c.in_bu) {
+        c.in_bu = 1;
+        c.awake = c.f_count;
+    }
+    return d;
+}
+
+// Picks c.dir for the next step: thread 0 applies the rule, warp 0 runs the
+// policy network from w (shared or global memory) where it applies.  Called
+// by every thread of the block.
+template <typename Shared>
+__device__ void decide_next(LevelState &c, const BfsParams &p, const PolicyBlob *w, Shared &sh)
+{
+    if (threadIdx.x == 0) { sh.rule_dir = rule_direction(c, p, sh.feat); }
+    __syncthreads();
+    if (!policy_applies(c, p)) {
+        if (threadIdx.x == 0) { c.dir = sh.rule_dir; }
+        return;
+    }
+    if (threadIdx.x < 32) {
+        const float gap = policy_gap_warp(w, sh.feat, sh.h1);
+        if (threadIdx.x == 0) { c.dir = apply_policy(c, w, sh.rule_dir, gap); }
+    }
+}
+
+// Advances the state over the step that just ended, from that step's
+// counters a and its end time.  One thread per CTA; every CTA computes the
+// same result.
+__device__ void advance(LevelState &c, const BfsParams &p, const Acc &a, long long t_end)
+{
+    const long long found = (long long)a.found;
+    const long long degsum = (long long)a.degsum;
+    const unsigned long long lp = a.large_packed;
+    const long long ns = t_end - c.t_last;
+    const int dir = c.dir;
+    c.visited_degsum += degsum;
+    c.reached += found;
     // once fewer than half of the live vertices are unvisited, bottom-up
     // work per bitmap word is sparse: switch to the lane-owned layout
-    c->bu_sparse = 2 * (p.n_live - c->reached) < p.n_live;
-    c->f_count = found;
-    c->f_degsum = degsum;
-    c->f_small = nsmall;
-    c->f_large = (long long)(lp >> kLargeShift);
-    c->f_chunks = (long long)(lp & kChunkMask);
-    c->prev_dir = dir;
-    c->prev_ns = ns;
-    if (dir == kDirTD) { c->td_steps += 1; } else { c->bu_steps += 1; }
-    c->level += 1;
-    c->q_cur ^= 1;
-    if (dir == kDirBU) { c->vis_cur ^= 1; }
+    c.bu_sparse = 2 * (p.n_live - c.reached) < p.n_live;
+    c.f_count = found;
+    c.f_degsum = degsum;
+    c.f_small = (long long)a.small_cnt;
+    c.f_large = (long long)(lp >> kLargeShift);
+    c.f_chunks = (long long)(lp & kChunkMask);
+    c.prev_dir = dir;
+    c.prev_ns = ns;
+    c.t_last = t_end;
+    if (dir == kDirTD) { c.td_steps += 1; } else { c.bu_steps += 1; }
+    c.level += 1;
+    c.q_cur ^= 1;
+    if (dir == kDirBU) { c.vis_cur ^= 1; }
     beamer_after_step(c, p, dir, found, degsum);
-    Acc *z = &c->acc[(s + 1) & 1];
-    z->found = 0;
-    z->degsum = 0;
-    z->small_cnt = 0;
-    z->large_packed = 0;
-    c->step = s + 1;
-    c->t_last = now;
+    c.step += 1;
 }
 
-// Grid barrier; the last CTA to arrive closes the step and picks the next
-// direction before releasing the others.  Every wait is bounded by
-// p.spin_limit polls; running out sets ctrl->error = BD_ERR_TIMEOUT.
+// The end of a step: block reduction of the counters, arrival at the grid
+// barrier (one release-add per CTA), acquire polling until every CTA has
+// arrived, then every CTA advances its copy of the state from the step's
+// counters and decides the next direction.  Every wait is bounded by
+// p.spin_limit polls; running out sets ctrl->error = BD_ERR_TIMEOUT and ends
+// this CTA's loop.
 template <int BLOCK>
-__device__ void barrier_decide(const BfsParams &p, SharedState<BLOCK> &sh)
+__device__ void end_step(const BfsParams &p, const StepView &sv, SharedState<BLOCK> &sh,
+                         Local &loc)
 {
     Ctrl *c = p.ctrl;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned gen = ld_acquire(&c->bar_gen);
-        __threadfence();
-        const unsigned prev = atomicAdd(&c->bar_count, 1u);
-        sh.is_last = (prev == p.expected_ctas - 1);
-        sh.gen = gen;
-    }
-    __syncthreads();
-    if (sh.is_last) {
-        __threadfence();
-        if (threadIdx.x == 0) { finish_step(c, p); }
-        __syncthreads();
-        choose_next<BLOCK>(c, p, &sh);
-        if (threadIdx.x == 0) {
-            atomicExch(&c->bar_count, 0u);
-            __threadfence();
-            st_release(&c->bar_gen, sh.gen + 1);
-        }
-    } else if (threadIdx.x == 0) {
-        long long it = 0;
-        while (ld_acquire(&c->bar_gen) == sh.gen) {
-            if (++it > p.spin_limit) {
-                atomicExch(&c->error, (int)BD_ERR_TIMEOUT);
-                break;
-            }
-            __nanosleep(64);
-        }
-    }
-    __syncthreads();
-}
-
-template <int BLOCK>
-__device__ void reduce_and_publish(const BfsParams &p, const StepView &sv, SharedState<BLOCK> &sh,
-                                   Local &loc)
-{
     const int lane = lane_id();
     const int warp = threadIdx.x >> 5;
-    unsigned long long f = warp_sum(loc.found);
-    unsigned long long d = warp_sum(loc.degsum);
+    const unsigned long long f = warp_sum(loc.found);
+    const unsigned long long d = warp_sum(loc.degsum);
     if (lane == 0) {
         sh.red_found[warp] = f;
         sh.red_deg[warp] = d;
     }
+    loc.found = 0;
+    loc.degsum = 0;
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long tf = 0, td = 0;
@@ -849,12 +748,55 @@ __device__ void reduce_and_publish(const BfsParams &p, const StepView &sv, Share
             tf += sh.red_found[i];
             td += sh.red_deg[i];
         }
-        Acc *acc = &p.ctrl->acc[sv.step & 1];
+        const int s = sv.step;
+        Acc *acc = &c->acc[s % 3];
         if (tf) { atomicAdd(&acc->found, tf); }
         if (td) { atomicAdd(&acc->degsum, td); }
+        if (blockIdx.x == 0) {
+            Acc *z = &c->acc[(s + 1) % 3];
+            z->found = z->degsum = z->small_cnt = z->large_packed = z->t_end = 0;
+        }
+        atomicMax(&acc->t_end, (unsigned long long)globaltimer());
+        red_release_add64(&c->bar, 1ull);
+        const unsigned long long target = (unsigned long long)(s + 1) * p.expected_ctas;
+        long long it = 0;
+        bool ok = true;
+        while (ld_acquire64(&c->bar) < target) {
+            if (++it > p.spin_limit) {
+                atomicExch(&c->error, (int)BD_ERR_TIMEOUT);
+                ok = false;
+                break;
+            }
+            __nanosleep(32);
+        }
+        if (ok && __ldcg(&c->error) == 0) {
+            Acc a;
+            a.found = __ldcg(&acc->found);
+            a.degsum = __ldcg(&acc->degsum);
+            a.small_cnt = __ldcg(&acc->small_cnt);
+            a.large_packed = __ldcg(&acc->large_packed);
+            const long long t_end = (long long)__ldcg(&acc->t_end);
+            LevelState &st = sh.st;
+            if (s == 0) { st.t_last = (long long)__ldcg(&c->t_start); }
+            if (blockIdx.x == 0 && s < p.rec_cap) {
+                bd_step r;
+                r.dir = st.dir;
+                r.level = st.level;
+                r.frontier = st.f_count;
+                r.frontier_edges = st.f_degsum;
+                r.unexplored_edges = 2 * p.m - st.visited_degsum;
+                r.found = (long long)a.found;
+                r.ns = t_end - st.t_last;
+                p.rec[s] = r;
+            }
+            advance(st, p, a, t_end);
+        } else {
+            sh.st.f_count = 0;  // leave the loop
+        }
     }
-    loc.found = 0;
-    loc.degsum = 0;
+    __syncthreads();
+    decide_next(sh.st, p, &sh.pol, sh);
+    __syncthreads();
 }
 
 // K bitmap words per warp step: 1, 2, 4 (warp-shared words) or 32 (one word
@@ -875,16 +817,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) bfs_persistent_kernel(BfsParams p
 {
     __shared__ SharedState<BLOCK> sh;
     Ctrl *c = p.ctrl;
-    if (blockIdx.x == 0 && threadIdx.x == 0) { c->t_last = globaltimer(); }
-    Local loc{0, 0};
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const volatile Ctrl *vc = c;
-            sh.exit_flag = (vc->error != 0) || (vc->dir == kDirDone);
+    if (threadIdx.x == 0) {
+        sh.st = c->st;  // written by the init kernel before this launch
+        atomicMin(&c->t_start, (unsigned long long)globaltimer());
+    }
+    if (p.policy) {
+        const float *src = reinterpret_cast<const float *>(p.policy);
+        float *dst = reinterpret_cast<float *>(&sh.pol);
+        for (int i = threadIdx.x; i < (int)(sizeof(PolicyBlob) / sizeof(float)); i += BLOCK) {
+            dst[i] = src[i];
         }
-        __syncthreads();
-        if (sh.exit_flag) { break; }
-        const StepView sv = read_view(c);
+    }
+    __syncthreads();
+    Local loc{0, 0};
+    while (sh.st.dir != kDirDone) {
+        const StepView sv = view_of(sh.st);
         if (sv.dir == kDirTD) {
             td_step<BLOCK>(p, sv, sh, loc);
         } else {
@@ -894,20 +841,32 @@ __global__ void __launch_bounds__(BLOCK, MINB) bfs_persistent_kernel(BfsParams p
                 bu_layout<BLOCK, KD>(p, sv, loc);
             }
         }
-        reduce_and_publish<BLOCK>(p, sv, sh, loc);
-        barrier_decide<BLOCK>(p, sh);
+        end_step<BLOCK>(p, sv, sh, loc);
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { c->st = sh.st; }
 }
 
+struct InitShared {
+    float feat[kPolicyIn];
+    float h1[kPolicyH];
+    float gap;
+    int rule_dir;
+    LevelState st;
+};
+
 // clear() + the source frontier (hybrid_bfs.cc:152-160 for one source; any
-// number of sources start as one frontier).  One CTA of 32 threads.
+// number of sources start as one frontier), and the first decision.  One
+// CTA of 32 threads.
 __global__ void init_sources_kernel(BfsParams p, const int64_t *sources, int64_t count,
                                     int64_t source_index)
 {
-    __shared__ SharedState<32> sh;
+    __shared__ InitShared sh;
     Ctrl *c = p.ctrl;
     if (threadIdx.x == 0) {
         memset(c, 0, sizeof(Ctrl));
+        c->t_start = ~0ull;
+        LevelState &st = sh.st;
+        memset(&st, 0, sizeof(LevelState));
         long long degsum = 0, nf = 0, nsmall = 0;
         unsigned long long lp = 0;
         const int64_t first = source_index >= 0 ? source_index : 0;
@@ -930,19 +889,21 @@ __global__ void init_sources_kernel(BfsParams p, const int64_t *sources, int64_t
                 p.qs[0][nsmall++] = s;
             }
         }
-        c->f_count = nf;
-        c->f_degsum = degsum;
-        c->f_small = nsmall;
-        c->f_large = (long long)(lp >> kLargeShift);
-        c->f_chunks = (long long)(lp & kChunkMask);
-        c->visited_degsum = degsum;
-        c->reached = nf;
-        c->etc = 2 * p.m;       // edges_to_check = num_edges * 2
-        c->scout = degsum;      // scout_count = out_degree(source)
-        c->prev_dir = kDirTD;
+        st.f_count = nf;
+        st.f_degsum = degsum;
+        st.f_small = nsmall;
+        st.f_large = (long long)(lp >> kLargeShift);
+        st.f_chunks = (long long)(lp & kChunkMask);
+        st.visited_degsum = degsum;
+        st.reached = nf;
+        st.etc = 2 * p.m;       // edges_to_check = num_edges * 2
+        st.scout = degsum;      // scout_count = out_degree(source)
+        st.prev_dir = kDirTD;
     }
     __syncthreads();
-    choose_next<32>(c, p, &sh);
+    decide_next(sh.st, p, p.policy, sh);
+    __syncthreads();
+    if (threadIdx.x == 0) { c->st = sh.st; }
 }
 
 // Deterministic tree: parent(v) = min{u in N(v) : depth[u] == depth[v]-1}.
@@ -1005,8 +966,8 @@ __global__ void finalize_parents_kernel(const int64_t *off, int64_t n, const int
 
 __global__ void save_result_kernel(const Ctrl *c, int64_t *out, int64_t i)
 {
-    out[2 * i] = c->visited_degsum / 2;
-    out[2 * i + 1] = c->reached;
+    out[2 * i] = c->st.visited_degsum / 2;
+    out[2 * i + 1] = c->st.reached;
 }
 
 int grid_for(int64_t items, int threads = 256)
@@ -1174,11 +1135,11 @@ bd_status collect(bd_bfs *b, bd_run_stats *stats, double ms)
     if (b->last.error) { return (bd_status)b->last.error; }
     if (stats) {
         stats->ms = ms;
-        stats->num_steps = b->last.step;
-        stats->reached = b->last.reached;
-        stats->traversed_edges = b->last.visited_degsum / 2;
-        stats->top_down_steps = b->last.td_steps;
-        stats->bottom_up_steps = b->last.bu_steps;
+        stats->num_steps = b->last.st.step;
+        stats->reached = b->last.st.reached;
+        stats->traversed_edges = b->last.st.visited_degsum / 2;
+        stats->top_down_steps = b->last.st.td_steps;
+        stats->bottom_up_steps = b->last.st.bu_steps;
     }
     return BD_OK;
 }
@@ -1462,7 +1423,7 @@ bd_status bd_bfs_count_traversed_edges(bd_bfs *b, int64_t *out)
 {
     if (!b || !out) { return BD_ERR_INVALID; }
     if (!b->ran) { return BD_ERR_STATE; }
-    *out = b->last.visited_degsum / 2;
+    *out = b->last.st.visited_degsum / 2;
     return BD_OK;
 }
 
@@ -1480,7 +1441,7 @@ bd_status bd_bfs_get_steps(bd_bfs *b, bd_step *steps, int64_t capacity, int64_t 
 {
     if (!b || !count || capacity < 0 || (!steps && capacity)) { return BD_ERR_INVALID; }
     if (!b->ran) { return BD_ERR_STATE; }
-    int64_t have = std::min<int64_t>(b->last.step, kRecCap);
+    int64_t have = std::min<int64_t>(b->last.st.step, kRecCap);
     int64_t take = std::min(have, capacity);
     if (take) {
         BD_CUDA(cudaSetDevice(b->device));
@@ -1651,6 +1612,6 @@ extern "C" bd_status bd_bfs_run_noalloc(const int64_t *d_offsets, const uint32_t
     BD_CUDA(cudaMemcpyAsync(&host, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
     BD_CUDA(cudaStreamSynchronize(s));
     if (host.error) { return (bd_status)host.error; }
-    if (traversed_edges) { *traversed_edges = host.visited_degsum / 2; }
+    if (traversed_edges) { *traversed_edges = host.st.visited_degsum / 2; }
     return BD_OK;
 }

@@ -8,16 +8,18 @@ namespace dev {
 
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p)
 {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
-__device__ __forceinline__ void st_release(unsigned *p, unsigned v)
+// Arrival at a grid barrier: orders every write the CTA made before it (the
+// CTA synchronised with __syncthreads first) ahead of the increment.
+__device__ __forceinline__ void red_release_add64(unsigned long long *p, unsigned long long v)
 {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ long long globaltimer()

@@ -46,6 +46,8 @@ constexpr int64_t kMsRecCap = 1 << 14;
 constexpr long long kMsDefaultSpin = 4000000;
 constexpr unsigned kRecSlots = 16;  // delivery records per vertex
 
+// Counters of one step, in a ring of three slots (step s uses s % 3; CTA 0
+// clears (s + 1) % 3 during step s, after every CTA has read it).
 struct MsAcc {
     ull vertices;    // vertices entering the next frontier
     ull degsum;      // their degree sum
@@ -53,19 +55,29 @@ struct MsAcc {
     ull small_cnt;
     ull large_packed;
     ull done_degsum; // degree sum of vertices that just got every lane
+    ull t_end;       // max over CTAs of their arrival time
+    ull pad;
 };
 
-struct MsCtrl {
-    unsigned bar_count, bar_gen;
-    int error, dir, level, step;
+// State between steps: written first by the init kernel, then kept by every
+// CTA as an identical copy in shared memory (advanced by the same function
+// of the same counters), written back by CTA 0 at the end.
+struct MsState {
+    int dir, level, step, prev_dir;
     long long f_count, f_degsum, f_small, f_large, f_chunks;
     long long p_small, p_large;  // lists of the frontier read by the previous step
     long long arcs_left;         // 2m - degree sum of vertices reached by all lanes
     long long lanes_total;
     long long t_last, push_steps, pull_steps;
-    int prev_dir, pad0;
     long long prev_ns, policy_overrides;
-    MsAcc acc[2];
+};
+
+struct MsCtrl {
+    ull bar;       // barrier arrivals; step s is complete at (s + 1) * CTAs
+    int error, pad0;
+    ull t_start;   // min over CTAs of their start time
+    MsState st;
+    MsAcc acc[3];
 };
 
 struct MsParams {
@@ -197,18 +209,17 @@ struct MsView {
     long long f_small, f_large, f_chunks, p_small, p_large;
 };
 
-__device__ __forceinline__ MsView ms_view(const MsCtrl *c)
+__device__ __forceinline__ MsView ms_view(const MsState &c)
 {
-    const volatile MsCtrl *vc = c;
     MsView v;
-    v.dir = vc->dir;
-    v.level = vc->level;
-    v.step = vc->step;
-    v.f_small = vc->f_small;
-    v.f_large = vc->f_large;
-    v.f_chunks = vc->f_chunks;
-    v.p_small = vc->p_small;
-    v.p_large = vc->p_large;
+    v.dir = c.dir;
+    v.level = c.level;
+    v.step = c.step;
+    v.f_small = c.f_small;
+    v.f_large = c.f_large;
+    v.f_chunks = c.f_chunks;
+    v.p_small = c.p_small;
+    v.p_large = c.p_large;
     return v;
 }
 
@@ -356,7 +367,7 @@ __device__ void ms_push_step(const MsParams &p, const MsView &sv, MsLocal &loc)
     const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
     const long long nw = (long long)gridDim.x * (BLOCK / 32);
     const int cur = sv.step % 3, nxt = (sv.step + 1) % 3;
-    MsAcc *acc = &p.ctrl->acc[sv.step & 1];
+    MsAcc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
     // large frontier vertices: chunk c of vertex ql[i]
     for (long long c = gw; c < sv.f_chunks; c += nw) {
@@ -395,7 +406,7 @@ __device__ void ms_pull_heavy(const MsParams &p, const MsView &sv, MsLocal &loc)
     const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
     const long long nw = (long long)gridDim.x * (BLOCK / 32);
     const int cur = sv.step % 3, nxt = (sv.step + 1) % 3;
-    MsAcc *acc = &p.ctrl->acc[sv.step & 1];
+    MsAcc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
     const long long total = p.n_heavy ? (long long)__ldg(&p.heavy_cbase[p.n_heavy]) : 0;
     for (long long c = gw; c < total; c += nw) {
@@ -457,7 +468,7 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
     const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
     const long long nw = (long long)gridDim.x * (BLOCK / 32);
     const int cur = sv.step % 3, nxt = (sv.step + 1) % 3;
-    MsAcc *acc = &p.ctrl->acc[sv.step & 1];
+    MsAcc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
     const long long words = (p.n + 31) / 32;
     for (long long w = gw; w < words; w += nw) {
@@ -567,149 +578,152 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
 template <int BLOCK>
 struct MsShared {
     ull red[4][BLOCK / 32];
-    int is_last;
-    unsigned gen;
-    int exit_flag;
+    MsState st;     // this CTA's copy of the state
+    PolicyBlob pol; // the learned policy's weights, staged once
     int rule_dir;
-    float gap;
     float feat[kPolicyIn];
     float h1[kPolicyH];
 };
 
 // The rule: pull once the frontier's edges are a sizeable share of the edges
 // still able to deliver a lane (Beamer's alpha test over the batch).
-__device__ int ms_rule(const MsCtrl *c, const MsParams &p)
+__device__ int ms_rule(const MsState &c, const MsParams &p)
 {
-    if (c->f_count == 0) { return kMsDone; }
+    if (c.f_count == 0) { return kMsDone; }
     if (p.force_dir >= 0) { return p.force_dir; }
-    return (c->f_degsum * p.alpha > c->arcs_left) ? kPull : kPush;
+    return (c.f_degsum * p.alpha > c.arcs_left) ? kPull : kPush;
 }
 
-__device__ void ms_finish_step(MsCtrl *c, const MsParams &p)
+// Advances the state over the step that just ended.  One thread per CTA;
+// every CTA computes the same result.
+__device__ void ms_advance(MsState &c, const MsAcc &a, long long t_end)
 {
-    const int s = c->step;
-    volatile MsAcc *a = &c->acc[s & 1];
-    const long long now = globaltimer();
-    const long long found = (long long)a->vertices;
-    if (s < p.rec_cap) {
-        bd_step r;
-        r.dir = c->dir;
-        r.level = c->level;
-        r.frontier = c->f_count;
-        r.frontier_edges = c->f_degsum;
-        r.unexplored_edges = c->arcs_left;
-        r.found = (long long)a->lanes;
-        r.ns = now - c->t_last;
-        p.rec[s] = r;
-    }
-    c->prev_dir = c->dir;
-    c->prev_ns = now - c->t_last;
-    c->lanes_total += (long long)a->lanes;
-    c->arcs_left -= (long long)a->done_degsum;
-    c->p_small = c->f_small;
-    c->p_large = c->f_large;
-    c->f_count = found;
-    c->f_degsum = (long long)a->degsum;
-    c->f_small = (long long)a->small_cnt;
-    c->f_large = (long long)(a->large_packed >> kLargeShift);
-    c->f_chunks = (long long)(a->large_packed & kChunkMask);
-    if (c->dir == kPush) { c->push_steps += 1; } else { c->pull_steps += 1; }
-    c->level += 1;
-    MsAcc *z = &c->acc[(s + 1) & 1];
-    z->vertices = z->degsum = z->lanes = z->small_cnt = z->large_packed = z->done_degsum = 0;
-    c->step = s + 1;
-    c->t_last = now;
+    c.prev_dir = c.dir;
+    c.prev_ns = t_end - c.t_last;
+    c.t_last = t_end;
+    c.lanes_total += (long long)a.lanes;
+    c.arcs_left -= (long long)a.done_degsum;
+    c.p_small = c.f_small;
+    c.p_large = c.f_large;
+    c.f_count = (long long)a.vertices;
+    c.f_degsum = (long long)a.degsum;
+    c.f_small = (long long)a.small_cnt;
+    c.f_large = (long long)(a.large_packed >> kLargeShift);
+    c.f_chunks = (long long)(a.large_packed & kChunkMask);
+    if (c.dir == kPush) { c.push_steps += 1; } else { c.pull_steps += 1; }
+    c.level += 1;
+    c.step += 1;
 }
 
-// Next direction by the CTA that closes a step: the rule, or the learned
-// policy (one warp) where it is installed, trusted and confident.
-template <int BLOCK>
-__device__ void ms_decide(MsCtrl *c, const MsParams &p, MsShared<BLOCK> &sh)
+// Next direction: the rule, or the learned policy (warp 0, weights from w)
+// where it is installed, trusted and confident.  Every thread of the block.
+template <typename Shared>
+__device__ void ms_decide(MsState &c, const MsParams &p, const PolicyBlob *w, Shared &sh)
 {
     const int tid = threadIdx.x;
     if (tid == 0) {
         sh.rule_dir = ms_rule(c, p);
-        policy_features(sh.feat, c->f_count, c->f_degsum, c->arcs_left, c->level, p.n, p.m,
-                        c->prev_dir, c->prev_ns);
+        policy_features(sh.feat, c.f_count, c.f_degsum, c.arcs_left, c.level, p.n, p.m,
+                        c.prev_dir, c.prev_ns);
     }
     __syncthreads();
     const bool learned = p.policy && p.force_dir < 0 && sh.rule_dir != kMsDone;
-    if (learned && tid < 32) {
-        const float gap = policy_gap_warp(p.policy, sh.feat, sh.h1);
-        if (tid == 0) { sh.gap = gap; }
+    if (!learned) {
+        if (tid == 0) { c.dir = sh.rule_dir; }
+        return;
     }
-    __syncthreads();
-    if (tid == 0) {
-        int d = sh.rule_dir;
-        if (learned && isfinite(sh.gap) && fabsf(sh.gap) >= p.policy->margin) {
-            const int pick = sh.gap > 0.f ? kPull : kPush;
-            if (pick != d) { c->policy_overrides += 1; }
-            d = pick;
+    if (tid < 32) {
+        const float gap = policy_gap_warp(w, sh.feat, sh.h1);
+        if (tid == 0) {
+            int d = sh.rule_dir;
+            if (isfinite(gap) && fabsf(gap) >= w->margin) {
+                const int pick = gap > 0.f ? kPull : kPush;
+                if (pick != d) { c.policy_overrides += 1; }
+                d = pick;
+            }
+            c.dir = d;
         }
-        c->dir = d;
     }
 }
 
+// The end of a step: block reduction of the counters, arrival at the grid
+// barrier (one release-add per CTA), acquire polling until all CTAs have
+// arrived, then every CTA advances its copy of the state and decides the
+// next direction.  Waits are bounded by p.spin_limit polls.
 template <int BLOCK>
-__device__ void ms_barrier(const MsParams &p, MsShared<BLOCK> &sh)
+__device__ void ms_end_step(const MsParams &p, const MsView &sv, MsShared<BLOCK> &sh, MsLocal &loc)
 {
     MsCtrl *c = p.ctrl;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned gen = ld_acquire(&c->bar_gen);
-        __threadfence();
-        const unsigned prev = atomicAdd(&c->bar_count, 1u);
-        sh.is_last = (prev == p.expected_ctas - 1);
-        sh.gen = gen;
-    }
-    __syncthreads();
-    if (sh.is_last) {
-        __threadfence();
-        if (threadIdx.x == 0) { ms_finish_step(c, p); }
-        __syncthreads();
-        ms_decide<BLOCK>(c, p, sh);
-        if (threadIdx.x == 0) {
-            atomicExch(&c->bar_count, 0u);
-            __threadfence();
-            st_release(&c->bar_gen, sh.gen + 1);
-        }
-    } else if (threadIdx.x == 0) {
-        long long it = 0;
-        while (ld_acquire(&c->bar_gen) == sh.gen) {
-            if (++it > p.spin_limit) {
-                atomicExch(&c->error, (int)BD_ERR_TIMEOUT);
-                break;
-            }
-            __nanosleep(64);
-        }
-    }
-    __syncthreads();
-}
-
-template <int BLOCK>
-__device__ void ms_publish(const MsParams &p, const MsView &sv, MsShared<BLOCK> &sh, MsLocal &loc)
-{
     const int lane = lane_id(), warp = threadIdx.x >> 5;
-    ull a = warp_sum(loc.vertices), b = warp_sum(loc.degsum), cc = warp_sum(loc.lanes),
-        d = warp_sum(loc.done_degsum);
+    const ull a0 = warp_sum(loc.vertices), a1 = warp_sum(loc.degsum), a2 = warp_sum(loc.lanes),
+              a3 = warp_sum(loc.done_degsum);
     if (lane == 0) {
-        sh.red[0][warp] = a;
-        sh.red[1][warp] = b;
-        sh.red[2][warp] = cc;
-        sh.red[3][warp] = d;
-    }
-    __syncthreads();
-    if (threadIdx.x < 4) {
-        ull t = 0;
-        for (int i = 0; i < BLOCK / 32; ++i) { t += sh.red[threadIdx.x][i]; }
-        MsAcc *acc = &p.ctrl->acc[sv.step & 1];
-        ull *dst = threadIdx.x == 0 ? &acc->vertices
-                   : threadIdx.x == 1 ? &acc->degsum
-                   : threadIdx.x == 2 ? &acc->lanes
-                                      : &acc->done_degsum;
-        if (t) { atomicAdd(dst, t); }
+        sh.red[0][warp] = a0;
+        sh.red[1][warp] = a1;
+        sh.red[2][warp] = a2;
+        sh.red[3][warp] = a3;
     }
     loc = MsLocal{0, 0, 0, 0};
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ull t[4] = {0, 0, 0, 0};
+        for (int i = 0; i < BLOCK / 32; ++i) {
+            for (int j = 0; j < 4; ++j) { t[j] += sh.red[j][i]; }
+        }
+        const int s = sv.step;
+        MsAcc *acc = &c->acc[s % 3];
+        if (t[0]) { atomicAdd(&acc->vertices, t[0]); }
+        if (t[1]) { atomicAdd(&acc->degsum, t[1]); }
+        if (t[2]) { atomicAdd(&acc->lanes, t[2]); }
+        if (t[3]) { atomicAdd(&acc->done_degsum, t[3]); }
+        if (blockIdx.x == 0) {
+            MsAcc *z = &c->acc[(s + 1) % 3];
+            z->vertices = z->degsum = z->lanes = z->small_cnt = z->large_packed = 0;
+            z->done_degsum = z->t_end = 0;
+        }
+        atomicMax(&acc->t_end, (ull)globaltimer());
+        red_release_add64(&c->bar, 1ull);
+        const ull target = (ull)(s + 1) * p.expected_ctas;
+        long long it = 0;
+        bool ok = true;
+        while (ld_acquire64(&c->bar) < target) {
+            if (++it > p.spin_limit) {
+                atomicExch(&c->error, (int)BD_ERR_TIMEOUT);
+                ok = false;
+                break;
+            }
+            __nanosleep(32);
+        }
+        MsState &st = sh.st;
+        if (ok && __ldcg(&c->error) == 0) {
+            MsAcc a;
+            a.vertices = __ldcg(&acc->vertices);
+            a.degsum = __ldcg(&acc->degsum);
+            a.lanes = __ldcg(&acc->lanes);
+            a.small_cnt = __ldcg(&acc->small_cnt);
+            a.large_packed = __ldcg(&acc->large_packed);
+            a.done_degsum = __ldcg(&acc->done_degsum);
+            const long long t_end = (long long)__ldcg(&acc->t_end);
+            if (s == 0) { st.t_last = (long long)__ldcg(&c->t_start); }
+            if (blockIdx.x == 0 && s < p.rec_cap) {
+                bd_step r;
+                r.dir = st.dir;
+                r.level = st.level;
+                r.frontier = st.f_count;
+                r.frontier_edges = st.f_degsum;
+                r.unexplored_edges = st.arcs_left;
+                r.found = (long long)a.lanes;
+                r.ns = t_end - st.t_last;
+                p.rec[s] = r;
+            }
+            ms_advance(st, a, t_end);
+        } else {
+            st.f_count = 0;  // leave the loop
+        }
+    }
+    __syncthreads();
+    ms_decide(sh.st, p, &sh.pol, sh);
+    __syncthreads();
 }
 
 template <int BLOCK, int MINB>
@@ -717,16 +731,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) msbfs_kernel(MsParams p)
 {
     __shared__ MsShared<BLOCK> sh;
     MsCtrl *c = p.ctrl;
-    if (blockIdx.x == 0 && threadIdx.x == 0) { c->t_last = globaltimer(); }
-    MsLocal loc{0, 0, 0, 0};
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const volatile MsCtrl *vc = c;
-            sh.exit_flag = (vc->error != 0) || (vc->dir == kMsDone);
+    if (threadIdx.x == 0) {
+        sh.st = c->st;  // written by the init kernel before this launch
+        atomicMin(&c->t_start, (ull)globaltimer());
+    }
+    if (p.policy) {
+        const float *src = reinterpret_cast<const float *>(p.policy);
+        float *dst = reinterpret_cast<float *>(&sh.pol);
+        for (int i = threadIdx.x; i < (int)(sizeof(PolicyBlob) / sizeof(float)); i += BLOCK) {
+            dst[i] = src[i];
         }
-        __syncthreads();
-        if (sh.exit_flag) { break; }
-        const MsView sv = ms_view(c);
+    }
+    __syncthreads();
+    MsLocal loc{0, 0, 0, 0};
+    while (sh.st.dir != kMsDone) {
+        const MsView sv = ms_view(sh.st);
         ms_clear_old(p, sv);
         if (sv.dir == kPush) {
             ms_push_step<BLOCK>(p, sv, loc);
@@ -734,9 +753,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) msbfs_kernel(MsParams p)
             ms_pull_heavy<BLOCK>(p, sv, loc);
             ms_pull_step<BLOCK>(p, sv, loc);
         }
-        ms_publish<BLOCK>(p, sv, sh, loc);
-        ms_barrier<BLOCK>(p, sh);
+        ms_end_step<BLOCK>(p, sv, sh, loc);
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { c->st = sh.st; }
 }
 
 // Sources: lane r starts at sources[r].  One thread (sources are few).
@@ -768,14 +787,16 @@ __global__ void ms_init_kernel(MsParams p, const int64_t *sources, int count)
             p.qs[0][nsmall++] = s;
         }
     }
-    c->f_count = nf;
-    c->f_degsum = degsum;
-    c->f_small = nsmall;
-    c->f_large = (long long)(lp >> kLargeShift);
-    c->f_chunks = (long long)(lp & kChunkMask);
-    c->arcs_left = 2 * p.m - done;
-    c->lanes_total = count;
-    c->dir = ms_rule(c, p);
+    c->t_start = ~0ull;
+    MsState &st = c->st;
+    st.f_count = nf;
+    st.f_degsum = degsum;
+    st.f_small = nsmall;
+    st.f_large = (long long)(lp >> kLargeShift);
+    st.f_chunks = (long long)(lp & kChunkMask);
+    st.arcs_left = 2 * p.m - done;
+    st.lanes_total = count;
+    st.dir = ms_rule(st, p);
 }
 
 // Per-lane reached count and degree sum (count_num_traversed_edges per root).
@@ -1232,7 +1253,7 @@ bd_status bd_msbfs_run(bd_msbfs *b, const int64_t *sources, int32_t count, bd_ru
         float ms = 0.f;
         BD_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
         stats->ms = ms;
-        stats->num_steps = b->last.step;
+        stats->num_steps = b->last.st.step;
         int64_t edges = 0, reached = 0;
         for (int i = 0; i < count; ++i) {
             const size_t base = (size_t)(i / 64) * 128;
@@ -1241,8 +1262,8 @@ bd_status bd_msbfs_run(bd_msbfs *b, const int64_t *sources, int32_t count, bd_ru
         }
         stats->traversed_edges = edges;
         stats->reached = reached;
-        stats->top_down_steps = b->last.push_steps;
-        stats->bottom_up_steps = b->last.pull_steps;
+        stats->top_down_steps = b->last.st.push_steps;
+        stats->bottom_up_steps = b->last.st.pull_steps;
     }
     return BD_OK;
 }
@@ -1283,7 +1304,7 @@ bd_status bd_msbfs_get_steps(bd_msbfs *b, bd_step *steps, int64_t capacity, int6
 {
     if (!b || !count || capacity < 0 || (!steps && capacity)) { return BD_ERR_INVALID; }
     if (!b->ran) { return BD_ERR_STATE; }
-    const int64_t have = std::min<int64_t>(b->last.step, kMsRecCap);
+    const int64_t have = std::min<int64_t>(b->last.st.step, kMsRecCap);
     const int64_t take = std::min(have, capacity);
     if (take) {
         BD_CUDA(cudaSetDevice(b->device));

@@ -2,8 +2,9 @@
 // forward pass, backward pass and Adam update are hand-written kernels.
 //
 // The network replaces the alpha/beta rule of run_beamer
-// (hybrid_bfs.cc:166-188) inside the persistent BFS kernel (choose_next in
-// bd_bfs.cu evaluates it on the device, one warp, once per level).  Training
+// (hybrid_bfs.cc:166-188) inside the persistent BFS kernel (decide_next in
+// bd_bfs.cu evaluates it on the device: one warp per CTA, once per level,
+// weights staged in shared memory).  Training
 // data are per-level timings of forced top-down and forced bottom-up runs:
 // both directions discover exactly the next BFS level, so the state after a
 // step does not depend on the direction taken and the two timings at the

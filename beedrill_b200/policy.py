@@ -334,10 +334,15 @@ def training_graph_specs(count=200, seed=2024):
     return specs
 
 
-def collect(specs, roots_per_graph=4, repeats=1, log=None):
+def collect(specs, roots_per_graph=4, repeats=1, log=None, order=None):
+    """Level tables of the training graphs, built with the adjacency order
+    the policy will run on (neighbour-degree order by default, as the
+    benchmark's graphs are; the order changes bottom-up costs)."""
+    order = bd.ORDER_DEGREE if order is None else order
     tables = []
     for i, s in enumerate(specs):
-        g = bd.Graph.rmat(s["scale"], s["edge_factor"], s["a"], s["b"], s["c"], s["d"], s["seed"])
+        g = bd.Graph.rmat(s["scale"], s["edge_factor"], s["a"], s["b"], s["c"], s["d"], s["seed"],
+                          order=order)
         roots = g.pick_roots(s["seed"], roots_per_graph)
         for t in measure_tables(g, roots, repeats=repeats):
             t.meta.update(s)
@@ -389,7 +394,7 @@ def train_batched(args, log):
                    "loss_last": float(hist[-1]), "margin": mgn,
                    "validation": {"rule": rb, "learned": rl},
                    "distribution": "RMAT scales 16-22, A~U[0.45,0.65], D=0.05, B=C=(1-A-D)/2, "
-                                   "ef 16, 64 roots per graph"}
+                                   "ef 16, 64 roots per graph, neighbour-degree adjacency order"}
     policy.save(args.out)
     log(f"saved {args.out}: rule regret {rb['regret_frac']:.3%}, learned {rl['regret_frac']:.3%}")
     return 0
@@ -431,7 +436,8 @@ def main(argv=None):
         "epochs": args.epochs, "lr": args.lr, "loss_first": float(hist[0]),
         "loss_last": float(hist[-1]), "margin": mgn,
         "validation": {"beamer": rb, "learned": rl},
-        "distribution": "RMAT scales 16-22, A~U[0.45,0.65], D=0.05, B=C=(1-A-D)/2, ef 16",
+        "distribution": "RMAT scales 16-22, A~U[0.45,0.65], D=0.05, B=C=(1-A-D)/2, ef 16, "
+                        "neighbour-degree adjacency order",
     }
     policy.save(args.out)
     log(f"saved {args.out}: beamer regret {rb['regret_frac']:.3%}, learned {rl['regret_frac']:.3%}")

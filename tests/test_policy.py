@@ -117,13 +117,38 @@ def test_trained_policy_vs_beamer_on_held_out_graphs():
     pol = P.Policy.load()
     tables = []
     for scale, a, b, d, seed in _held_out_specs(10, 1):
-        g = bd.Graph.rmat(scale, 16, a, b, b, d, seed)
+        g = bd.Graph.rmat(scale, 16, a, b, b, d, seed, order=bd.ORDER_DEGREE)
         tables += P.measure_tables(g, g.pick_roots(seed, 2), repeats=2, with_beamer=False)
         g.close()
     rb = P.regret(tables, P.beamer_dirs)
     rl = P.regret(tables, lambda t: P.policy_dirs(pol, t))
     print(f"held-out regret: Beamer {rb['regret_frac']:.2%}, learned {rl['regret_frac']:.2%}")
     assert rl["cost_ms"] <= rb["cost_ms"] * 1.005, (rl, rb)
+
+
+@pytest.mark.gpu
+def test_trained_policies_at_scale24_held_out():
+    """The evaluation case: RMAT scale 24 (A=.57 B=C=.19 D=.05) with a seed
+    no training graph used, beyond the training scales (16-22); the
+    single-source policy against Beamer's alpha=15/beta=18 switch over 16
+    roots, the batched policy against its rule over one 64-root batch."""
+    bd = pytest.importorskip("beedrill_b200")
+    from beedrill_b200 import policy as P
+    if not (os.path.exists(P.DEFAULT_PATH) and os.path.exists(P.BATCHED_PATH)):
+        pytest.skip("no trained policies committed")
+    g = bd.Graph.rmat(24, 16, seed=2424, order=bd.ORDER_DEGREE)
+    tables = P.measure_tables(g, g.pick_roots(7, 16), repeats=2, with_beamer=False)
+    pol = P.Policy.load()
+    rb = P.regret(tables, P.beamer_dirs)
+    rl = P.regret(tables, lambda t: P.policy_dirs(pol, t))
+    print(f"scale 24 regret: Beamer {rb['regret_frac']:.2%}, learned {rl['regret_frac']:.2%}")
+    assert rl["cost_ms"] <= rb["cost_ms"] * 1.005, (rl, rb)
+    tab = P.measure_tables_batched(g, g.pick_roots(8, 64), repeats=2)
+    bpol = P.Policy.load(P.BATCHED_PATH)
+    rule = P.regret([tab], P.alpha_dirs)
+    rl = P.regret([tab], lambda t: P.policy_dirs(bpol, t, rule=P.alpha_dirs(t)))
+    print(f"scale 24 batched regret: rule {rule['regret_frac']:.2%}, learned {rl['regret_frac']:.2%}")
+    assert rl["cost_ms"] <= rule["cost_ms"] * 1.005, (rl, rule)
 
 
 @pytest.mark.gpu
