@@ -13,7 +13,8 @@ NVFLAGS := -O3 -std=c++17 $(ARCH) -lineinfo -Xcompiler -fPIC -Xcompiler -Wall \
 CSRC := beedrill_b200/csrc
 CU_SRCS := $(CSRC)/bd_common.cu $(CSRC)/bd_graph.cu $(CSRC)/bd_bfs.cu $(CSRC)/bd_policy.cu $(CSRC)/bd_msbfs.cu
 CU_OBJS := $(patsubst $(CSRC)/%.cu,beedrill_b200/_build/%.o,$(CU_SRCS))
-HDRS := include/beedrill_b200.h $(CSRC)/bd_internal.h $(CSRC)/bd_bfs_device.cuh $(CSRC)/bd_device_util.cuh
+HDRS := include/beedrill_b200.h $(CSRC)/bd_internal.h $(CSRC)/bd_bfs_device.cuh $(CSRC)/bd_device_util.cuh \
+        $(CSRC)/bd_policy.cuh
 LIB := beedrill_b200/lib/libbeedrill_b200.so
 CLI := beedrill_b200/bin/hybrid_bfs
 

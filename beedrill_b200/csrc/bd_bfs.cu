@@ -223,9 +223,6 @@ struct SharedState {
     unsigned long long red_deg[BLOCK / 32];
     LevelState st;       // this CTA's copy of the traversal state
     PolicyBlob pol;      // the learned policy's weights, staged once
-    float feat[kPolicyIn];
-    float h1[kPolicyH];
-    float gap;
     int rule_dir;
 };
 
@@ -637,20 +634,13 @@ __device__ __forceinline__ bool policy_applies(const LevelState &c, const BfsPar
 }
 
 // The rule's direction for the next step (committed into the Beamer state
-// unless the learned policy will decide), and the policy's raw features.
-// One thread.
-__device__ int rule_direction(LevelState &c, const BfsParams &p, float *feat)
+// unless the learned policy will decide).  One thread.
+__device__ int rule_direction(LevelState &c, const BfsParams &p)
 {
     if (c.f_count == 0) { return kDirDone; }
     if (p.alg == BD_ALG_TOP_DOWN) { return kDirTD; }
     if (p.alg == BD_ALG_BOTTOM_UP) { return kDirBU; }
-    const bool learned = policy_applies(c, p);
-    const int d = beamer_choose(c, p, !learned);
-    if (learned) {
-        policy_features(feat, c.f_count, c.f_degsum, 2 * p.m - c.visited_degsum, c.level, p.n, p.m,
-                        c.prev_dir, c.prev_ns);
-    }
-    return d;
+    return beamer_choose(c, p, !policy_applies(c, p));
 }
 
 // The learned policy's pick over the rule's (NaN gap: a feature outside the
@@ -677,14 +667,15 @@ __device__ int apply_policy(LevelState &c, const PolicyBlob *w, int rule, float 
 template <typename Shared>
 __device__ void decide_next(LevelState &c, const BfsParams &p, const PolicyBlob *w, Shared &sh)
 {
-    if (threadIdx.x == 0) { sh.rule_dir = rule_direction(c, p, sh.feat); }
+    if (threadIdx.x == 0) { sh.rule_dir = rule_direction(c, p); }
     __syncthreads();
     if (!policy_applies(c, p)) {
         if (threadIdx.x == 0) { c.dir = sh.rule_dir; }
         return;
     }
     if (threadIdx.x < 32) {
-        const float gap = policy_gap_warp(w, sh.feat, sh.h1);
+        const float gap = policy_gap_warp(w, c.f_count, c.f_degsum, 2 * p.m - c.visited_degsum,
+                                          c.level, p.n, p.m, c.prev_dir, c.prev_ns);
         if (threadIdx.x == 0) { c.dir = apply_policy(c, w, sh.rule_dir, gap); }
     }
 }
@@ -847,9 +838,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) bfs_persistent_kernel(BfsParams p
 }
 
 struct InitShared {
-    float feat[kPolicyIn];
-    float h1[kPolicyH];
-    float gap;
     int rule_dir;
     LevelState st;
 };

@@ -581,8 +581,6 @@ struct MsShared {
     MsState st;     // this CTA's copy of the state
     PolicyBlob pol; // the learned policy's weights, staged once
     int rule_dir;
-    float feat[kPolicyIn];
-    float h1[kPolicyH];
 };
 
 // The rule: pull once the frontier's edges are a sizeable share of the edges
@@ -621,11 +619,7 @@ template <typename Shared>
 __device__ void ms_decide(MsState &c, const MsParams &p, const PolicyBlob *w, Shared &sh)
 {
     const int tid = threadIdx.x;
-    if (tid == 0) {
-        sh.rule_dir = ms_rule(c, p);
-        policy_features(sh.feat, c.f_count, c.f_degsum, c.arcs_left, c.level, p.n, p.m,
-                        c.prev_dir, c.prev_ns);
-    }
+    if (tid == 0) { sh.rule_dir = ms_rule(c, p); }
     __syncthreads();
     const bool learned = p.policy && p.force_dir < 0 && sh.rule_dir != kMsDone;
     if (!learned) {
@@ -633,7 +627,8 @@ __device__ void ms_decide(MsState &c, const MsParams &p, const PolicyBlob *w, Sh
         return;
     }
     if (tid < 32) {
-        const float gap = policy_gap_warp(w, sh.feat, sh.h1);
+        const float gap = policy_gap_warp(w, c.f_count, c.f_degsum, c.arcs_left, c.level, p.n,
+                                          p.m, c.prev_dir, c.prev_ns);
         if (tid == 0) {
             int d = sh.rule_dir;
             if (isfinite(gap) && fabsf(gap) >= w->margin) {

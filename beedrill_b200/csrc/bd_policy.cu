@@ -195,7 +195,23 @@ bd_status policy_blob(const float *params, const float *mean, const float *inv_s
 {
     if (!params || !mean || !inv_std || !(margin >= 0)) { return BD_ERR_INVALID; }
     memset(blob, 0, sizeof *blob);
-    memcpy(blob, params, sizeof(float) * kP);
+    // params: w1[32][8], b1[32], w2[32][32], b2[32], w3[2][32], b3[2]
+    const float *w1 = params;
+    const float *b1 = w1 + kPolicyH * kPolicyIn;
+    const float *w2 = b1 + kPolicyH;
+    const float *b2 = w2 + kPolicyH * kPolicyH;
+    const float *w3 = b2 + kPolicyH;
+    const float *b3 = w3 + kPolicyOut * kPolicyH;
+    for (int j = 0; j < kPolicyH; ++j) {
+        for (int i = 0; i < kPolicyIn; ++i) { blob->w1t[i][j] = w1[j * kPolicyIn + i]; }
+        for (int i = 0; i < kPolicyH; ++i) { blob->w2t[i][j] = w2[j * kPolicyH + i]; }
+        blob->b1[j] = b1[j];
+        blob->b2[j] = b2[j];
+        blob->w3[0][j] = w3[j];
+        blob->w3[1][j] = w3[kPolicyH + j];
+    }
+    blob->b3[0] = b3[0];
+    blob->b3[1] = b3[1];
     memcpy(blob->mean, mean, sizeof(float) * kPolicyIn);
     memcpy(blob->inv_std, inv_std, sizeof(float) * kPolicyIn);
     for (int i = 0; i < kPolicyIn; ++i) {

@@ -7,16 +7,19 @@
 
 namespace bd {
 
-// 8-32-32-2 MLP, fp32, row-major weights.
+// 8-32-32-2 MLP, fp32.  The parameter vector the trainer uses is row-major
+// (w1[32][8], b1, w2[32][32], b2, w3[2][32], b3); the traversal kernels keep
+// the first two weight matrices transposed, so that lane j of the evaluating
+// warp reads column j of consecutive rows (no shared-memory bank conflicts).
 constexpr int kPolicyIn = 8;
 constexpr int kPolicyH = 32;
 constexpr int kPolicyOut = 2;
 constexpr int kPolicyParams = kPolicyH * kPolicyIn + kPolicyH + kPolicyH * kPolicyH + kPolicyH +
                               kPolicyOut * kPolicyH + kPolicyOut;  // 1410
 struct PolicyBlob {
-    float w1[kPolicyH][kPolicyIn];
+    float w1t[kPolicyIn][kPolicyH];  // w1t[i][j] = w1[j][i]
     float b1[kPolicyH];
-    float w2[kPolicyH][kPolicyH];
+    float w2t[kPolicyH][kPolicyH];   // w2t[i][j] = w2[j][i]
     float b2[kPolicyH];
     float w3[kPolicyOut][kPolicyH];
     float b3[kPolicyOut];
@@ -28,54 +31,64 @@ struct PolicyBlob {
     float pad[3];
 };
 
-__device__ __forceinline__ float policy_log2p1(double x) { return (float)log2(1.0 + (x > 0 ? x : 0)); }
-
-// Raw features, in the order the trainer uses: log2(1 + frontier vertices),
+// Raw feature i, in the order the trainer uses: log2(1 + frontier vertices),
 // log2(1 + frontier degree sum), log2(1 + unexplored degree sum), level,
 // log2(1 + n), log2(1 + m), previous direction, log2(1 + previous step us).
-__device__ __forceinline__ void policy_features(float *f, long long frontier,
-                                                long long frontier_edges, long long unexplored,
-                                                int level, long long n, long long m,
-                                                int prev_dir, long long prev_ns)
+// The lanes of a warp each pick their argument, then take one logarithm
+// together (no divergent branches around the call).
+__device__ __forceinline__ float policy_feature(int i, long long frontier, long long frontier_edges,
+                                                long long unexplored, int level, long long n,
+                                                long long m, int prev_dir, long long prev_ns)
 {
-    f[0] = policy_log2p1((double)frontier);
-    f[1] = policy_log2p1((double)frontier_edges);
-    f[2] = policy_log2p1((double)unexplored);
-    f[3] = (float)level;
-    f[4] = policy_log2p1((double)n);
-    f[5] = policy_log2p1((double)m);
-    f[6] = (float)prev_dir;
-    f[7] = policy_log2p1((double)prev_ns * 1e-3);
+    const long long counts[6] = {frontier, frontier_edges, unexplored, n, m, prev_ns};
+    const int which = i < 3 ? i : (i == 4 ? 3 : (i == 5 ? 4 : 5));
+    long long v = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { v = which == k ? counts[k] : v; }
+    float arg = (float)(v > 0 ? v : 0);
+    if (i == 7) { arg *= 1e-3f; }  // ns -> us
+    const float lg = log2f(1.0f + arg);
+    return i == 3 ? (float)level : (i == 6 ? (float)prev_dir : lg);
 }
 
-// Forward pass by the 32 lanes of one warp (lane j owns hidden unit j).
-// feat and h1 live in shared memory.  Returns, in every lane, the logit gap
-// (bottom-up minus top-down), or NaN when a feature lies outside the
-// trusted range.
-__device__ __forceinline__ float policy_gap_warp(const PolicyBlob *w, const float *feat, float *h1)
+// Forward pass by the 32 lanes of one warp (lane j owns hidden unit j;
+// lanes 0-7 compute the features, activations move by shuffles).  Returns,
+// in every lane, the logit gap (bottom-up minus top-down), or NaN when a
+// feature lies outside the trusted range.  w may point to shared or global
+// memory.
+__device__ __forceinline__ float policy_gap_warp(const PolicyBlob *w, long long frontier,
+                                                 long long frontier_edges, long long unexplored,
+                                                 int level, long long n, long long m,
+                                                 int prev_dir, long long prev_ns)
 {
+    const unsigned full = 0xFFFFFFFFu;
     const int j = threadIdx.x & 31;
-    bool trusted = true;
-#pragma unroll
-    for (int i = 0; i < kPolicyIn; ++i) {
-        trusted = trusted && feat[i] >= w->lo[i] && feat[i] <= w->hi[i];
+    float x = 0.f;
+    bool ok = true;
+    if (j < kPolicyIn) {
+        const float f = policy_feature(j, frontier, frontier_edges, unexplored, level, n, m,
+                                       prev_dir, prev_ns);
+        ok = f >= w->lo[j] && f <= w->hi[j];
+        x = (f - w->mean[j]) * w->inv_std[j];
     }
+    const bool trusted = __all_sync(full, ok);
     float a1 = w->b1[j];
 #pragma unroll
-    for (int i = 0; i < kPolicyIn; ++i) { a1 += w->w1[j][i] * ((feat[i] - w->mean[i]) * w->inv_std[i]); }
-    h1[j] = fmaxf(a1, 0.f);
-    __syncwarp();
-    float a2 = w->b2[j];
-#pragma unroll 8
-    for (int i = 0; i < kPolicyH; ++i) { a2 += w->w2[j][i] * h1[i]; }
-    const float h2 = fmaxf(a2, 0.f);
+    for (int i = 0; i < kPolicyIn; ++i) { a1 += w->w1t[i][j] * __shfl_sync(full, x, i); }
+    const float h1 = fmaxf(a1, 0.f);
+    float a2 = w->b2[j], a2b = 0.f;  // two chains: half the dependent adds
+#pragma unroll
+    for (int i = 0; i < kPolicyH; i += 2) {
+        a2 += w->w2t[i][j] * __shfl_sync(full, h1, i);
+        a2b += w->w2t[i + 1][j] * __shfl_sync(full, h1, i + 1);
+    }
+    const float h2 = fmaxf(a2 + a2b, 0.f);
     float o0 = w->w3[0][j] * h2, o1 = w->w3[1][j] * h2;
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
-        o0 += __shfl_xor_sync(0xFFFFFFFFu, o0, d);
-        o1 += __shfl_xor_sync(0xFFFFFFFFu, o1, d);
+        o0 += __shfl_xor_sync(full, o0, d);
+        o1 += __shfl_xor_sync(full, o1, d);
     }
-    __syncwarp();
     const float gap = (o1 + w->b3[1]) - (o0 + w->b3[0]);
     return trusted ? gap : nanf("");
 }

@@ -43,18 +43,27 @@ BATCHED_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "policy"
 
 
 def raw_features(frontier, frontier_edges, unexplored, level, n, m, prev_dir, prev_ns):
-    """The features choose_next computes on the device (bd_bfs.cu), in the
-    same order and the same units."""
-    f = np.empty(NUM_FEATURES, np.float64)
-    f[0] = np.log2(1.0 + max(frontier, 0))
-    f[1] = np.log2(1.0 + max(frontier_edges, 0))
-    f[2] = np.log2(1.0 + max(unexplored, 0))
+    """The features the traversal kernels compute on the device
+    (policy_feature in bd_policy.cuh), in the same order, units and float32
+    arithmetic."""
+    one = np.float32(1.0)
+
+    def lg(x, scale=None):
+        v = np.float32(max(int(x), 0))
+        if scale is not None:
+            v = np.float32(v * np.float32(scale))
+        return np.log2(one + v, dtype=np.float32)
+
+    f = np.empty(NUM_FEATURES, np.float32)
+    f[0] = lg(frontier)
+    f[1] = lg(frontier_edges)
+    f[2] = lg(unexplored)
     f[3] = level
-    f[4] = np.log2(1.0 + n)
-    f[5] = np.log2(1.0 + m)
+    f[4] = lg(n)
+    f[5] = lg(m)
     f[6] = prev_dir
-    f[7] = np.log2(1.0 + max(prev_ns, 0) * 1e-3)
-    return f.astype(np.float32)
+    f[7] = lg(prev_ns, 1e-3)
+    return f
 
 
 @dataclass

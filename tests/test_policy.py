@@ -167,3 +167,50 @@ def test_trained_batched_policy_vs_rule_on_held_out_graphs():
     rl = P.regret(tables, lambda t: P.policy_dirs(pol, t, rule=P.alpha_dirs(t)))
     print(f"held-out regret: rule {rule['regret_frac']:.2%}, learned {rl['regret_frac']:.2%}")
     assert rl["cost_ms"] <= rule["cost_ms"] * 1.005, (rl, rule)
+
+
+def _decisions_agree(pol, steps, m2):
+    """Rebuilds the features each step's decision saw from the run's own
+    step records and checks every confident, trusted decision against the
+    host float32 forward pass."""
+    from beedrill_b200 import policy as P
+    checked = 0
+    for s, st in enumerate(steps):
+        prev_dir = steps[s - 1]["dir"] if s else 0
+        prev_ns = steps[s - 1]["ns"] if s else 0
+        raw = P.raw_features(st["frontier"], st["frontier_edges"], st["unexplored_edges"],
+                             st["level"], m2[0], m2[1], prev_dir, prev_ns)
+        gap = float(np.diff(pol.logits(raw)[0])[0])
+        if not pol.trusts(raw) or abs(abs(gap) - pol.margin) < 1e-3 or abs(gap) < pol.margin:
+            continue
+        assert st["dir"] == (1 if gap > 0 else 0), (s, gap, st)
+        checked += 1
+    return checked
+
+
+@pytest.mark.gpu
+def test_in_kernel_decisions_follow_the_network():
+    """The traversal kernels' own evaluation of the network (transposed
+    weights in shared memory, shuffles) decides as the host forward pass
+    does, single-source and batched."""
+    bd = pytest.importorskip("beedrill_b200")
+    from beedrill_b200 import policy as P
+    rng = np.random.default_rng(11)
+    pol = P.Policy(PO.init_params(21).astype(np.float32), np.array(
+        [10, 20, 25, 3, 18, 22, 0.5, 5], np.float32), np.full(8, 0.25, np.float32), 0.05)
+    checked = 0
+    for scale in (14, 16, 17):
+        g = bd.Graph.rmat(scale, 16, seed=int(rng.integers(1 << 30)), order=bd.ORDER_DEGREE)
+        n, m = g.num_vertices(), g.num_edges()
+        bfs = bd.HybridBFS(g, alg="learned")
+        pol.install(bfs)
+        for root in g.pick_roots(3, 4):
+            bfs.clear()
+            bfs.run(int(root))
+            checked += _decisions_agree(pol, bfs.steps(), (n, m))
+        ms = bd.BatchedBFS(g, 64)
+        pol.install(ms)
+        ms.run(g.pick_roots(4, 64))
+        checked += _decisions_agree(pol, ms.steps(), (n, m))
+        g.close()
+    assert checked > 20
