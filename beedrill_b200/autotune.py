@@ -12,10 +12,11 @@ Picks, by measurement on the GPU it runs on:
 
 Search is coordinate descent over those axes (each axis swept with the
 others held), repeated until nothing improves, scored by the harmonic mean
-of per-root GTEPS over a fixed root set.  Results go to a JSON file that
+of per-root GTEPS over a fixed root set of an RMAT graph whose seed differs
+from the benchmark graph's.  Results go to a JSON file that
 beedrill_b200.tuned_options() reads:
 
-    python -m beedrill_b200.autotune --scale 22 --out beedrill_b200/tuning/b200.json
+    python -m beedrill_b200.autotune --scale 24 --seed 1024 --out beedrill_b200/tuning/b200.json
 """
 from __future__ import annotations
 
@@ -42,8 +43,8 @@ SINGLE_SPACE = {
 BATCHED_SPACE = {
     "block_size": [256, 512, 1024],
     "alpha": [1, 2, 4, 8, 16],
-    "large_degree": [32, 128, 1024],
-    "chunk_edges": [256, 1024],
+    "large_degree": [16, 32, 64, 128, 1024],
+    "chunk_edges": [128, 256, 512, 1024],
     "pull_prefix": [8, 16, 32, 64],
     "heavy_degree": [1024, 4096, 16384],
     "heavy_chunk": [512, 2048, 8192],
@@ -108,14 +109,14 @@ def coordinate_descent(space, start, score, log=None, rounds=3):
     return cur, cur_score, table
 
 
-def tune(scale=22, roots=32, seed=22, order=bd.ORDER_DEGREE, log=None):
+def tune(scale=24, roots=64, seed=1024, order=bd.ORDER_DEGREE, log=None):
     g = bd.Graph.rmat(scale, 16, seed=seed, order=order)
     rs = g.pick_roots(0, roots)
     start_single = {"block_size": 1024, "bu_words": 4, "bu_sparse_words": 32, "large_degree": 256,
                     "chunk_edges": 128, "bu_prefix": 8}
     single, s_score, s_table = coordinate_descent(
         SINGLE_SPACE, start_single, lambda p: score_single(g, rs, p), log)
-    start_batched = {"block_size": 512, "alpha": 4, "large_degree": 1024, "chunk_edges": 1024,
+    start_batched = {"block_size": 512, "alpha": 4, "large_degree": 32, "chunk_edges": 256,
                      "pull_prefix": 16, "heavy_degree": 4096, "heavy_chunk": 2048}
     batched, b_score, b_table = coordinate_descent(
         BATCHED_SPACE, start_batched, lambda p: score_batched(g, rs[:64], p), log)
@@ -132,13 +133,15 @@ def tune(scale=22, roots=32, seed=22, order=bd.ORDER_DEGREE, log=None):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description="tune the BFS kernels on this GPU")
-    ap.add_argument("--scale", type=int, default=22)
-    ap.add_argument("--roots", type=int, default=32)
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--roots", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=1024,
+                    help="graph seed (the benchmark's graph uses another)")
     ap.add_argument("--out", default=DEFAULT_PATH)
     ap.add_argument("--order", type=int, default=bd.ORDER_DEGREE)
     args = ap.parse_args(argv)
     log = lambda s: print(f"[autotune] {s}", flush=True)  # noqa: E731
-    res = tune(args.scale, args.roots, order=args.order, log=log)
+    res = tune(args.scale, args.roots, seed=args.seed, order=args.order, log=log)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     with open(args.out, "w") as f:
         json.dump(res, f, indent=1)

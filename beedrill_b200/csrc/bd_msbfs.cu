@@ -22,6 +22,9 @@
 //   F[3]    uint64[n]      frontier words, three buffers: step s reads
 //                          F[s%3], writes F[(s+1)%3], clears F[(s+2)%3]
 //   Q[3]                   the vertex lists of those frontiers (degree bins)
+//   done    uint32[n/32]   vertices every lane has reached, and isolated ones:
+//                          pull steps skip them by the word, push steps
+//                          drop arcs into them before touching seen
 //   depth   int32[n][R]    vertex-major, so a vertex's lanes share sectors
 //   parent  uint32[n][R]   vertex-major; widened to the reference's int64
 //                          encoding when copied out
@@ -83,7 +86,7 @@ struct MsCtrl {
 struct MsParams {
     const int64_t *off;
     const uint32_t *adj;
-    const uint32_t *isolated;
+    uint32_t *done;   // bit v: every lane reached v, or v is isolated (no lane can)
     int64_t n, m;
     ull *seen;
     ull *F[3];
@@ -312,55 +315,86 @@ __device__ __forceinline__ void ms_append_k(const MsParams &p, MsAcc *acc, int q
 // rows and the pull steps' records never hold the same pair).
 constexpr int kPushU = 4;
 
+// One round of up to kPushU arcs per lane: arc i of this lane goes from
+// src[i] (whose frontier lanes are bits[i]) to v[i].
+__device__ __forceinline__ void push_arcs(const MsParams &p, MsAcc *acc, int cur, int nxt,
+                                          int new_level, const bool (&in)[kPushU],
+                                          const uint32_t (&v)[kPushU],
+                                          const uint32_t (&src)[kPushU],
+                                          const ull (&bits)[kPushU], MsLocal &loc)
+{
+    uint32_t dn[kPushU];
+#pragma unroll
+    for (int i = 0; i < kPushU; ++i) { dn[i] = in[i] ? __ldcg(&p.done[v[i] >> 5]) : ~0u; }
+    ull vis[kPushU];
+#pragma unroll
+    for (int i = 0; i < kPushU; ++i) {
+        const bool open = in[i] && !((dn[i] >> (v[i] & 31)) & 1u);
+        vis[i] = open ? (__ldcg(&p.seen[v[i]]) | frontier_word(p, cur, v[i])) : ~0ull;
+    }
+    ull old[kPushU], give[kPushU];
+#pragma unroll
+    for (int i = 0; i < kPushU; ++i) {
+        give[i] = bits[i] & ~vis[i];
+        old[i] = give[i] ? atomicOr(&p.F[nxt][v[i]], give[i]) : ~0ull;
+    }
+    bool first[kPushU];
+    int64_t deg[kPushU];
+#pragma unroll
+    for (int i = 0; i < kPushU; ++i) {
+        const ull fresh = give[i] & ~old[i];
+        first[i] = give[i] != 0 && old[i] == 0ull;
+        deg[i] = 0;
+        if (fresh) {
+            write_rows(p, v[i], fresh, new_level, src[i]);
+            loc.lanes += __popcll(fresh);
+        }
+        if (first[i] || (fresh && ((vis[i] | old[i] | fresh) & p.all) == p.all)) {
+            deg[i] = ms_degree(p, v[i]);
+        }
+        if (fresh && ((vis[i] | old[i] | fresh) & p.all) == p.all) {
+            loc.done_degsum += (ull)deg[i];
+            atomicOr(&p.done[v[i] >> 5], 1u << (v[i] & 31));
+        }
+        if (first[i]) { atomicOr(&p.fb[nxt][v[i] >> 5], 1u << (v[i] & 31)); }
+        if (!first[i]) { deg[i] = 0; }
+    }
+    ms_append_k<kPushU>(p, acc, nxt, first, v, deg, loc);
+}
+
+// Arcs [b, e) of frontier vertex u (lanes `bits`), all 32 lanes, coalesced.
 __device__ __forceinline__ void push_edges(const MsParams &p, MsAcc *acc, int cur, int nxt,
                                            int new_level, uint32_t u, ull bits, int64_t b,
                                            int64_t e, MsLocal &loc)
 {
     const int lane = lane_id();
     for (int64_t base = b; base < e; base += 32 * kPushU) {
-        uint32_t v[kPushU];
+        uint32_t v[kPushU], src[kPushU];
+        ull bt[kPushU];
         bool in[kPushU];
 #pragma unroll
         for (int i = 0; i < kPushU; ++i) {
             const int64_t k = base + 32 * i + lane;
             in[i] = k < e;
             v[i] = in[i] ? __ldg(&p.adj[k]) : 0u;
+            src[i] = u;
+            bt[i] = bits;
         }
-        ull vis[kPushU];
-#pragma unroll
-        for (int i = 0; i < kPushU; ++i) {
-            vis[i] = in[i] ? (__ldcg(&p.seen[v[i]]) | frontier_word(p, cur, v[i])) : ~0ull;
-        }
-        ull old[kPushU], give[kPushU];
-#pragma unroll
-        for (int i = 0; i < kPushU; ++i) {
-            give[i] = bits & ~vis[i];
-            old[i] = give[i] ? atomicOr(&p.F[nxt][v[i]], give[i]) : ~0ull;
-        }
-        bool first[kPushU];
-        int64_t deg[kPushU];
-#pragma unroll
-        for (int i = 0; i < kPushU; ++i) {
-            const ull fresh = give[i] & ~old[i];
-            first[i] = give[i] != 0 && old[i] == 0ull;
-            deg[i] = 0;
-            if (fresh) {
-                write_rows(p, v[i], fresh, new_level, u);
-                loc.lanes += __popcll(fresh);
-            }
-            if (first[i] || (fresh && ((vis[i] | old[i] | fresh) & p.all) == p.all)) {
-                deg[i] = ms_degree(p, v[i]);
-            }
-            if (fresh && ((vis[i] | old[i] | fresh) & p.all) == p.all) { loc.done_degsum += (ull)deg[i]; }
-            if (first[i]) { atomicOr(&p.fb[nxt][v[i] >> 5], 1u << (v[i] & 31)); }
-            if (!first[i]) { deg[i] = 0; }
-        }
-        ms_append_k<kPushU>(p, acc, nxt, first, v, deg, loc);
+        push_arcs(p, acc, cur, nxt, new_level, in, v, src, bt, loc);
     }
 }
 
+// Per-warp scratch of the small-vertex push: 32 frontier vertices, their
+// lanes, list starts and the inclusive prefix of their degrees.
+struct MsWarpScratch {
+    int32_t incl[32];
+    uint32_t u[32];
+    int64_t beg[32];
+    ull bits[32];
+};
+
 template <int BLOCK>
-__device__ void ms_push_step(const MsParams &p, const MsView &sv, MsLocal &loc)
+__device__ void ms_push_step(const MsParams &p, const MsView &sv, MsWarpScratch &ws, MsLocal &loc)
 {
     const int lane = lane_id();
     const int warp = threadIdx.x >> 5;
@@ -384,12 +418,54 @@ __device__ void ms_push_step(const MsParams &p, const MsView &sv, MsLocal &loc)
         const int64_t b = ub + j * (int64_t)p.chunk;
         push_edges(p, acc, cur, nxt, new_level, u, bits, b, min(ue, b + (int64_t)p.chunk), loc);
     }
-    // small frontier vertices: one warp walks one vertex at a time
-    for (long long i = gw; i < sv.f_small; i += nw) {
-        const uint32_t u = __ldcg(&p.qs[cur][i]);
-        const ull bits = __ldcg(&p.F[cur][u]);
-        if (lane == 0) { p.seen[u] |= bits; }
-        push_edges(p, acc, cur, nxt, new_level, u, bits, __ldg(&p.off[u]), __ldg(&p.off[u + 1]), loc);
+    // small frontier vertices, 32 per warp: their lists are laid end to end
+    // and dealt to the lanes kPushU x 32 arcs at a time
+    for (long long g = gw; g * 32 < sv.f_small; g += nw) {
+        const long long idx = g * 32 + lane;
+        uint32_t u = 0;
+        ull bits = 0;
+        int64_t beg = 0;
+        int32_t deg = 0;
+        if (idx < sv.f_small) {
+            u = __ldcg(&p.qs[cur][idx]);
+            bits = __ldcg(&p.F[cur][u]);
+            beg = __ldg(&p.off[u]);
+            deg = (int32_t)(__ldg(&p.off[u + 1]) - beg);
+            p.seen[u] |= bits;
+        }
+        const int32_t incl = warp_incl_scan(deg);
+        const int32_t total = __shfl_sync(kFullMask, incl, 31);
+        ws.incl[lane] = incl;
+        ws.u[lane] = u;
+        ws.beg[lane] = beg;
+        ws.bits[lane] = bits;
+        __syncwarp();
+        for (int32_t base = 0; base < total; base += 32 * kPushU) {
+            uint32_t v[kPushU], src[kPushU];
+            ull bt[kPushU];
+            bool in[kPushU];
+#pragma unroll
+            for (int i = 0; i < kPushU; ++i) {
+                const int32_t e = base + i * 32 + lane;
+                in[i] = e < total;
+                v[i] = 0;
+                src[i] = 0;
+                bt[i] = 0;
+                if (in[i]) {
+                    int lo = 0, hi = 31;  // first owner with incl > e
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (ws.incl[mid] > e) { hi = mid; } else { lo = mid + 1; }
+                    }
+                    const int32_t excl = lo ? ws.incl[lo - 1] : 0;
+                    src[i] = ws.u[lo];
+                    bt[i] = ws.bits[lo];
+                    v[i] = __ldg(&p.adj[ws.beg[lo] + (e - excl)]);
+                }
+            }
+            push_arcs(p, acc, cur, nxt, new_level, in, v, src, bt, loc);
+        }
+        __syncwarp();
     }
 }
 
@@ -450,7 +526,10 @@ __device__ void ms_pull_heavy(const MsParams &p, const MsView &sv, MsLocal &loc)
                 const bool first = lane == 0 && old == 0ull;
                 if (lane == 0 && fresh) {
                     loc.lanes += __popcll(fresh);
-                    if (((vis | old | fresh) & p.all) == p.all) { loc.done_degsum += (ull)(ve - vb); }
+                    if (((vis | old | fresh) & p.all) == p.all) {
+                        loc.done_degsum += (ull)(ve - vb);
+                        atomicOr(&p.done[v >> 5], 1u << (v & 31));
+                    }
                 }
                 if (first) { atomicOr(&p.fb[nxt][v >> 5], 1u << (v & 31)); }
                 ms_append(p, acc, nxt, first, v, ve - vb, loc);
@@ -471,112 +550,132 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
     MsAcc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
     const long long words = (p.n + 31) / 32;
-    for (long long w = gw; w < words; w += nw) {
-        const uint32_t iso = __ldg(&p.isolated[w]);
-        if (iso == kFullMask) { continue; }
-        const uint32_t v = (uint32_t)(w * 32 + lane);
-        const bool live = !((iso >> lane) & 1u);
-        ull need = 0, got = 0;
-        int64_t beg = 0, end = 0, next = 0;
-        unsigned cnt = 0, cnt0 = 0;  // this vertex's delivery records
-        if (live) {
-            const ull f = __ldcg(&p.F[cur][v]);
-            ull s = __ldcg(&p.seen[v]);
-            if (f) {
-                s |= f;
-                p.seen[v] = s;
-            }
-            need = p.all & ~s;
-            if (need) {
-                beg = __ldg(&p.off[v]);
-                end = __ldg(&p.off[v + 1]);
-                if (end - beg > p.heavy_deg) {
-                    // scanned in chunks by ms_pull_heavy
-                    need = 0;
-                    beg = end = 0;
+    // Warp gw owns words gw, gw + nw, gw + 2 nw, ...; it loads 32 of their
+    // skip masks at once (one per lane) and walks only the words with work.
+    // Done vertices outside the frontier have nothing to do (frontier ones
+    // still fold their frontier lanes into seen below).
+    for (long long t0 = 0; gw + t0 * nw < words; t0 += 32) {
+        const long long wl = gw + (t0 + lane) * nw;
+        const uint32_t sk =
+            wl < words ? (__ldcg(&p.done[wl]) & ~__ldcg(&p.fb[cur][wl])) : kFullMask;
+        unsigned todo = __ballot_sync(kFullMask, sk != kFullMask);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const long long w = gw + (t0 + src) * nw;
+            const uint32_t skip = __shfl_sync(kFullMask, sk, src);
+            const uint32_t v = (uint32_t)(w * 32 + lane);
+            const bool live = !((skip >> lane) & 1u);
+            ull need = 0, got = 0;
+            int64_t beg = 0, end = 0, next = 0;
+            unsigned cnt = 0, cnt0 = 0;  // this vertex's delivery records
+            if (live) {
+                const ull f = __ldcg(&p.F[cur][v]);
+                ull s = __ldcg(&p.seen[v]);
+                if (f) {
+                    s |= f;
+                    p.seen[v] = s;
                 }
-            }
-            if (need) {
-                cnt = cnt0 = __ldcg(&p.drec_cnt[v]);
-                const int64_t lim = min(end, beg + (int64_t)p.prefix);
-                int64_t k = beg;
-                // four arcs in flight per round
-                for (; k < lim && got != need; k += 4) {
-                    uint32_t u[4];
-                    ull fu[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) { u[i] = (k + i < lim) ? __ldg(&p.adj[k + i]) : 0u; }
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) { fu[i] = (k + i < lim) ? frontier_word(p, cur, u[i]) : 0ull; }
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const ull f = fu[i] & need & ~got;
-                        if (f) {
-                            got |= f;
-                            put_record(p, v, cnt++, f, new_level, u[i]);
-                        }
+                need = p.all & ~s;
+                if (need) {
+                    beg = __ldg(&p.off[v]);
+                    end = __ldg(&p.off[v + 1]);
+                    if (end - beg > p.heavy_deg) {
+                        // scanned in chunks by ms_pull_heavy
+                        need = 0;
+                        beg = end = 0;
                     }
                 }
-                next = (got == need) ? end : min(k, lim);
-            }
-        }
-        unsigned pending = __ballot_sync(kFullMask, need != 0 && got != need && next < end);
-        while (pending) {
-            const int owner = __ffs(pending) - 1;
-            pending &= pending - 1;
-            const int64_t b = __shfl_sync(kFullMask, next, owner);
-            const int64_t e = __shfl_sync(kFullMask, end, owner);
-            const ull nd = __shfl_sync(kFullMask, need, owner);
-            ull have = __shfl_sync(kFullMask, got, owner);
-            const uint32_t vo = __shfl_sync(kFullMask, v, owner);
-            unsigned c = __shfl_sync(kFullMask, cnt, owner);
-            // 128 arcs per round: four independent gathers per lane
-            for (int64_t base = b; base < e && have != nd; base += 128) {
-                uint32_t u[4];
-                ull fu[4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int64_t k = base + 32 * i + lane;
-                    u[i] = k < e ? __ldg(&p.adj[k]) : 0u;
-                }
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int64_t k = base + 32 * i + lane;
-                    fu[i] = k < e ? frontier_word(p, cur, u[i]) & nd : 0ull;
-                }
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const ull f = fu[i] & ~have;
-                    if (!__any_sync(kFullMask, f != 0)) { continue; }
-                    // arcs earlier in the list win: each lane keeps the bits
-                    // no lower lane of this batch already delivered
-                    const ull mine = f & ~warp_excl_or(f);
-                    const unsigned bm = __ballot_sync(kFullMask, mine != 0);
-                    if (mine) { put_record(p, vo, c + __popc(bm & lanemask_lt()), mine, new_level, u[i]); }
-                    c += __popc(bm);
-                    have |= warp_or(f);
+                if (need) {
+                    cnt = cnt0 = __ldcg(&p.drec_cnt[v]);
+                    const int64_t lim = min(end, beg + (int64_t)p.prefix);
+                    int64_t k = beg;
+                    // four arcs in flight per round
+                    for (; k < lim && got != need; k += 4) {
+                        uint32_t u[4];
+                        ull fu[4];
+    #pragma unroll
+                        for (int i = 0; i < 4; ++i) { u[i] = (k + i < lim) ? __ldg(&p.adj[k + i]) : 0u; }
+    #pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            fu[i] = (k + i < lim) ? frontier_word(p, cur, u[i]) : 0ull;
+                        }
+    #pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const ull f = fu[i] & need & ~got;
+                            if (f) {
+                                got |= f;
+                                put_record(p, v, cnt++, f, new_level, u[i]);
+                            }
+                        }
+                    }
+                    next = (got == need) ? end : min(k, lim);
                 }
             }
-            if (lane == owner) {
-                got = have;
-                cnt = c;
+            unsigned pending = __ballot_sync(kFullMask, need != 0 && got != need && next < end);
+            while (pending) {
+                const int owner = __ffs(pending) - 1;
+                pending &= pending - 1;
+                const int64_t b = __shfl_sync(kFullMask, next, owner);
+                const int64_t e = __shfl_sync(kFullMask, end, owner);
+                const ull nd = __shfl_sync(kFullMask, need, owner);
+                ull have = __shfl_sync(kFullMask, got, owner);
+                const uint32_t vo = __shfl_sync(kFullMask, v, owner);
+                unsigned c = __shfl_sync(kFullMask, cnt, owner);
+                // 128 arcs per round: four independent gathers per lane
+                for (int64_t base = b; base < e && have != nd; base += 128) {
+                    uint32_t u[4];
+                    ull fu[4];
+    #pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const int64_t k = base + 32 * i + lane;
+                        u[i] = k < e ? __ldg(&p.adj[k]) : 0u;
+                    }
+    #pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const int64_t k = base + 32 * i + lane;
+                        fu[i] = k < e ? frontier_word(p, cur, u[i]) & nd : 0ull;
+                    }
+    #pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const ull f = fu[i] & ~have;
+                        if (!__any_sync(kFullMask, f != 0)) { continue; }
+                        // arcs earlier in the list win: each lane keeps the bits
+                        // no lower lane of this batch already delivered
+                        const ull mine = f & ~warp_excl_or(f);
+                        const unsigned bm = __ballot_sync(kFullMask, mine != 0);
+                        if (mine) {
+                            put_record(p, vo, c + __popc(bm & lanemask_lt()), mine, new_level, u[i]);
+                        }
+                        c += __popc(bm);
+                        have |= warp_or(f);
+                    }
+                }
+                if (lane == owner) {
+                    got = have;
+                    cnt = c;
+                }
             }
+            if (cnt != cnt0) { p.drec_cnt[v] = cnt; }
+            const bool gained = got != 0;
+            const unsigned gm = __ballot_sync(kFullMask, gained);
+            if (lane == 0 && gm) { atomicOr(&p.fb[nxt][w], gm); }
+            const bool completed = gained && ((p.all & ~need) | got) == p.all;
+            const unsigned cm = __ballot_sync(kFullMask, completed);
+            if (lane == 0 && cm) { atomicOr(&p.done[w], cm); }
+            if (gained) {
+                p.F[nxt][v] = got;
+                loc.lanes += __popcll(got);
+                if (completed) { loc.done_degsum += (ull)(end - beg); }
+            }
+            ms_append(p, acc, nxt, gained, v, end - beg, loc);
         }
-        if (cnt != cnt0) { p.drec_cnt[v] = cnt; }
-        const bool gained = got != 0;
-        const unsigned gm = __ballot_sync(kFullMask, gained);
-        if (lane == 0 && gm) { atomicOr(&p.fb[nxt][w], gm); }
-        if (gained) {
-            p.F[nxt][v] = got;
-            loc.lanes += __popcll(got);
-            if (((p.all & ~need) | got) == p.all) { loc.done_degsum += (ull)(end - beg); }
-        }
-        ms_append(p, acc, nxt, gained, v, end - beg, loc);
     }
 }
 
 template <int BLOCK>
 struct MsShared {
+    MsWarpScratch warp[BLOCK / 32];
     ull red[4][BLOCK / 32];
     MsState st;     // this CTA's copy of the state
     PolicyBlob pol; // the learned policy's weights, staged once
@@ -743,7 +842,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) msbfs_kernel(MsParams p)
         const MsView sv = ms_view(sh.st);
         ms_clear_old(p, sv);
         if (sv.dir == kPush) {
-            ms_push_step<BLOCK>(p, sv, loc);
+            ms_push_step<BLOCK>(p, sv, sh.warp[threadIdx.x >> 5], loc);
         } else {
             ms_pull_heavy<BLOCK>(p, sv, loc);
             ms_pull_step<BLOCK>(p, sv, loc);
@@ -769,7 +868,10 @@ __global__ void ms_init_kernel(MsParams p, const int64_t *sources, int count)
         p.seen[s] |= bit;
         put_record(p, s, p.drec_cnt[s]++, bit, 0, s);
         const int64_t deg = p.off[s + 1] - p.off[s];
-        if (p.seen[s] == p.all) { done += deg; }
+        if (p.seen[s] == p.all) {
+            done += deg;
+            p.done[s >> 5] |= 1u << (s & 31);
+        }
         if (before) { continue; }
         nf += 1;
         degsum += deg;
@@ -909,6 +1011,7 @@ struct bd_msbfs {
     uint32_t *parent = nullptr;  // [groups][n][R]
     uint4 *drec = nullptr;       // [groups][n][kRecSlots]
     uint32_t *drec_cnt = nullptr;  // [groups][n]
+    uint32_t *done = nullptr;      // [n/32], rewritten for each group
     MsCtrl *ctrl = nullptr;
     bd_step *rec = nullptr;
     int64_t *d_sources = nullptr;         // [max_roots]
@@ -947,7 +1050,7 @@ MsParams ms_params(bd_msbfs *b, int group, int count)
     MsParams p{};
     p.off = b->g->d_off;
     p.adj = b->g->d_adj;
-    p.isolated = b->g->d_isolated;
+    p.done = b->done;
     p.n = b->g->n;
     p.m = b->g->m;
     p.seen = b->seen + group * b->g->n;
@@ -991,6 +1094,8 @@ bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
     const int64_t n = b->g->n;
     BD_CUDA(cudaMemsetAsync(b->seen + group * n, 0, sizeof(ull) * n, b->stream));
     BD_CUDA(cudaMemsetAsync(b->drec_cnt + group * n, 0, sizeof(uint32_t) * n, b->stream));
+    BD_CUDA(cudaMemcpyAsync(b->done, b->g->d_isolated, sizeof(uint32_t) * ((n + 31) / 32),
+                            cudaMemcpyDeviceToDevice, b->stream));
     for (int i = 0; i < 3; ++i) {
         BD_CUDA(cudaMemsetAsync(b->F[i], 0, sizeof(ull) * n, b->stream));
         BD_CUDA(cudaMemsetAsync(b->fb[i], 0, sizeof(uint32_t) * ((n + 31) / 32), b->stream));
@@ -1058,6 +1163,7 @@ void ms_free(bd_msbfs *b)
     if (b->stream) { cudaStreamSynchronize(b->stream); }
     if (b->graph) { cudaGraphExecDestroy(b->graph); }
     cudaFree(b->seen);
+    cudaFree(b->done);
     for (int i = 0; i < 3; ++i) {
         cudaFree(b->F[i]);
         cudaFree(b->fb[i]);
@@ -1139,9 +1245,9 @@ bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *o
     if (o.alpha <= 0 || o.force_dir < -1 || o.force_dir > 1) { return BD_ERR_INVALID; }
     if (o.block_size == 0) { o.block_size = 512; }
     if (o.block_size != 256 && o.block_size != 512 && o.block_size != 1024) { return BD_ERR_INVALID; }
-    if (o.large_degree <= 0) { o.large_degree = 1024; }
+    if (o.large_degree <= 0) { o.large_degree = 32; }
     if (o.large_degree > (1 << 20)) { return BD_ERR_INVALID; }
-    if (o.chunk_edges <= 0) { o.chunk_edges = 1024; }
+    if (o.chunk_edges <= 0) { o.chunk_edges = 256; }
     if (o.pull_prefix <= 0) { o.pull_prefix = 16; }
     if (o.heavy_degree <= 0) { o.heavy_degree = 4096; }
     if (o.heavy_chunk <= 0) { o.heavy_chunk = 2048; }
@@ -1165,6 +1271,7 @@ bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *o
     }
     const size_t slots = (size_t)n * b->R * b->groups;
     bool ok = cudaMalloc(&b->seen, sizeof(ull) * n * b->groups) == cudaSuccess &&
+              cudaMalloc(&b->done, sizeof(uint32_t) * ((n + 31) / 32)) == cudaSuccess &&
               cudaMalloc(&b->depth, sizeof(int32_t) * slots) == cudaSuccess &&
               cudaMalloc(&b->parent, sizeof(uint32_t) * slots) == cudaSuccess &&
               cudaMalloc(&b->drec, sizeof(uint4) * (size_t)n * kRecSlots * b->groups) == cudaSuccess &&
