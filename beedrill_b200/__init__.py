@@ -38,7 +38,7 @@ STATUS_NAMES = {
     -5: "BD_ERR_CUDA", -6: "BD_ERR_TIMEOUT", -7: "BD_ERR_RANGE", -8: "BD_ERR_STATE",
     -9: "BD_ERR_NODEV", -10: "BD_ERR_LIMIT",
 }
-ORDER_INSERTION, ORDER_SORTED, ORDER_DEGREE = 0, 1, 2
+ORDER_INSERTION, ORDER_SORTED, ORDER_DEGREE, ORDER_HUB = 0, 1, 2, 3
 ALG_BEAMER, ALG_TOP_DOWN, ALG_BOTTOM_UP, ALG_LEARNED = 0, 1, 2, 3
 
 # The reference's --algorithm values (hybrid_bfs_main.cc:228-245) plus the

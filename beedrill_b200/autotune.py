@@ -109,7 +109,7 @@ def coordinate_descent(space, start, score, log=None, rounds=3):
     return cur, cur_score, table
 
 
-def tune(scale=24, roots=64, seed=1024, order=bd.ORDER_DEGREE, log=None):
+def tune(scale=24, roots=64, seed=1024, order=bd.ORDER_HUB, log=None):
     g = bd.Graph.rmat(scale, 16, seed=seed, order=order)
     rs = g.pick_roots(0, roots)
     start_single = {"block_size": 1024, "bu_words": 4, "bu_sparse_words": 32, "large_degree": 256,
@@ -138,7 +138,7 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=1024,
                     help="graph seed (the benchmark's graph uses another)")
     ap.add_argument("--out", default=DEFAULT_PATH)
-    ap.add_argument("--order", type=int, default=bd.ORDER_DEGREE)
+    ap.add_argument("--order", type=int, default=bd.ORDER_HUB)
     args = ap.parse_args(argv)
     log = lambda s: print(f"[autotune] {s}", flush=True)  # noqa: E731
     res = tune(args.scale, args.roots, seed=args.seed, order=args.order, log=log)

@@ -860,7 +860,7 @@ __global__ void init_sources_kernel(BfsParams p, const int64_t *sources, int64_t
         const int64_t first = source_index >= 0 ? source_index : 0;
         const int64_t last = source_index >= 0 ? source_index + 1 : count;
         for (int64_t i = first; i < last; ++i) {
-            const uint32_t s = (uint32_t)sources[i];
+            const uint32_t s = p.perm ? p.perm[sources[i]] : (uint32_t)sources[i];
             if (p.depth[s] == 0) { continue; }  // repeated source
             p.depth[s] = 0;
             p.parent[s] = (int64_t)s;
@@ -952,6 +952,27 @@ __global__ void finalize_parents_kernel(const int64_t *off, int64_t n, const int
     }
 }
 
+// BD_ORDER_HUB: depths and parents in the caller's numbering (traversal
+// arrays are indexed, and parents named, by traversal id), with the
+// reference's encoding of unreached vertices.
+__global__ void hub_outputs_kernel(const uint32_t *perm, const uint32_t *iperm, const int64_t *off,
+                                   int64_t n, const int32_t *depth, const int64_t *parent,
+                                   int32_t *out_depth, int64_t *out_parent)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t t = perm[v];
+        const int32_t d = depth[t];
+        out_depth[v] = d;
+        if (d >= 0) {
+            out_parent[v] = (int64_t)iperm[parent[t]];
+        } else {
+            const int64_t deg = off[v + 1] - off[v];
+            out_parent[v] = deg != 0 ? -deg : -1;
+        }
+    }
+}
+
 __global__ void save_result_kernel(const Ctrl *c, int64_t *out, int64_t i)
 {
     out[2 * i] = c->st.visited_degsum / 2;
@@ -1013,9 +1034,13 @@ struct bd_bfs {
     int block = 512;
     int grid = 0;
     int64_t cap_large = 0;
+    // BD_ORDER_HUB graphs: depths and parents in the caller's numbering,
+    // filled from the traversal arrays when first read after a run
+    int32_t *out_depth = nullptr;
+    int64_t *out_parent = nullptr;
     bool cleared = false;
     bool ran = false;
-    bool parents_final = false;
+    bool parents_final = false;  // caller-visible depths and parents are up to date
     int64_t last_source = -1;
     Ctrl last{};
 };
@@ -1040,8 +1065,8 @@ namespace {
 BfsParams make_params(bd_bfs *b)
 {
     BfsParams p{};
-    p.off = b->g->d_off;
-    p.adj = b->g->d_adj;
+    p.off = traversal_off(b->g);
+    p.adj = traversal_adj(b->g);
     p.n = b->g->n;
     p.m = b->g->m;
     p.depth = b->depth;
@@ -1067,6 +1092,7 @@ BfsParams make_params(bd_bfs *b)
     p.spin_limit = b->opts.spin_limit;
     p.expected_ctas = (unsigned)(b->grid + b->opts.test_extra_ctas);
     p.policy = b->policy;
+    p.perm = b->g->d_perm;
     return p;
 }
 
@@ -1074,8 +1100,9 @@ bd_status enqueue_clear(bd_bfs *b)
 {
     const int64_t n = b->g->n;
     BD_CUDA(cudaMemsetAsync(b->depth, 0xFF, sizeof(int32_t) * n, b->stream));
-    BD_CUDA(cudaMemcpyAsync(b->vis[0], b->g->d_isolated, sizeof(uint32_t) * bitmap_words(n),
-                            cudaMemcpyDeviceToDevice, b->stream));
+    BD_CUDA(cudaMemcpyAsync(b->vis[0], traversal_isolated(b->g),
+                            sizeof(uint32_t) * bitmap_words(n), cudaMemcpyDeviceToDevice,
+                            b->stream));
     return BD_OK;
 }
 
@@ -1105,8 +1132,21 @@ bd_status enqueue_bfs(bd_bfs *b, int64_t count, int64_t index, cudaEvent_t start
     BD_CUDA(cudaLaunchCooperativeKernel((const void *)b->kernel, dim3(b->grid), dim3(b->block),
                                         args, 0, b->stream));
     if (b->opts.min_parent) {
-        min_parent_kernel<<<grid_for(bitmap_words(b->g->n) * 32), 256, 0, b->stream>>>(
-            b->g->d_off, b->g->d_adj, b->g->n, b->depth, b->parent);
+        // the smallest parent in the caller's numbering: on a hub graph, map
+        // the outputs back first, then pick parents on the caller's CSR
+        const int64_t n = b->g->n;
+        int32_t *depth = b->depth;
+        int64_t *parent = b->parent;
+        if (b->out_depth) {
+            hub_outputs_kernel<<<grid_for(n), 256, 0, b->stream>>>(
+                b->g->d_perm, b->g->d_iperm, b->g->d_off, n, b->depth, b->parent, b->out_depth,
+                b->out_parent);
+            BD_CUDA(cudaGetLastError());
+            depth = b->out_depth;
+            parent = b->out_parent;
+        }
+        min_parent_kernel<<<grid_for(bitmap_words(n) * 32), 256, 0, b->stream>>>(
+            b->g->d_off, b->g->d_adj, n, depth, parent);
         BD_CUDA(cudaGetLastError());
     }
     if (stop) { BD_CUDA(cudaEventRecord(stop, b->stream)); }
@@ -1119,7 +1159,8 @@ bd_status collect(bd_bfs *b, bd_run_stats *stats, double ms)
     BD_CUDA(cudaStreamSynchronize(b->stream));
     b->ran = true;
     b->cleared = false;
-    b->parents_final = false;
+    // a min-parent run on a hub graph wrote the caller-order outputs itself
+    b->parents_final = b->out_depth != nullptr && b->opts.min_parent;
     if (b->last.error) { return (bd_status)b->last.error; }
     if (stats) {
         stats->ms = ms;
@@ -1151,12 +1192,22 @@ bd_status run_sources(bd_bfs *b, const int64_t *sources, int64_t count, bd_run_s
     return collect(b, stats, (double)ms);
 }
 
+// Makes the caller-visible depths and parents current: the reference's
+// -deg / -1 encoding of unreached vertices, and on a hub graph the mapping
+// back to the caller's numbering.
 bd_status finalize_parents(bd_bfs *b)
 {
     if (!b->ran) { return BD_ERR_STATE; }
     if (b->parents_final) { return BD_OK; }
-    finalize_parents_kernel<<<grid_for(b->g->n), 256, 0, b->stream>>>(b->g->d_off, b->g->n,
-                                                                      b->depth, b->parent);
+    const int64_t n = b->g->n;
+    if (b->out_depth) {
+        hub_outputs_kernel<<<grid_for(n), 256, 0, b->stream>>>(
+            b->g->d_perm, b->g->d_iperm, b->g->d_off, n, b->depth, b->parent, b->out_depth,
+            b->out_parent);
+    } else {
+        finalize_parents_kernel<<<grid_for(n), 256, 0, b->stream>>>(b->g->d_off, n, b->depth,
+                                                                  b->parent);
+    }
     BD_CUDA(cudaGetLastError());
     BD_CUDA(cudaStreamSynchronize(b->stream));
     b->parents_final = true;
@@ -1170,6 +1221,8 @@ void bfs_free(bd_bfs *b)
     if (b->stream) { cudaStreamSynchronize(b->stream); }
     cudaFree(b->depth);
     cudaFree(b->parent);
+    cudaFree(b->out_depth);
+    cudaFree(b->out_parent);
     for (int i = 0; i < 2; ++i) {
         cudaFree(b->vis[i]);
         cudaFree(b->qs[i]);
@@ -1234,6 +1287,8 @@ bd_status bd_bfs_create(bd_graph *g, const bd_bfs_opts *opts, bd_bfs **out)
     }
     bool ok = cudaMalloc(&b->depth, sizeof(int32_t) * n) == cudaSuccess &&
               cudaMalloc(&b->parent, sizeof(int64_t) * n) == cudaSuccess &&
+              (!g->d_perm || (cudaMalloc(&b->out_depth, sizeof(int32_t) * n) == cudaSuccess &&
+                              cudaMalloc(&b->out_parent, sizeof(int64_t) * n) == cudaSuccess)) &&
               cudaMalloc(&b->ctrl, sizeof(Ctrl)) == cudaSuccess &&
               cudaMalloc(&b->rec, sizeof(bd_step) * kRecCap) == cudaSuccess;
     for (int i = 0; i < 2 && ok; ++i) {
@@ -1384,7 +1439,9 @@ bd_status bd_bfs_get_depths(bd_bfs *b, int32_t *depth)
     if (!b || !depth) { return BD_ERR_INVALID; }
     if (!b->ran) { return BD_ERR_STATE; }
     BD_CUDA(cudaSetDevice(b->device));
-    BD_CUDA(cudaMemcpy(depth, b->depth, sizeof(int32_t) * b->g->n, cudaMemcpyDeviceToHost));
+    BD_TRY(finalize_parents(b));
+    BD_CUDA(cudaMemcpy(depth, b->out_depth ? b->out_depth : b->depth, sizeof(int32_t) * b->g->n,
+                       cudaMemcpyDeviceToHost));
     return BD_OK;
 }
 
@@ -1393,7 +1450,8 @@ bd_status bd_bfs_get_parents(bd_bfs *b, int64_t *parent)
     if (!b || !parent) { return BD_ERR_INVALID; }
     BD_CUDA(cudaSetDevice(b->device));
     BD_TRY(finalize_parents(b));
-    BD_CUDA(cudaMemcpy(parent, b->parent, sizeof(int64_t) * b->g->n, cudaMemcpyDeviceToHost));
+    BD_CUDA(cudaMemcpy(parent, b->out_parent ? b->out_parent : b->parent,
+                       sizeof(int64_t) * b->g->n, cudaMemcpyDeviceToHost));
     return BD_OK;
 }
 
@@ -1402,8 +1460,8 @@ bd_status bd_bfs_device_ptrs(bd_bfs *b, const int32_t **depth, const int64_t **p
     if (!b) { return BD_ERR_INVALID; }
     BD_CUDA(cudaSetDevice(b->device));
     BD_TRY(finalize_parents(b));
-    if (depth) { *depth = b->depth; }
-    if (parent) { *parent = b->parent; }
+    if (depth) { *depth = b->out_depth ? b->out_depth : b->depth; }
+    if (parent) { *parent = b->out_parent ? b->out_parent : b->parent; }
     return BD_OK;
 }
 

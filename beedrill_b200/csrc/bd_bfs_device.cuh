@@ -101,6 +101,7 @@ struct BfsParams {
     long long spin_limit;
     unsigned expected_ctas;
     const PolicyBlob *policy;  // null: no learned policy loaded
+    const uint32_t *perm;      // caller id -> traversal id (BD_ORDER_HUB), or null
 };
 
 }  // namespace bd

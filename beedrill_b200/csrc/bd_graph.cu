@@ -357,6 +357,47 @@ __global__ void isolated_bitmap_kernel(const int64_t *off, int64_t n, uint32_t *
     }
 }
 
+// Hub numbering: sort key of vertex v = (complement of its degree, v), so
+// the ascending sort lists vertices by degree, highest first, ties by id.
+__global__ void hub_keys_kernel(const int64_t *off, int64_t n, uint64_t *key)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = off[v + 1] - off[v];
+        const uint32_t dc = 0xFFFFFFFFu - (uint32_t)(d < 0xFFFFFFFFll ? d : 0xFFFFFFFFll);
+        key[v] = ((uint64_t)dc << 32) | (uint64_t)v;
+    }
+}
+
+// From the sorted keys: iperm (new -> old), perm (old -> new) and the
+// degree of each new vertex (the scan input of the new offsets).
+__global__ void hub_perm_kernel(const uint64_t *sorted, const int64_t *off, int64_t n,
+                                uint32_t *perm, uint32_t *iperm, int64_t *tdeg)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = (uint32_t)sorted[i];
+        iperm[i] = v;
+        perm[v] = (uint32_t)i;
+        tdeg[i] = off[v + 1] - off[v];
+    }
+}
+
+// Neighbour list of new vertex i = the list of old vertex iperm[i], each
+// neighbour renamed; one warp per vertex, 32 arcs at a time.
+__global__ void hub_adj_kernel(const int64_t *off, const uint32_t *adj, const uint32_t *perm,
+                               const uint32_t *iperm, const int64_t *toff, int64_t n,
+                               uint32_t *tadj)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const uint32_t v = iperm[i];
+        const int64_t b = off[v], e = off[v + 1], t = toff[i];
+        for (int64_t k = b + lane; k < e; k += 32) { tadj[t + (k - b)] = perm[adj[k]]; }
+    }
+}
+
 __global__ void validate_csr_kernel(const int64_t *off, const uint32_t *adj, int64_t n,
                                     int64_t arcs, int *bad)
 {
@@ -549,7 +590,50 @@ void graph_free(bd_graph *g)
     cudaFree(g->d_isolated);
     cudaFree(g->d_src);
     cudaFree(g->d_dst);
+    cudaFree(g->d_toff);
+    cudaFree(g->d_tadj);
+    cudaFree(g->d_tisolated);
+    cudaFree(g->d_perm);
+    cudaFree(g->d_iperm);
     delete g;
+}
+
+bd_status graph_build_hub(bd_graph *g, cudaStream_t s)
+{
+    const int64_t n = g->n;
+    const int64_t words = bitmap_words(n);
+    if (cudaMalloc(&g->d_toff, sizeof(int64_t) * (n + 1)) != cudaSuccess ||
+        cudaMalloc(&g->d_tadj, sizeof(uint32_t) * (g->arcs ? g->arcs : 1)) != cudaSuccess ||
+        cudaMalloc(&g->d_tisolated, sizeof(uint32_t) * (words ? words : 1)) != cudaSuccess ||
+        cudaMalloc(&g->d_perm, sizeof(uint32_t) * (n ? n : 1)) != cudaSuccess ||
+        cudaMalloc(&g->d_iperm, sizeof(uint32_t) * (n ? n : 1)) != cudaSuccess) {
+        return BD_ERR_OOM;
+    }
+    DevBuf<uint64_t> key, sorted;
+    DevBuf<int64_t> tdeg;
+    if (key.alloc(n) != cudaSuccess || sorted.alloc(n) != cudaSuccess ||
+        tdeg.alloc(n + 1) != cudaSuccess) {
+        return BD_ERR_OOM;
+    }
+    hub_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(g->d_off, n, key.p);
+    BD_CUDA(cudaGetLastError());
+    BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
+        return cub::DeviceRadixSort::SortKeys(tmp, bytes, key.p, sorted.p, n, 0, 64, s);
+    }, s));
+    hub_perm_kernel<<<grid_for(n), kThreads, 0, s>>>(sorted.p, g->d_off, n, g->d_perm, g->d_iperm,
+                                                     tdeg.p);
+    BD_CUDA(cudaGetLastError());
+    BD_CUDA(cudaMemsetAsync(tdeg.p + n, 0, sizeof(int64_t), s));
+    BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
+        return cub::DeviceScan::ExclusiveSum(tmp, bytes, tdeg.p, g->d_toff, n + 1, s);
+    }, s));
+    hub_adj_kernel<<<grid_for(n * 32), kThreads, 0, s>>>(g->d_off, g->d_adj, g->d_perm, g->d_iperm,
+                                                          g->d_toff, n, g->d_tadj);
+    BD_CUDA(cudaGetLastError());
+    isolated_bitmap_kernel<<<grid_for(words), kThreads, 0, s>>>(g->d_toff, n, g->d_tisolated);
+    BD_CUDA(cudaGetLastError());
+    BD_CUDA(cudaStreamSynchronize(s));
+    return BD_OK;
 }
 
 bd_status graph_finish(bd_graph *g, cudaStream_t s)
@@ -627,7 +711,7 @@ bd_status graph_from_device_edges(int64_t n, int64_t m, int64_t *d_src, int64_t 
     int flag = 0;
     if (read_flag(bad.p, &flag) != BD_OK) { return fail(BD_ERR_CUDA); }
     if (flag) { return fail(BD_ERR_RANGE); }
-    if (order == BD_ORDER_DEGREE) {
+    if (order == BD_ORDER_DEGREE || order == BD_ORDER_HUB) {
         // Re-sort every list by neighbour degree, highest first; the stable
         // sort keeps insertion order among equal degrees.
         DevBuf<uint64_t> k_in, k_out;
@@ -651,6 +735,7 @@ bd_status graph_from_device_edges(int64_t n, int64_t m, int64_t *d_src, int64_t 
         }
     }
     bd_status st = graph_finish(g, s);
+    if (st == BD_OK && order == BD_ORDER_HUB) { st = graph_build_hub(g, s); }
     if (st != BD_OK) { return fail(st); }
     *out = g;
     return BD_OK;
@@ -668,7 +753,7 @@ bd_status bd_graph_from_edges(int64_t num_vertices, int64_t num_edges, const int
     if (!out || (!src && num_edges) || (!dst && num_edges) || num_vertices <= 0 || num_edges < 0) {
         return BD_ERR_INVALID;
     }
-    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_DEGREE) {
+    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_HUB) {
         return BD_ERR_INVALID;
     }
     if (num_vertices > (int64_t)UINT32_MAX) { return BD_ERR_LIMIT; }
@@ -695,7 +780,7 @@ bd_status bd_graph_from_edges(int64_t num_vertices, int64_t num_edges, const int
 bd_status bd_graph_from_el64(const char *path, int32_t adjacency_order, bd_graph **out)
 {
     if (!path || !out) { return BD_ERR_INVALID; }
-    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_DEGREE) {
+    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_HUB) {
         return BD_ERR_INVALID;
     }
     FILE *fp = fopen(path, "rb");
@@ -801,6 +886,7 @@ bd_status bd_graph_from_csr(int64_t num_vertices, int64_t num_arcs, const int64_
     }
     if (flag) { graph_free(g); return BD_ERR_FORMAT; }
     bd_status st = graph_finish(g, 0);
+    if (st == BD_OK && g->order == BD_ORDER_HUB) { st = graph_build_hub(g, 0); }
     if (st != BD_OK) { graph_free(g); return st; }
     *out = g;
     return BD_OK;
@@ -815,7 +901,7 @@ bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, 
     if (!(a >= 0 && b >= 0 && c >= 0 && d >= 0 && a <= 1 && b <= 1 && c <= 1 && d <= 1)) {
         return BD_ERR_INVALID;
     }
-    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_DEGREE) {
+    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_HUB) {
         return BD_ERR_INVALID;
     }
     BD_TRY(ensure_device());
@@ -891,7 +977,7 @@ bd_status bd_graph_grid(int64_t rows, int64_t cols, double delete_frac, uint64_t
     if (!out || rows < 1 || cols < 1 || !(delete_frac >= 0.0 && delete_frac <= 1.0)) {
         return BD_ERR_INVALID;
     }
-    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_DEGREE) {
+    if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_HUB) {
         return BD_ERR_INVALID;
     }
     if (rows * cols > (int64_t)UINT32_MAX) { return BD_ERR_LIMIT; }

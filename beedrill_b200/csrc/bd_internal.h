@@ -50,11 +50,27 @@ struct bd_graph {
     // Edge list in file / generation order, kept for el64 export and check.
     int64_t *d_src = nullptr;     // [m] or null
     int64_t *d_dst = nullptr;     // [m] or null
+    // BD_ORDER_HUB: the traversal CSR, vertices renumbered by degree
+    // (highest first), its isolated bitmap, and the two numberings.
+    // Null for the other orders: the traversal kernels use d_off / d_adj.
+    int64_t *d_toff = nullptr;      // [n + 1]
+    uint32_t *d_tadj = nullptr;     // [arcs]
+    uint32_t *d_tisolated = nullptr;  // [words(n)]
+    uint32_t *d_perm = nullptr;     // [n] caller id -> traversal id
+    uint32_t *d_iperm = nullptr;    // [n] traversal id -> caller id
 };
 
 namespace bd {
 
 inline int64_t bitmap_words(int64_t n) { return (n + 31) / 32; }
+
+// The CSR the traversal kernels run on.
+inline const int64_t *traversal_off(const bd_graph *g) { return g->d_toff ? g->d_toff : g->d_off; }
+inline const uint32_t *traversal_adj(const bd_graph *g) { return g->d_tadj ? g->d_tadj : g->d_adj; }
+inline const uint32_t *traversal_isolated(const bd_graph *g)
+{
+    return g->d_tisolated ? g->d_tisolated : g->d_isolated;
+}
 
 // Builds the CSR of an edge list that is already on the device (src/dst
 // int64[m]); takes ownership of d_src/d_dst.
@@ -67,6 +83,8 @@ bd_status policy_blob(const float *params, const float *mean, const float *inv_s
 // hybrid_bfs::check on the host for a parent array in the reference's
 // encoding; *ok = 1 when it passes.
 bd_status check_parents(const bd_graph *g, int64_t source, const int64_t *parent, int32_t *ok);
+// BD_ORDER_HUB: builds the renumbered traversal CSR of a finished graph.
+bd_status graph_build_hub(bd_graph *g, cudaStream_t s);
 // Fills d_isolated from d_off.
 bd_status graph_finish(bd_graph *g, cudaStream_t s);
 void graph_free(bd_graph *g);

@@ -110,6 +110,7 @@ struct MsParams {
     unsigned expected_ctas;
     int force_dir;  // -1 rule, kPush, kPull
     const PolicyBlob *policy;  // null: the rule decides
+    const uint32_t *perm;      // caller id -> traversal id (BD_ORDER_HUB), or null
     // vertices whose pull scan is split into chunks over all warps
     const uint32_t *heavy;           // [n_heavy]
     const ull *heavy_cbase;          // [n_heavy + 1] chunk prefix sums
@@ -860,7 +861,7 @@ __global__ void ms_init_kernel(MsParams p, const int64_t *sources, int count)
     long long nsmall = 0, nf = 0, degsum = 0, done = 0;
     ull lp = 0;
     for (int r = 0; r < count; ++r) {
-        const uint32_t s = (uint32_t)sources[r];
+        const uint32_t s = p.perm ? p.perm[sources[r]] : (uint32_t)sources[r];
         const ull bit = 1ull << r;
         const ull before = p.F[0][s];
         p.F[0][s] = before | bit;
@@ -944,17 +945,22 @@ __global__ void ms_count_kernel(const ull *seen, const int64_t *off, int64_t n, 
 // clearing between runs (only the record counts do).
 __global__ void ms_extract_kernel(const int32_t *depth, const uint32_t *parent, const uint4 *rec,
                                   const uint32_t *rec_cnt, const ull *seen, const int64_t *off,
-                                  int64_t n, int R, int r, int32_t *depth_out, int64_t *parent_out)
+                                  int64_t n, int R, int r, const uint32_t *perm,
+                                  const uint32_t *iperm, int32_t *depth_out, int64_t *parent_out)
 {
+    // v: the caller's vertex id (output index, off); t: its traversal id
+    // (state index, parents named by traversal id) -- equal unless the
+    // graph has a hub numbering
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
          v += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = perm ? (int64_t)perm[v] : v;
         int32_t d = -1;
         uint32_t par = 0;
-        if ((seen[v] >> r) & 1ull) {
-            const unsigned cnt = min(rec_cnt[v], kRecSlots);
+        if ((seen[t] >> r) & 1ull) {
+            const unsigned cnt = min(rec_cnt[t], kRecSlots);
             bool found = false;
             for (unsigned i = 0; i < cnt && !found; ++i) {
-                const uint4 x = rec[v * kRecSlots + i];
+                const uint4 x = rec[t * kRecSlots + i];
                 const ull mask = ((ull)x.y << 32) | x.x;
                 if ((mask >> r) & 1ull) {
                     d = (int32_t)x.w;
@@ -963,14 +969,14 @@ __global__ void ms_extract_kernel(const int32_t *depth, const uint32_t *parent, 
                 }
             }
             if (!found) {
-                d = depth[v * R + r];
-                par = parent[v * R + r];
+                d = depth[t * R + r];
+                par = parent[t * R + r];
             }
         }
         if (depth_out) { depth_out[v] = d; }
         if (parent_out) {
             if (d >= 0) {
-                parent_out[v] = (int64_t)par;
+                parent_out[v] = (int64_t)(iperm ? iperm[par] : par);
             } else {
                 const int64_t g = off[v + 1] - off[v];
                 parent_out[v] = g != 0 ? -g : -1;
@@ -1048,8 +1054,9 @@ MsKernel ms_pick(int block)
 MsParams ms_params(bd_msbfs *b, int group, int count)
 {
     MsParams p{};
-    p.off = b->g->d_off;
-    p.adj = b->g->d_adj;
+    p.off = traversal_off(b->g);
+    p.adj = traversal_adj(b->g);
+    p.perm = b->g->d_perm;
     p.done = b->done;
     p.n = b->g->n;
     p.m = b->g->m;
@@ -1094,7 +1101,7 @@ bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
     const int64_t n = b->g->n;
     BD_CUDA(cudaMemsetAsync(b->seen + group * n, 0, sizeof(ull) * n, b->stream));
     BD_CUDA(cudaMemsetAsync(b->drec_cnt + group * n, 0, sizeof(uint32_t) * n, b->stream));
-    BD_CUDA(cudaMemcpyAsync(b->done, b->g->d_isolated, sizeof(uint32_t) * ((n + 31) / 32),
+    BD_CUDA(cudaMemcpyAsync(b->done, traversal_isolated(b->g), sizeof(uint32_t) * ((n + 31) / 32),
                             cudaMemcpyDeviceToDevice, b->stream));
     for (int i = 0; i < 3; ++i) {
         BD_CUDA(cudaMemsetAsync(b->F[i], 0, sizeof(ull) * n, b->stream));
@@ -1108,7 +1115,7 @@ bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
                                         dim3(b->block), args, 0, b->stream));
     unsigned long long *dst = b->d_counts + 128 * group;
     BD_CUDA(cudaMemsetAsync(dst, 0, sizeof(unsigned long long) * 128, b->stream));
-    ms_count_kernel<<<148 * 8, 256, 0, b->stream>>>(p.seen, b->g->d_off, n, p.all, count, dst);
+    ms_count_kernel<<<148 * 8, 256, 0, b->stream>>>(p.seen, p.off, n, p.all, count, dst);
     BD_CUDA(cudaGetLastError());
     return BD_OK;
 }
@@ -1207,9 +1214,9 @@ bd_status ms_extract(bd_msbfs *b, int32_t root_index, int32_t *depth, int64_t *p
     BD_CUDA(cudaMalloc(&tmp, bytes));
     ms_extract_kernel<<<ms_grid_for(n), 256, 0, b->stream>>>(
         b->depth + group * slice, b->parent + group * slice, b->drec + group * n * (int64_t)kRecSlots,
-        b->drec_cnt + group * n, b->seen + group * n, b->g->d_off, n,
-        b->R, lane,
-        depth ? static_cast<int32_t *>(tmp) : nullptr, parent ? static_cast<int64_t *>(tmp) : nullptr);
+        b->drec_cnt + group * n, b->seen + group * n, b->g->d_off, n, b->R, lane, b->g->d_perm,
+        b->g->d_iperm, depth ? static_cast<int32_t *>(tmp) : nullptr,
+        parent ? static_cast<int64_t *>(tmp) : nullptr);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) {
         e = cudaMemcpyAsync(depth ? (void *)depth : (void *)parent, tmp, bytes,
@@ -1299,7 +1306,8 @@ bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *o
     // heavy vertices and their chunk prefix sums (host, once per handle)
     {
         std::vector<int64_t> off(n + 1);
-        if (cudaMemcpy(off.data(), g->d_off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost) !=
+        if (cudaMemcpy(off.data(), traversal_off(g), sizeof(int64_t) * (n + 1),
+                       cudaMemcpyDeviceToHost) !=
             cudaSuccess) {
             return fail(BD_ERR_CUDA);
         }

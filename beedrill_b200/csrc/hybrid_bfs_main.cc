@@ -18,6 +18,8 @@
 //                      time divided evenly
 //   --degree_order     neighbour lists ordered by neighbour degree, highest
 //                      first (results are unchanged)
+//   --hub_layout       --degree_order, and the traversal runs on vertices
+//                      renumbered by degree (results in the file's ids)
 // Algorithms: the reference's four names plus top_down, bottom_up, learned.
 #include <getopt.h>
 #include <unistd.h>
@@ -58,6 +60,7 @@ const struct option long_options[] = {
     {"policy_file", required_argument, nullptr, 0},
     {"batched", no_argument, nullptr, 0},
     {"degree_order", no_argument, nullptr, 0},
+    {"hub_layout", no_argument, nullptr, 0},
     {nullptr, 0, nullptr, 0},
 };
 
@@ -87,6 +90,7 @@ void print_help(const char *argv0)
     printf("\t--policy_file FILE   Trained direction policy for --algorithm learned\n");
     printf("\t--batched            Run all trials' roots together (64 per group)\n");
     printf("\t--degree_order       Order neighbour lists by neighbour degree\n");
+    printf("\t--hub_layout         Traverse with vertices renumbered by degree\n");
     printf("\t--version            Print version info\n");
     printf("\t--help               Print command line help\n");
 }
@@ -112,6 +116,7 @@ struct bfs_args {
     const char *policy_file = nullptr;
     bool batched = false;
     bool degree_order = false;
+    bool hub_layout = false;
 };
 
 bfs_args parse(int argc, char **argv)
@@ -147,6 +152,7 @@ bfs_args parse(int argc, char **argv)
         else if (name == "policy_file") { a.policy_file = optarg; }
         else if (name == "batched") { a.batched = true; }
         else if (name == "degree_order") { a.degree_order = true; }
+        else if (name == "hub_layout") { a.hub_layout = true; }
         else if (name == "version") {
             printf("%s\n", bd_version());
             exit(0);
@@ -266,7 +272,8 @@ int main(int argc, char **argv)
     bool success = true;
     bfs_args args = parse(argc, argv);
     try {
-        const int32_t order = args.degree_order       ? BD_ORDER_DEGREE
+        const int32_t order = args.hub_layout         ? BD_ORDER_HUB
+                              : args.degree_order     ? BD_ORDER_DEGREE
                               : args.sort_edge_blocks ? BD_ORDER_SORTED
                                                       : BD_ORDER_INSERTION;
         beedrill::graph g = args.rmat_scale > 0

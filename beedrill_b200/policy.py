@@ -344,10 +344,10 @@ def training_graph_specs(count=200, seed=2024):
 
 
 def collect(specs, roots_per_graph=4, repeats=1, log=None, order=None):
-    """Level tables of the training graphs, built with the adjacency order
-    the policy will run on (neighbour-degree order by default, as the
-    benchmark's graphs are; the order changes bottom-up costs)."""
-    order = bd.ORDER_DEGREE if order is None else order
+    """Level tables of the training graphs, built with the layout the
+    policy will run on (the hub numbering by default, as the benchmark's
+    graphs are; the layout changes step costs)."""
+    order = bd.ORDER_HUB if order is None else order
     tables = []
     for i, s in enumerate(specs):
         g = bd.Graph.rmat(s["scale"], s["edge_factor"], s["a"], s["b"], s["c"], s["d"], s["seed"],
@@ -382,7 +382,7 @@ def train_batched(args, log):
     t0 = time.time()
     for i, s in enumerate(specs):
         g = bd.Graph.rmat(s["scale"], s["edge_factor"], s["a"], s["b"], s["c"], s["d"], s["seed"],
-                          order=bd.ORDER_DEGREE)
+                          order=bd.ORDER_HUB)
         tab = measure_tables_batched(g, g.pick_roots(s["seed"], 64))
         tab.meta.update(s)
         tables.append(tab)
@@ -403,7 +403,7 @@ def train_batched(args, log):
                    "loss_last": float(hist[-1]), "margin": mgn,
                    "validation": {"rule": rb, "learned": rl},
                    "distribution": "RMAT scales 16-22, A~U[0.45,0.65], D=0.05, B=C=(1-A-D)/2, "
-                                   "ef 16, 64 roots per graph, neighbour-degree adjacency order"}
+                                   "ef 16, 64 roots per graph, hub numbering"}
     policy.save(args.out)
     log(f"saved {args.out}: rule regret {rb['regret_frac']:.3%}, learned {rl['regret_frac']:.3%}")
     return 0
@@ -446,7 +446,7 @@ def main(argv=None):
         "loss_last": float(hist[-1]), "margin": mgn,
         "validation": {"beamer": rb, "learned": rl},
         "distribution": "RMAT scales 16-22, A~U[0.45,0.65], D=0.05, B=C=(1-A-D)/2, ef 16, "
-                        "neighbour-degree adjacency order",
+                        "hub numbering",
     }
     policy.save(args.out)
     log(f"saved {args.out}: beamer regret {rb['regret_frac']:.3%}, learned {rl['regret_frac']:.3%}")

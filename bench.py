@@ -296,8 +296,8 @@ def main():
     ap.add_argument("--scale", type=int, default=None, help="override the RMAT scale")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-roots", type=int, default=3)
-    ap.add_argument("--order", default="degree", choices=["insertion", "sorted", "degree"],
-                    help="adjacency order of the CSR (results are the same for all three)")
+    ap.add_argument("--order", default="hub", choices=["insertion", "sorted", "degree", "hub"],
+                    help="adjacency order / numbering the kernels run on (same results for all)")
     args = ap.parse_args()
     if args.impl == "reference":
         return impl_reference(args)
@@ -313,7 +313,7 @@ def main():
 
     w = dict(WORKLOADS[args.workload])
     order = {"insertion": bd.ORDER_INSERTION, "sorted": bd.ORDER_SORTED,
-             "degree": bd.ORDER_DEGREE}[args.order]
+             "degree": bd.ORDER_DEGREE, "hub": bd.ORDER_HUB}[args.order]
     if w["kind"] == "packed":
         if world > 1:
             raise SystemExit("packed512 runs on one GPU")

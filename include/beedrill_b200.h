@@ -58,6 +58,14 @@ typedef struct bd_bfs bd_bfs;
 #define BD_ORDER_SORTED 1    /* ascending neighbour id                          */
 #define BD_ORDER_DEGREE 2    /* highest-degree neighbour first (ties: insertion
                                 order); bottom-up scans meet visited hubs first */
+#define BD_ORDER_HUB 3       /* BD_ORDER_DEGREE, and the traversal kernels run on
+                                a second CSR whose vertices are renumbered by
+                                degree, highest first (ties: id): the state of
+                                the hubs most arcs lead to is packed into a few
+                                cache lines.  Every call still takes and returns
+                                the caller's vertex ids; the CSR the graph calls
+                                expose is the BD_ORDER_DEGREE one.  No
+                                counterpart in the reference. */
 
 /* Direction policies (the reference's --algorithm values map onto these). */
 #define BD_ALG_BEAMER 0    /* beamer_hybrid, remote_writes_hybrid                */

@@ -35,7 +35,7 @@ def test_cli_runs_and_checks(alg):
 
 def test_cli_batched_matches_one_by_one():
     rc1, one = _run("--rmat_scale", "14", "--num_trials", "70", "--degree_order")
-    rc2, bat = _run("--rmat_scale", "14", "--num_trials", "70", "--degree_order", "--batched",
+    rc2, bat = _run("--rmat_scale", "14", "--num_trials", "70", "--hub_layout", "--batched",
                     "--algorithm", "learned", "--check_results")
     assert rc1 == 0 and rc2 == 0, (one, bat)
     assert bat.count("PASS") == 70 and "FAIL" not in bat

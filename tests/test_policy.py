@@ -117,7 +117,7 @@ def test_trained_policy_vs_beamer_on_held_out_graphs():
     pol = P.Policy.load()
     tables = []
     for scale, a, b, d, seed in _held_out_specs(10, 1):
-        g = bd.Graph.rmat(scale, 16, a, b, b, d, seed, order=bd.ORDER_DEGREE)
+        g = bd.Graph.rmat(scale, 16, a, b, b, d, seed, order=bd.ORDER_HUB)
         tables += P.measure_tables(g, g.pick_roots(seed, 2), repeats=2, with_beamer=False)
         g.close()
     rb = P.regret(tables, P.beamer_dirs)
@@ -136,7 +136,7 @@ def test_trained_policies_at_scale24_held_out():
     from beedrill_b200 import policy as P
     if not (os.path.exists(P.DEFAULT_PATH) and os.path.exists(P.BATCHED_PATH)):
         pytest.skip("no trained policies committed")
-    g = bd.Graph.rmat(24, 16, seed=2424, order=bd.ORDER_DEGREE)
+    g = bd.Graph.rmat(24, 16, seed=2424, order=bd.ORDER_HUB)
     tables = P.measure_tables(g, g.pick_roots(7, 16), repeats=2, with_beamer=False)
     pol = P.Policy.load()
     rb = P.regret(tables, P.beamer_dirs)
@@ -160,7 +160,7 @@ def test_trained_batched_policy_vs_rule_on_held_out_graphs():
     pol = P.Policy.load(P.BATCHED_PATH)
     tables = []
     for scale, a, b, d, seed in _held_out_specs(5, 2):
-        g = bd.Graph.rmat(scale, 16, a, b, b, d, seed, order=bd.ORDER_DEGREE)
+        g = bd.Graph.rmat(scale, 16, a, b, b, d, seed, order=bd.ORDER_HUB)
         tables.append(P.measure_tables_batched(g, g.pick_roots(seed, 64), repeats=2))
         g.close()
     rule = P.regret(tables, P.alpha_dirs)
