@@ -339,106 +339,119 @@ __device__ void bu_step(const BfsParams &p, const StepView &sv, Local &loc)
     Acc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
 
-    for (long long w0 = gw * K; w0 < p.words; w0 += nw * K) {
-        uint32_t word[K];
-        unsigned open = 0;  // words with work
+    // Warp gw owns groups gw, gw + nw, gw + 2 nw, ... of K words.  It loads
+    // 32 / K of its groups at once (one word per lane), passes full groups
+    // through, and works only on the groups with unvisited vertices: late
+    // levels, where most words are full, cost a bitmap sweep.
+    constexpr int GPB = 32 / K;
+    constexpr unsigned kGroupMask = (1u << K) - 1u;
+    for (long long t0 = 0; (gw + t0 * nw) * K < p.words; t0 += GPB) {
+        const int j = lane / K;
+        const long long wl = (gw + (t0 + j) * nw) * K + lane % K;
+        const uint32_t mw = wl < p.words ? __ldcg(&vin[wl]) : kFull;
+        const unsigned openm = __ballot_sync(kFull, mw != kFull);
+        if (!((openm >> (j * K)) & kGroupMask) && wl < p.words) { vout[wl] = kFull; }
+        unsigned groups = 0;
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-            word[k] = (w0 + k < p.words) ? __ldcg(&vin[w0 + k]) : kFull;
-            if (word[k] != kFull) { open |= 1u << k; }
+        for (int g = 0; g < GPB; ++g) {
+            if ((openm >> (g * K)) & kGroupMask) { groups |= 1u << g; }
         }
-        if (!open) {
-            if (lane < K && w0 + lane < p.words) { vout[w0 + lane] = kFull; }
-            continue;
-        }
-        uint32_t v[K], par[K];
-        bool found[K], unv[K];
-        int64_t beg[K], end[K], next[K];
+        while (groups) {
+            const int g = __ffs(groups) - 1;
+            groups &= groups - 1;
+            const long long w0 = (gw + (t0 + g) * nw) * K;
+            uint32_t word[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-            v[k] = (uint32_t)((w0 + k) * 32 + lane);
-            unv[k] = !((word[k] >> lane) & 1u);
-            found[k] = false;
-            par[k] = 0;
-            beg[k] = end[k] = next[k] = 0;
-            if (unv[k]) {
-                beg[k] = __ldg(&p.off[v[k]]);
-                end[k] = __ldg(&p.off[v[k] + 1]);
-            }
-        }
-        // per-lane scan of the first bu_prefix arcs, P arcs per word per round
-        for (int r = 0; r < p.bu_prefix; r += P) {
-            uint32_t x[K][P];
-            bool in[K][P];
+            for (int k = 0; k < K; ++k) { word[k] = __shfl_sync(kFull, mw, g * K + k); }
+            uint32_t v[K], par[K];
+            bool found[K], unv[K];
+            int64_t beg[K], end[K], next[K];
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-#pragma unroll
-                for (int j = 0; j < P; ++j) {
-                    const int64_t e = beg[k] + r + j;
-                    in[k][j] = unv[k] && !found[k] && e < end[k];
-                    x[k][j] = in[k][j] ? __ldg(&p.adj[e]) : 0u;
+                v[k] = (uint32_t)((w0 + k) * 32 + lane);
+                unv[k] = !((word[k] >> lane) & 1u);
+                found[k] = false;
+                par[k] = 0;
+                beg[k] = end[k] = next[k] = 0;
+                if (unv[k]) {
+                    beg[k] = __ldg(&p.off[v[k]]);
+                    end[k] = __ldg(&p.off[v[k] + 1]);
                 }
             }
-            uint32_t bits[K][P];
+            // per-lane scan of the first bu_prefix arcs, P arcs per word per round
+            for (int r = 0; r < p.bu_prefix; r += P) {
+                uint32_t x[K][P];
+                bool in[K][P];
 #pragma unroll
-            for (int k = 0; k < K; ++k) {
+                for (int k = 0; k < K; ++k) {
 #pragma unroll
-                for (int j = 0; j < P; ++j) { bits[k][j] = in[k][j] ? ld_bits(&vin[x[k][j] >> 5]) : 0u; }
-            }
-            bool more = false;
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-#pragma unroll
-                for (int j = 0; j < P; ++j) {
-                    if (in[k][j] && !found[k] && ((bits[k][j] >> (x[k][j] & 31)) & 1u)) {
-                        found[k] = true;
-                        par[k] = x[k][j];
+                    for (int j = 0; j < P; ++j) {
+                        const int64_t e = beg[k] + r + j;
+                        in[k][j] = unv[k] && !found[k] && e < end[k];
+                        x[k][j] = in[k][j] ? __ldg(&p.adj[e]) : 0u;
                     }
                 }
-                more |= unv[k] && !found[k] && beg[k] + r + P < end[k];
-            }
-            if (!__any_sync(kFull, more)) { break; }
-        }
+                uint32_t bits[K][P];
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int64_t lim = min(end[k], beg[k] + (int64_t)((p.bu_prefix + P - 1) / P * P));
-            next[k] = found[k] ? end[k] : lim;
-            unsigned pending = __ballot_sync(kFull, unv[k] && !found[k] && next[k] < end[k]);
-            while (pending) {
-                const int owner = __ffs(pending) - 1;
-                pending &= pending - 1;
-                const int64_t b = __shfl_sync(kFull, next[k], owner);
-                const int64_t e = __shfl_sync(kFull, end[k], owner);
-                for (int64_t base = b; base < e; base += 32) {
-                    const int64_t kk = base + lane;
-                    bool hit = false;
-                    uint32_t xx = 0;
-                    if (kk < e) {
-                        xx = __ldg(&p.adj[kk]);
-                        hit = (ld_bits(&vin[xx >> 5]) >> (xx & 31)) & 1u;
-                    }
-                    const unsigned hm = __ballot_sync(kFull, hit);
-                    if (hm) {
-                        const uint32_t hx = __shfl_sync(kFull, xx, __ffs(hm) - 1);
-                        if (lane == owner) {
+                for (int k = 0; k < K; ++k) {
+#pragma unroll
+                    for (int j = 0; j < P; ++j) { bits[k][j] = in[k][j] ? ld_bits(&vin[x[k][j] >> 5]) : 0u; }
+                }
+                bool more = false;
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+#pragma unroll
+                    for (int j = 0; j < P; ++j) {
+                        if (in[k][j] && !found[k] && ((bits[k][j] >> (x[k][j] & 31)) & 1u)) {
                             found[k] = true;
-                            par[k] = hx;
+                            par[k] = x[k][j];
                         }
-                        break;
+                    }
+                    more |= unv[k] && !found[k] && beg[k] + r + P < end[k];
+                }
+                if (!__any_sync(kFull, more)) { break; }
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int64_t lim = min(end[k], beg[k] + (int64_t)((p.bu_prefix + P - 1) / P * P));
+                next[k] = found[k] ? end[k] : lim;
+                unsigned pending = __ballot_sync(kFull, unv[k] && !found[k] && next[k] < end[k]);
+                while (pending) {
+                    const int owner = __ffs(pending) - 1;
+                    pending &= pending - 1;
+                    const int64_t b = __shfl_sync(kFull, next[k], owner);
+                    const int64_t e = __shfl_sync(kFull, end[k], owner);
+                    for (int64_t base = b; base < e; base += 32) {
+                        const int64_t kk = base + lane;
+                        bool hit = false;
+                        uint32_t xx = 0;
+                        if (kk < e) {
+                            xx = __ldg(&p.adj[kk]);
+                            hit = (ld_bits(&vin[xx >> 5]) >> (xx & 31)) & 1u;
+                        }
+                        const unsigned hm = __ballot_sync(kFull, hit);
+                        if (hm) {
+                            const uint32_t hx = __shfl_sync(kFull, xx, __ffs(hm) - 1);
+                            if (lane == owner) {
+                                found[k] = true;
+                                par[k] = hx;
+                            }
+                            break;
+                        }
                     }
                 }
+                const unsigned fm = __ballot_sync(kFull, found[k]);
+                if (lane == 0 && w0 + k < p.words) { vout[w0 + k] = word[k] | fm; }
+                if (found[k]) {
+                    p.depth[v[k]] = new_level;
+                    p.parent[v[k]] = (int64_t)par[k];
+                }
             }
-            const unsigned fm = __ballot_sync(kFull, found[k]);
-            if (lane == 0 && w0 + k < p.words) { vout[w0 + k] = word[k] | fm; }
-            if (found[k]) {
-                p.depth[v[k]] = new_level;
-                p.parent[v[k]] = (int64_t)par[k];
-            }
-        }
-        int64_t deg[K];
+            int64_t deg[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) { deg[k] = end[k] - beg[k]; }
-        warp_append_k<K>(p, acc, qout, found, v, deg, loc);
+            for (int k = 0; k < K; ++k) { deg[k] = end[k] - beg[k]; }
+            warp_append_k<K>(p, acc, qout, found, v, deg, loc);
+        }
     }
 }
 
