@@ -71,7 +71,8 @@ __device__ __forceinline__ float policy_gap_warp(const PolicyBlob *w, long long 
         ok = f >= w->lo[j] && f <= w->hi[j];
         x = (f - w->mean[j]) * w->inv_std[j];
     }
-    const bool trusted = __all_sync(full, ok);
+    // outside the trusted range the rule decides: skip the network
+    if (!__all_sync(full, ok)) { return nanf(""); }
     float a1 = w->b1[j];
 #pragma unroll
     for (int i = 0; i < kPolicyIn; ++i) { a1 += w->w1t[i][j] * __shfl_sync(full, x, i); }
@@ -89,8 +90,7 @@ __device__ __forceinline__ float policy_gap_warp(const PolicyBlob *w, long long 
         o0 += __shfl_xor_sync(full, o0, d);
         o1 += __shfl_xor_sync(full, o1, d);
     }
-    const float gap = (o1 + w->b3[1]) - (o0 + w->b3[0]);
-    return trusted ? gap : nanf("");
+    return (o1 + w->b3[1]) - (o0 + w->b3[0]);
 }
 
 }  // namespace bd

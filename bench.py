@@ -116,6 +116,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def reduce_over_ranks(step_ms: float, value: float, e2e: float, device=None):
+    """Replicas: every rank ran its own roots.  The step time is the slowest
+    rank's; the whole-job throughput is world x the slowest rank's (so a
+    fast rank cannot hide a slow one).  One all_reduce(MAX); `device` is the
+    rank's GPU under NCCL, None (CPU tensors) under gloo."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size()
+    t = torch.tensor([step_ms, -value, -e2e], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t[0]), world * -float(t[1]), world * -float(t[2])
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -442,13 +455,8 @@ def main():
     head = modes[best]
     value_rank, e2e_rank, step_ms = head["gteps"], head["e2e"], head["step_ms"]
     if world > 1:
-        import torch
-        t = torch.tensor([step_ms, -value_rank, -e2e_rank], device=f"cuda:{local}",
-                         dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms, worst, worst_e2e = float(t[0]), -float(t[1]), -float(t[2])
-        value = world * worst
-        e2e_value = world * worst_e2e
+        step_ms, value, e2e_value = reduce_over_ranks(step_ms, value_rank, e2e_rank,
+                                                      device=f"cuda:{local}")
     else:
         value, e2e_value = value_rank, e2e_rank
 
