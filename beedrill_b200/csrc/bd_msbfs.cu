@@ -1429,7 +1429,7 @@ bd_status bd_msbfs_set_policy(bd_msbfs *b, const float *params, const float *mea
 {
     if (!b) { return BD_ERR_INVALID; }
     BD_CUDA(cudaSetDevice(b->device));
-    if (!params) {
+    if (!params || isinf(margin)) {  // +inf margin: the rule decides, nothing is evaluated
         cudaFree(b->policy);
         b->policy = nullptr;
         b->graph_count = -1;  // captured launches hold the old pointer

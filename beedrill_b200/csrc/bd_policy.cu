@@ -321,7 +321,8 @@ bd_status bd_bfs_set_policy(bd_bfs *b, const float *params, const float *mean,
                             const float *inv_std, const float *lo, const float *hi, float margin)
 {
     if (!b) { return BD_ERR_INVALID; }
-    if (!params) { return bfs_install_policy(b, nullptr); }
+    // a margin of +inf: the rule decides every step, nothing is evaluated
+    if (!params || isinf(margin)) { return bfs_install_policy(b, nullptr); }
     PolicyBlob blob;
     BD_TRY(policy_blob(params, mean, inv_std, lo, hi, margin, &blob));
     return bfs_install_policy(b, &blob);

@@ -256,6 +256,17 @@ class Policy:
         bfs.set_policy(self.params, self.mean, self.inv_std, self.margin, self.lo, self.hi)
 
 
+def decisions_policy(policy: Policy) -> Policy | None:
+    """The trained network with the trusted range and margin that its
+    decisions alone favour (before its inference cost is counted), or None
+    if the trainer found none better than the rule."""
+    d = policy.info.get("decisions_only", {})
+    if d.get("lo") is None:
+        return None
+    return Policy(policy.params, policy.mean, policy.inv_std, float(d["margin"]), policy.info,
+                  np.array(d["lo"], np.float32), np.array(d["hi"], np.float32))
+
+
 def beamer_dirs(tab: LevelTable, alpha=15, beta=18) -> str:
     """run_beamer's decisions over a level table (hybrid_bfs.cc:152-191)."""
     etc, scout = 2 * tab.m, int(tab.frontier_edges[0])
@@ -339,42 +350,132 @@ def set_widen(pol: Policy, widen: float) -> None:
 
 WIDEN_CANDIDATES = (0.0, 0.5, 1.0, 2.0, 3.0)
 MARGIN_CANDIDATES = (0.0, 0.25, 0.5, 1.0, 2.0)
+OFF = float("inf")  # margin of a policy that leaves every step to the rule
 
 
-def train_policy(tables, rule_fn, args, log):
-    """Training with hyperparameters chosen for extrapolation.  The trusted
-    range (how far past the training extremes the network may decide) and
-    the margin are picked by training on the smaller training scales and
-    validating on the largest one; the final network is then trained on
-    every scale with those choices.  Every 5th graph (by seed) is kept out
-    of both for the report."""
+def inference_overhead(spec, policy, batched: bool, roots=16, repeats=3):
+    """Measured cost of the policy inside the traversal kernel, in ns per
+    level: (features only, features + network).  Three handles run the same
+    roots: no policy, a policy trusted nowhere (the kernel computes the
+    features and stops), and one trusted everywhere whose margin never lets
+    it override (the network runs, the rule still decides)."""
+    g = bd.Graph.rmat(spec["scale"], spec["edge_factor"], spec["a"], spec["b"], spec["c"],
+                      spec["d"], spec["seed"], order=bd.ORDER_HUB)
+    rs = g.pick_roots(spec["seed"] + 1, 64 if batched else roots)
+    big = np.full(NUM_FEATURES, 1e30, np.float32)
+    make = (lambda: bd.BatchedBFS(g, len(rs))) if batched else \
+        (lambda: bd.HybridBFS(g, alg="learned"))
+    variants = {"none": None, "features": (big, -big, 1.0), "network": (-big, big, 1e30)}
+    out = {}
+    for name, v in variants.items():
+        h = make()
+        if v is not None:
+            h.set_policy(policy.params, policy.mean, policy.inv_std, v[2], v[0], v[1])
+        ms, levels = [], []
+        for _ in range(repeats + 1):
+            if batched:
+                st = h.run(rs)
+                ms.append(st.ms)
+                levels.append(len(h.steps()))
+            else:
+                t, lv = 0.0, 0
+                for r in rs:
+                    h.clear()
+                    st = h.run(int(r))
+                    t += st.ms
+                    lv += len(h.steps())
+                ms.append(t)
+                levels.append(lv)
+        out[name] = (min(ms[1:]), float(np.mean(levels[1:])))
+        h.close()
+    g.close()
+    per_level = lambda a: max(0.0, (out[a][0] - out["none"][0]) * 1e6 / out["none"][1])  # noqa: E731
+    return per_level("features"), per_level("network")
+
+
+def priced_cost_ns(policy: Policy, tables, rule_fn, overhead) -> float:
+    """Cost of the policy's decisions plus its own inference cost: the
+    features at every level it is installed for, the network at the levels
+    its features are trusted."""
+    if policy.margin == OFF:
+        return sum(t.cost_ns(rule_fn(t)) for t in tables)
+    total = 0.0
+    for t in tables:
+        dirs = policy_dirs(policy, t, rule=rule_fn(t))
+        total += t.cost_ns(dirs)
+        prev_dir, prev_ns = 0, 0.0
+        for lv, d in enumerate(dirs):
+            raw = t.features(lv, prev_dir, prev_ns)
+            total += overhead[1] if policy.trusts(raw) else overhead[0]
+            prev_dir = 1 if d == "B" else 0
+            prev_ns = t.t_bu[lv] if d == "B" else t.t_td[lv]
+    return total
+
+
+def train_policy(tables, rule_fn, args, log, batched=False):
+    """Training with its two choices made on graphs it did not train on.
+
+    * How far past the training extremes the network may decide (its
+      trusted range) is chosen for extrapolation: a probe network trained
+      on the smaller training scales is scored, decisions alone, on the
+      largest one.
+    * Whether the network decides at all, and with what margin, is chosen
+      on validation graphs of every training scale, priced with the
+      network's measured inference cost inside the traversal kernel: the
+      network is kept only where its decisions save more than it costs.
+
+    Graphs split by seed: every 5th (seed % 5 == 0) for the report, the
+    next (seed % 5 == 1) for the margin, the rest for training."""
     report = [t for t in tables if t.meta["seed"] % 5 == 0]
-    rest = [t for t in tables if t.meta["seed"] % 5 != 0]
-    top = max(t.meta["scale"] for t in rest)
-    lower = [t for t in rest if t.meta["scale"] < top]
-    upper = [t for t in rest if t.meta["scale"] == top]
+    val = [t for t in tables if t.meta["seed"] % 5 == 1]
+    train = [t for t in tables if t.meta["seed"] % 5 > 1]
+    top = max(t.meta["scale"] for t in train)
+    lower = [t for t in train if t.meta["scale"] < top]
+    upper = [t for t in train if t.meta["scale"] == top]
     X, y, w = dataset(lower)
     probe, _ = fit(X, y, w, epochs=args.epochs, lr=args.lr)
-    best = None
+    widen_cost = []
     for widen in WIDEN_CANDIDATES:
         set_widen(probe, widen)
-        for mgn in MARGIN_CANDIDATES:
-            probe.margin = mgn
-            cost = regret(upper, lambda t: policy_dirs(probe, t, rule=rule_fn(t)))["cost_ms"]
-            if best is None or cost < best[0] - 1e-9:
-                best = (cost, widen, mgn)
-    log(f"extrapolation to scale {top}: trust +{best[1]} sd, margin {best[2]} "
-        f"({best[0]:.3f} ms vs rule {regret(upper, rule_fn)['cost_ms']:.3f} ms)")
-    X, y, w = dataset(rest)
-    policy, hist = fit(X, y, w, epochs=args.epochs, lr=args.lr, widen=best[1])
-    policy.margin = best[2]
+        widen_cost.append((regret(upper, lambda t: policy_dirs(probe, t, rule=rule_fn(t)))["cost_ms"],
+                           widen))
+    widen = min(widen_cost)[1]
+    log(f"trusted range for extrapolation to scale {top}: training extremes +{widen} sd")
+    X, y, w = dataset(train)
+    policy, hist = fit(X, y, w, epochs=args.epochs, lr=args.lr, widen=widen)
+    overhead = inference_overhead(upper[0].meta, policy, batched)
+    log(f"inference cost per level: features {overhead[0]:.0f} ns, network {overhead[1]:.0f} ns")
+    policy.margin = OFF
+    rule_cost = priced_cost_ns(policy, val, rule_fn, overhead)
+    best, best_d = (rule_cost, OFF), (rule_cost, OFF)
+    for mgn in MARGIN_CANDIDATES:
+        policy.margin = mgn
+        cost = priced_cost_ns(policy, val, rule_fn, overhead)
+        cost_d = priced_cost_ns(policy, val, rule_fn, (0.0, 0.0))
+        if cost < best[0] - 1e-6:
+            best = (cost, mgn)
+        if cost_d < best_d[0] - 1e-6:
+            best_d = (cost_d, mgn)
+    log(f"margin {best[1]} ({best[0] * 1e-6:.3f} ms with inference vs rule {rule_cost * 1e-6:.3f} ms "
+        f"on {len(val)} validation tables); decisions alone favour margin {best_d[1]}")
     rb = regret(report, rule_fn)
+    decisions = {"trust_widen_sd": widen, "margin": best_d[1]}
+    if best_d[1] != OFF:
+        policy.margin = best_d[1]
+        decisions.update(lo=[float(v) for v in policy.lo], hi=[float(v) for v in policy.hi],
+                         validation={"rule": rb, "learned": regret(
+                             report, lambda t: policy_dirs(policy, t, rule=rule_fn(t)))})
+    policy.margin = best[1]
     rl = regret(report, lambda t: policy_dirs(policy, t, rule=rule_fn(t)))
     policy.info = {"samples": int(len(y)), "epochs": args.epochs, "lr": args.lr,
                    "loss_first": float(hist[0]), "loss_last": float(hist[-1]),
-                   "margin": best[2], "trust_widen_sd": best[1],
-                   "selection": f"train on scales < {top}, validate on scale {top}",
-                   "validation": {"rule": rb, "learned": rl}}
+                   "margin": best[1], "trust_widen_sd": widen,
+                   "inference_ns_per_level": {"features": overhead[0], "network": overhead[1]},
+                   "selection": f"trusted range: train on scales < {top}, score on {top}; margin: "
+                                "validation graphs of every scale, priced with the measured "
+                                "inference cost",
+                   "validation": {"rule": rb, "learned": rl},
+                   "decisions_only": decisions}
     return policy, rb, rl
 
 
@@ -427,7 +528,7 @@ def train_batched(args, log):
         if (i + 1) % 20 == 0:
             log(f"collected {i + 1}/{len(specs)} graphs")
     log(f"{len(tables)} batched level tables in {time.time() - t0:.1f} s")
-    policy, rb, rl = train_policy(tables, alpha_dirs, args, log)
+    policy, rb, rl = train_policy(tables, alpha_dirs, args, log, batched=True)
     policy.info.update({"kind": "batched", "graphs": args.graphs,
                         "distribution": "RMAT scales 16-22, A~U[0.45,0.65], D=0.05, "
                                         "B=C=(1-A-D)/2, ef 16, 64 roots per graph, hub numbering"})

@@ -285,10 +285,10 @@ bd_status bd_msbfs_destroy(bd_msbfs *b);
  * |logit gap| < margin, and always when no policy is installed. */
 #define BD_POLICY_PARAMS 1410
 #define BD_POLICY_FEATURES 8
-/* Installs (or, with params == NULL, removes) the policy used by
- * BD_ALG_LEARNED.  lo / hi (8 floats each, may be NULL for no limit) bound
- * the raw features the policy is trusted on; outside them the Beamer rule
- * decides.  Host pointers; copied. */
+/* Installs (or, with params == NULL or margin == +inf, removes) the policy
+ * used by BD_ALG_LEARNED.  lo / hi (8 floats each, may be NULL for no limit)
+ * bound the raw features the policy is trusted on; outside them the Beamer
+ * rule decides.  Host pointers; copied. */
 bd_status bd_bfs_set_policy(bd_bfs *b, const float *params, const float *mean,
                             const float *inv_std, const float *lo, const float *hi,
                             float margin);
