@@ -59,7 +59,7 @@ struct MsAcc {
     ull large_packed;
     ull done_degsum; // degree sum of vertices that just got every lane
     ull t_end;       // max over CTAs of their arrival time
-    ull pad;
+    ull work;        // pull steps: next bitmap word to hand out
 };
 
 // State between steps: written first by the init kernel, then kept by every
@@ -544,26 +544,32 @@ template <int BLOCK>
 __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
 {
     const int lane = lane_id();
-    const int warp = threadIdx.x >> 5;
-    const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
-    const long long nw = (long long)gridDim.x * (BLOCK / 32);
     const int cur = sv.step % 3, nxt = (sv.step + 1) % 3;
     MsAcc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
     const long long words = (p.n + 31) / 32;
-    // Warp gw owns words gw, gw + nw, gw + 2 nw, ...; it loads 32 of their
-    // skip masks at once (one per lane) and walks only the words with work.
-    // Done vertices outside the frontier have nothing to do (frontier ones
-    // still fold their frontier lanes into seen below).
-    for (long long t0 = 0; gw + t0 * nw < words; t0 += 32) {
-        const long long wl = gw + (t0 + lane) * nw;
+    // Warps take chunks of 32 bitmap words from a counter of the step (work
+    // per word varies widely: dynamic hand-out keeps the warps of a CTA
+    // finishing together).  Chunk c holds words c, c + C, c + 2C, ... (C
+    // chunks in all), so the heavy low-numbered words of a hub layout are
+    // spread over all chunks.  A warp loads its chunk's 32 skip masks at once
+    // (one per lane) and walks only the words with work.  Done vertices
+    // outside the frontier have nothing to do (frontier ones still fold
+    // their frontier lanes into seen below).
+    const long long chunks = (words + 31) / 32;
+    for (;;) {
+        ull c = 0;
+        if (lane == 0) { c = atomicAdd(&acc->work, 1ull); }
+        c = __shfl_sync(kFullMask, c, 0);
+        if ((long long)c >= chunks) { break; }
+        const long long wl = (long long)c + lane * chunks;
         const uint32_t sk =
             wl < words ? (__ldcg(&p.done[wl]) & ~__ldcg(&p.fb[cur][wl])) : kFullMask;
         unsigned todo = __ballot_sync(kFullMask, sk != kFullMask);
         while (todo) {
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
-            const long long w = gw + (t0 + src) * nw;
+            const long long w = (long long)c + src * chunks;
             const uint32_t skip = __shfl_sync(kFullMask, sk, src);
             const uint32_t v = (uint32_t)(w * 32 + lane);
             const bool live = !((skip >> lane) & 1u);
@@ -774,7 +780,7 @@ __device__ void ms_end_step(const MsParams &p, const MsView &sv, MsShared<BLOCK>
         if (blockIdx.x == 0) {
             MsAcc *z = &c->acc[(s + 1) % 3];
             z->vertices = z->degsum = z->lanes = z->small_cnt = z->large_packed = 0;
-            z->done_degsum = z->t_end = 0;
+            z->done_degsum = z->t_end = z->work = 0;
         }
         atomicMax(&acc->t_end, (ull)globaltimer());
         red_release_add64(&c->bar, 1ull);
