@@ -327,17 +327,22 @@ __device__ __forceinline__ void push_arcs(const MsParams &p, MsAcc *acc, int cur
     uint32_t dn[kPushU];
 #pragma unroll
     for (int i = 0; i < kPushU; ++i) { dn[i] = in[i] ? __ldcg(&p.done[v[i] >> 5]) : ~0u; }
-    ull vis[kPushU];
+    // lanes v already has (seen, current frontier) or was already given in
+    // this step (a plain read of its next word: hot targets of many pushers
+    // then skip the atomic; a stale read only costs an atomic that changes
+    // nothing)
+    ull vis[kPushU], nxt_seen[kPushU];
 #pragma unroll
     for (int i = 0; i < kPushU; ++i) {
         const bool open = in[i] && !((dn[i] >> (v[i] & 31)) & 1u);
         vis[i] = open ? (__ldcg(&p.seen[v[i]]) | frontier_word(p, cur, v[i])) : ~0ull;
+        nxt_seen[i] = open ? __ldcg(&p.F[nxt][v[i]]) : ~0ull;
     }
     ull old[kPushU], give[kPushU];
 #pragma unroll
     for (int i = 0; i < kPushU; ++i) {
         give[i] = bits[i] & ~vis[i];
-        old[i] = give[i] ? atomicOr(&p.F[nxt][v[i]], give[i]) : ~0ull;
+        old[i] = (give[i] & ~nxt_seen[i]) ? atomicOr(&p.F[nxt][v[i]], give[i]) : ~0ull;
     }
     bool first[kPushU];
     int64_t deg[kPushU];
