@@ -695,12 +695,15 @@ struct MsShared {
 };
 
 // The rule: pull once the frontier's edges are a sizeable share of the edges
-// still able to deliver a lane (Beamer's alpha test over the batch).
+// still able to deliver a lane (Beamer's alpha test over the batch) ...
 __device__ int ms_rule(const MsState &c, const MsParams &p)
 {
     if (c.f_count == 0) { return kMsDone; }
     if (p.force_dir >= 0) { return p.force_dir; }
-    return (c.f_degsum * p.alpha > c.arcs_left) ? kPull : kPush;
+    // ... and only once the frontier holds at least n / 1024 vertices: a
+    // pull step sweeps the done bitmap, which a handful of frontier
+    // vertices pushing their arcs does not pay for
+    return (c.f_degsum * p.alpha > c.arcs_left && c.f_count * 1024 >= p.n) ? kPull : kPush;
 }
 
 // Advances the state over the step that just ended.  One thread per CTA;
@@ -861,6 +864,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) msbfs_kernel(MsParams p)
         }
         ms_end_step<BLOCK>(p, sv, sh, loc);
     }
+    // Leave the frontier buffers zero for the next group or call: the only
+    // words still set are those of the last frontier read (the queues of
+    // step - 1); after an error the host clears them instead.
+    if (__ldcg(&c->error) == 0) { ms_clear_old(p, ms_view(sh.st)); }
     if (blockIdx.x == 0 && threadIdx.x == 0) { c->st = sh.st; }
 }
 
@@ -868,7 +875,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) msbfs_kernel(MsParams p)
 __global__ void ms_init_kernel(MsParams p, const int64_t *sources, int count)
 {
     MsCtrl *c = p.ctrl;
+    const int error = c->error;  // an earlier group's, reported for the call
     memset(c, 0, sizeof(MsCtrl));
+    c->error = error;
     long long nsmall = 0, nf = 0, degsum = 0, done = 0;
     ull lp = 0;
     for (int r = 0; r < count; ++r) {
@@ -1046,6 +1055,7 @@ struct bd_msbfs {
     cudaGraphExec_t graph = nullptr;
     int graph_count = -1;
     bool graph_ok = true;
+    bool frontier_clean = false;  // F and fb are all zero (kernels leave them so)
     MsCtrl last{};
     std::vector<unsigned long long> counts;
 };
@@ -1114,10 +1124,6 @@ bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
     BD_CUDA(cudaMemsetAsync(b->drec_cnt + group * n, 0, sizeof(uint32_t) * n, b->stream));
     BD_CUDA(cudaMemcpyAsync(b->done, traversal_isolated(b->g), sizeof(uint32_t) * ((n + 31) / 32),
                             cudaMemcpyDeviceToDevice, b->stream));
-    for (int i = 0; i < 3; ++i) {
-        BD_CUDA(cudaMemsetAsync(b->F[i], 0, sizeof(ull) * n, b->stream));
-        BD_CUDA(cudaMemsetAsync(b->fb[i], 0, sizeof(uint32_t) * ((n + 31) / 32), b->stream));
-    }
     MsParams p = ms_params(b, group, count);
     ms_init_kernel<<<1, 1, 0, b->stream>>>(p, b->d_sources + group * 64, count);
     BD_CUDA(cudaGetLastError());
@@ -1133,6 +1139,7 @@ bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
 
 bd_status ms_enqueue_all(bd_msbfs *b, int count)
 {
+    BD_CUDA(cudaMemsetAsync(&b->ctrl->error, 0, sizeof(int), b->stream));
     for (int gi = 0; gi * 64 < count; ++gi) {
         BD_TRY(ms_enqueue_group(b, gi, std::min(64, count - gi * 64)));
     }
@@ -1143,6 +1150,16 @@ bd_status ms_enqueue_all(bd_msbfs *b, int count)
 // count); falls back to plain stream launches if capture is refused.
 bd_status ms_launch(bd_msbfs *b, int count)
 {
+    // The kernels leave F and fb zero; after a first use or an error, zero
+    // them here (outside any captured graph).
+    if (!b->frontier_clean) {
+        const int64_t n = b->g->n;
+        for (int i = 0; i < 3; ++i) {
+            BD_CUDA(cudaMemsetAsync(b->F[i], 0, sizeof(ull) * n, b->stream));
+            BD_CUDA(cudaMemsetAsync(b->fb[i], 0, sizeof(uint32_t) * ((n + 31) / 32), b->stream));
+        }
+    }
+    b->frontier_clean = false;  // until this call is known to have finished cleanly
     if (b->opts.use_graph && b->graph_ok) {
         if (b->graph_count != count) {
             if (b->graph) {
@@ -1369,6 +1386,7 @@ bd_status bd_msbfs_run(bd_msbfs *b, const int64_t *sources, int32_t count, bd_ru
     b->count = count;
     b->sources.assign(sources, sources + count);
     b->ran = true;
+    b->frontier_clean = b->last.error == 0;
     if (b->last.error) { return (bd_status)b->last.error; }
     if (stats) {
         float ms = 0.f;
