@@ -177,11 +177,15 @@ def measure_tables_batched(graph: "bd.Graph", roots, repeats: int = 1, alpha: in
 
 
 def alpha_dirs(tab: LevelTable, alpha=4) -> str:
-    """The batched traversal's rule over a level table: pull when the
-    frontier's degree sum times alpha exceeds the unexplored degree sum."""
+    """The batched traversal's rule over a level table (ms_rule in
+    bd_msbfs.cu): pull when the frontier's degree sum times alpha exceeds
+    the unexplored degree sum and the frontier holds at least n / 1024
+    vertices."""
     out = []
     for lv in range(tab.levels):
-        out.append("B" if tab.frontier_edges[lv] * alpha > tab.unexplored[lv] else "T")
+        pull = (tab.frontier_edges[lv] * alpha > tab.unexplored[lv]
+                and tab.frontier[lv] * 1024 >= tab.n)
+        out.append("B" if pull else "T")
     return "".join(out)
 
 
@@ -342,10 +346,17 @@ def fit(X, y, w, epochs=3000, lr=3e-3, weight_decay=1e-4, seed=0, widen=3.0):
     return pol, hist
 
 
+# raw features that measure the graph's size (log2 n, log2 m): the network is
+# never trusted on a graph larger than every graph it was trained on
+SIZE_FEATURES = (4, 5)
+
+
 def set_widen(pol: Policy, widen: float) -> None:
     xmin, xmax, std = pol.extremes
     pol.lo = (xmin - widen * std).astype(np.float32)
     pol.hi = (xmax + widen * std).astype(np.float32)
+    for i in SIZE_FEATURES:
+        pol.hi[i] = xmax[i]
 
 
 WIDEN_CANDIDATES = (0.0, 0.5, 1.0, 2.0, 3.0)
