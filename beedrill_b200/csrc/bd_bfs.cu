@@ -330,29 +330,24 @@ __device__ void bu_step(const BfsParams &p, const StepView &sv, Local &loc)
 {
     constexpr int P = K >= 4 ? 2 : 4;
     const int lane = lane_id();
+    const int warp = threadIdx.x >> 5;
+    const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
+    const long long nw = (long long)gridDim.x * (BLOCK / 32);
     const uint32_t *vin = p.vis[sv.vis_cur];
     uint32_t *vout = p.vis[sv.vis_cur ^ 1];
     const int qout = sv.q_cur ^ 1;
     Acc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
 
-    // Warps take chunks of 32 / K groups of K words from a counter of the
-    // step; chunk c holds groups c, c + C, c + 2C, ... (C chunks in all), so
-    // the heavy low-numbered words of a hub layout are spread over all
-    // chunks.  A warp loads its chunk at once (one word per lane), passes
-    // full groups through, and works only on the groups with unvisited
-    // vertices: late levels, where most words are full, cost a bitmap sweep.
+    // Warp gw owns groups gw, gw + nw, gw + 2 nw, ... of K words.  It loads
+    // 32 / K of its groups at once (one word per lane), passes full groups
+    // through, and works only on the groups with unvisited vertices: late
+    // levels, where most words are full, cost a bitmap sweep.
     constexpr int GPB = 32 / K;
     constexpr unsigned kGroupMask = (1u << K) - 1u;
-    const long long ngroups = (p.words + K - 1) / K;
-    const long long chunks = (ngroups + GPB - 1) / GPB;
-    for (;;) {
-        unsigned long long c = 0;
-        if (lane == 0) { c = atomicAdd(&acc->work, 1ull); }
-        c = __shfl_sync(kFull, c, 0);
-        if ((long long)c >= chunks) { break; }
+    for (long long t0 = 0; (gw + t0 * nw) * K < p.words; t0 += GPB) {
         const int j = lane / K;
-        const long long wl = ((long long)c + j * chunks) * K + lane % K;
+        const long long wl = (gw + (t0 + j) * nw) * K + lane % K;
         const uint32_t mw = wl < p.words ? __ldcg(&vin[wl]) : kFull;
         const unsigned openm = __ballot_sync(kFull, mw != kFull);
         if (!((openm >> (j * K)) & kGroupMask) && wl < p.words) { vout[wl] = kFull; }
@@ -364,7 +359,7 @@ __device__ void bu_step(const BfsParams &p, const StepView &sv, Local &loc)
         while (groups) {
             const int g = __ffs(groups) - 1;
             groups &= groups - 1;
-            const long long w0 = ((long long)c + g * chunks) * K;
+            const long long w0 = (gw + (t0 + g) * nw) * K;
             uint32_t word[K];
 #pragma unroll
             for (int k = 0; k < K; ++k) { word[k] = __shfl_sync(kFull, mw, g * K + k); }
@@ -474,21 +469,17 @@ __device__ void bu_step_lanes(const BfsParams &p, const StepView &sv, Local &loc
 {
     constexpr int P = 4;
     const int lane = lane_id();
+    const int warp = threadIdx.x >> 5;
+    const long long gw = (long long)blockIdx.x * (BLOCK / 32) + warp;
+    const long long nw = (long long)gridDim.x * (BLOCK / 32);
     const uint32_t *vin = p.vis[sv.vis_cur];
     uint32_t *vout = p.vis[sv.vis_cur ^ 1];
     const int qout = sv.q_cur ^ 1;
     Acc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
 
-    // Chunks of 32 words from a counter of the step, interleaved: chunk c
-    // holds words c, c + C, c + 2C, ... (C chunks); each lane owns one word.
-    const long long chunks = (p.words + 31) / 32;
-    for (;;) {
-        unsigned long long c = 0;
-        if (lane == 0) { c = atomicAdd(&acc->work, 1ull); }
-        c = __shfl_sync(kFull, c, 0);
-        if ((long long)c >= chunks) { break; }
-        const long long w = (long long)c + lane * chunks;
+    for (long long base = gw * 32; base < p.words; base += nw * 32) {
+        const long long w = base + lane;
         const bool mine = w < p.words;
         const uint32_t word = mine ? __ldcg(&vin[w]) : kFull;
         uint32_t todo = ~word;     // unvisited vertices of this lane's word
@@ -767,7 +758,7 @@ __device__ void end_step(const BfsParams &p, const StepView &sv, SharedState<BLO
         if (td) { atomicAdd(&acc->degsum, td); }
         if (blockIdx.x == 0) {
             Acc *z = &c->acc[(s + 1) % 3];
-            z->found = z->degsum = z->small_cnt = z->large_packed = z->t_end = z->work = 0;
+            z->found = z->degsum = z->small_cnt = z->large_packed = z->t_end = 0;
         }
         atomicMax(&acc->t_end, (unsigned long long)globaltimer());
         red_release_add64(&c->bar, 1ull);

@@ -37,8 +37,7 @@ struct Acc {
     unsigned long long small_cnt;
     unsigned long long large_packed;
     unsigned long long t_end;  // max over CTAs of their arrival time
-    unsigned long long work;   // bottom-up steps: next chunk of bitmap words to hand out
-    unsigned long long pad[2];
+    unsigned long long pad[3];
 };
 
 // The traversal state between steps.  The init kernel writes the first one

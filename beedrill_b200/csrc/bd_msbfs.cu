@@ -545,6 +545,17 @@ __device__ void ms_pull_heavy(const MsParams &p, const MsView &sv, MsLocal &loc)
     }
 }
 
+// The next chunk of a step's work for the calling warp: its own first
+// (index gw, no atomic), then, when there are more chunks than warps, from
+// the step's counter as chunk nw + k.
+__device__ __forceinline__ ull ms_next_chunk(ull *counter, long long nw, long long chunks)
+{
+    if (chunks <= nw) { return (ull)chunks; }
+    ull x = 0;
+    if (lane_id() == 0) { x = atomicAdd(counter, 1ull); }
+    return (ull)nw + __shfl_sync(kFullMask, x, 0);
+}
+
 template <int BLOCK>
 __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
 {
@@ -553,28 +564,33 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
     MsAcc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
     const long long words = (p.n + 31) / 32;
-    // Warps take chunks of 32 bitmap words from a counter of the step (work
-    // per word varies widely: dynamic hand-out keeps the warps of a CTA
-    // finishing together).  Chunk c holds words c, c + C, c + 2C, ... (C
-    // chunks in all), so the heavy low-numbered words of a hub layout are
-    // spread over all chunks.  A warp loads its chunk's 32 skip masks at once
-    // (one per lane) and walks only the words with work.  Done vertices
-    // outside the frontier have nothing to do (frontier ones still fold
-    // their frontier lanes into seen below).
+    // Which words a warp walks.  Large graphs (at least two 32-word chunks
+    // per warp): chunks handed out dynamically -- the warp's own first, then
+    // from a counter of the step -- because work per word varies widely and
+    // dynamic hand-out keeps the warps of a CTA finishing together; chunk c
+    // holds words c, c + C, c + 2C, ... (C chunks), so the heavy
+    // low-numbered words of a hub layout are spread over all chunks.
+    // Smaller graphs: warp gw owns words gw, gw + nw, gw + 2 nw, ... (a
+    // chunk per warp would leave most warps idle).  Either way a warp loads
+    // 32 skip masks at once (one per lane) and walks only the words with
+    // work.  Done vertices outside the frontier have nothing to do (frontier
+    // ones still fold their frontier lanes into seen below).
+    const long long gw = (long long)blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5);
+    const long long nw = (long long)gridDim.x * (BLOCK / 32);
     const long long chunks = (words + 31) / 32;
-    for (;;) {
-        ull c = 0;
-        if (lane == 0) { c = atomicAdd(&acc->work, 1ull); }
-        c = __shfl_sync(kFullMask, c, 0);
-        if ((long long)c >= chunks) { break; }
-        const long long wl = (long long)c + lane * chunks;
+    const bool dynamic = chunks >= 2 * nw;
+    const long long stride = dynamic ? chunks : nw;
+    const long long limit = dynamic ? chunks : words;
+    for (long long base = gw; base < limit;
+         base = dynamic ? (long long)ms_next_chunk(&acc->work, nw, chunks) : base + 32 * nw) {
+        const long long wl = base + lane * stride;
         const uint32_t sk =
             wl < words ? (__ldcg(&p.done[wl]) & ~__ldcg(&p.fb[cur][wl])) : kFullMask;
         unsigned todo = __ballot_sync(kFullMask, sk != kFullMask);
         while (todo) {
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
-            const long long w = (long long)c + src * chunks;
+            const long long w = base + src * stride;
             const uint32_t skip = __shfl_sync(kFullMask, sk, src);
             const uint32_t v = (uint32_t)(w * 32 + lane);
             const bool live = !((skip >> lane) & 1u);
