@@ -100,14 +100,23 @@ _lib = None
 TUNING_PATH = os.path.join(HERE, "tuning", "b200.json")
 
 
-def tuned_options(kind: str) -> dict:
+def tuned_options(kind: str, num_vertices: int | None = None) -> dict:
     """Launch parameters picked by beedrill_b200.autotune for `kind`
-    ("single" or "batched"), or {} when no tuning file exists."""
+    ("single" or "batched"): those tuned at the scale nearest to
+    log2(num_vertices) when the file holds several, else the default entry;
+    {} when no tuning file exists."""
     if not os.path.exists(TUNING_PATH):
         return {}
     import json
+    import math
     with open(TUNING_PATH) as f:
-        return dict(json.load(f).get(kind, {}))
+        d = json.load(f)
+    by_scale = d.get("by_scale") or {}
+    if num_vertices and by_scale:
+        scale = math.log2(max(num_vertices, 2))
+        key = min(by_scale, key=lambda k: (abs(int(k) - scale), -int(k)))
+        return dict(by_scale[key].get(kind, {}))
+    return dict(d.get(kind, {}))
 
 
 def lib() -> ctypes.CDLL:
@@ -336,7 +345,7 @@ class HybridBFS:
         if alg not in ALGORITHMS:
             raise ValueError(f"Algorithm '{alg}' not implemented!")
         if tuned:
-            t = tuned_options("single")
+            t = tuned_options("single", graph.num_vertices())
             block_size = block_size or t.get("block_size", 0)
             large_degree = large_degree or t.get("large_degree", 0)
             chunk_edges = chunk_edges or t.get("chunk_edges", 0)
@@ -490,7 +499,7 @@ class BatchedBFS:
                  chunk_edges: int = 0, pull_prefix: int = 0, spin_limit: int = 0,
                  heavy_degree: int = 0, heavy_chunk: int = 0, tuned: bool = True):
         if tuned:
-            t = tuned_options("batched")
+            t = tuned_options("batched", graph.num_vertices())
             alpha = alpha or t.get("alpha", 0)
             block_size = block_size or t.get("block_size", 0)
             large_degree = large_degree or t.get("large_degree", 0)

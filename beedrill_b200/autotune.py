@@ -17,6 +17,7 @@ from the benchmark graph's.  Results go to a JSON file that
 beedrill_b200.tuned_options() reads:
 
     python -m beedrill_b200.autotune --scale 24 --seed 1024 --out beedrill_b200/tuning/b200.json
+    python -m beedrill_b200.autotune --scale 20 --merge --out beedrill_b200/tuning/b200.json
 """
 from __future__ import annotations
 
@@ -139,12 +140,29 @@ def main(argv=None):
                     help="graph seed (the benchmark's graph uses another)")
     ap.add_argument("--out", default=DEFAULT_PATH)
     ap.add_argument("--order", type=int, default=bd.ORDER_HUB)
+    ap.add_argument("--merge", action="store_true",
+                    help="add this scale's entry to an existing tuning file")
     args = ap.parse_args(argv)
     log = lambda s: print(f"[autotune] {s}", flush=True)  # noqa: E731
     res = tune(args.scale, args.roots, seed=args.seed, order=args.order, log=log)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+    # One entry per tuned scale (handles use the one nearest their graph);
+    # the top-level entry is the largest scale tuned so far.
+    data = {}
+    if args.merge and os.path.exists(args.out):
+        with open(args.out) as f:
+            data = json.load(f)
+    keys = ("single", "batched", "single_gteps", "batched_gteps", "graph", "when")
+    by_scale = data.get("by_scale", {})
+    if not by_scale and "graph" in data:  # a file with one entry
+        by_scale[str(data["graph"]["scale"])] = {k: data[k] for k in keys if k in data}
+    by_scale[str(args.scale)] = {k: res[k] for k in keys}
+    top = max(by_scale, key=int)
+    data.update({k: v for k, v in res.items() if k != "tables"} if args.scale >= int(top) else {})
+    data["by_scale"] = by_scale
+    data.setdefault("tables", {})[str(args.scale)] = res["tables"]
     with open(args.out, "w") as f:
-        json.dump(res, f, indent=1)
+        json.dump(data, f, indent=1)
         f.write("\n")
     log(f"single {res['single']} {res['single_gteps']:.2f} GTEPS; "
         f"batched {res['batched']} {res['batched_gteps']:.2f} GTEPS -> {args.out}")

@@ -142,7 +142,7 @@ def measure_tables(graph: "bd.Graph", roots, repeats: int = 1, with_beamer: bool
     return tables
 
 
-def measure_tables_batched(graph: "bd.Graph", roots, repeats: int = 1, alpha: int = 4):
+def measure_tables_batched(graph: "bd.Graph", roots, repeats: int = 1, alpha: int | None = None):
     """Forced push and forced pull runs of one batch of up to 64 roots; one
     LevelTable whose top-down / bottom-up columns hold push / pull times,
     `found` counts new (vertex, root) pairs and `unexplored` is the degree
@@ -162,6 +162,8 @@ def measure_tables_batched(graph: "bd.Graph", roots, repeats: int = 1, alpha: in
     a, b = runs["push"], runs["pull"]
     if len(a) != len(b) or any(x["found"] != y["found"] for x, y in zip(a, b)):
         raise RuntimeError("forced batched runs disagree on the level structure")
+    if alpha is None:  # the rule a batched handle on this graph uses
+        alpha = bd.tuned_options("batched", n).get("alpha", 4)
     rule = bd.BatchedBFS(graph, len(roots), alpha=alpha)
     st = rule.run(roots)
     tab = LevelTable(
@@ -176,11 +178,14 @@ def measure_tables_batched(graph: "bd.Graph", roots, repeats: int = 1, alpha: in
     return tab
 
 
-def alpha_dirs(tab: LevelTable, alpha=4) -> str:
+def alpha_dirs(tab: LevelTable, alpha=None) -> str:
     """The batched traversal's rule over a level table (ms_rule in
     bd_msbfs.cu): pull when the frontier's degree sum times alpha exceeds
     the unexplored degree sum and the frontier holds at least n / 1024
-    vertices."""
+    vertices.  alpha defaults to the tuned value a batched handle on a
+    graph of that size uses."""
+    if alpha is None:
+        alpha = bd.tuned_options("batched", tab.n).get("alpha", 4)
     out = []
     for lv in range(tab.levels):
         pull = (tab.frontier_edges[lv] * alpha > tab.unexplored[lv]
