@@ -204,6 +204,9 @@ WORKLOADS = {
     "rmat20-256": {"kind": "rmat", "scale": 20, "roots": 256},
     # the largest single-GPU case
     "rmat26": {"kind": "rmat", "scale": 26, "roots": 64},
+    # graphs inside the learned policies' training range (scales 16-18),
+    # seeds the trainer never used: 64-root batches, learned vs rule
+    "policy16-18": {"kind": "policy_set", "scales": (16, 17, 18), "seeds": (7001, 7002, 7003)},
     # high-diameter contrast: 4096 x 4096 grid, 1% of its edges deleted
     "grid4096": {"kind": "grid", "rows": 4096, "cols": 4096, "delete": 0.01, "roots": 64},
     # 512 independent RMAT graphs (scales 10-18, edge factors 4-32), one root each
@@ -307,6 +310,67 @@ def bench_packed(args, w, bd, order, local):
     return 0
 
 
+def bench_policy_set(args, w, bd, order, local):
+    """Held-out graphs of the learned policies' training range (RMAT A=.57
+    B=C=.19 D=.05, edge factor 16, graph seeds the trainer never used), one
+    64-root batch each, with the learned push/pull policy ("batched") and
+    with the rule alone ("batched_rule").  GTEPS = sum of m_c over all
+    roots of all graphs / sum of the batch times."""
+    from beedrill_b200 import policy as P
+    import torch
+    flush_buf = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def flush_l2():  # > the 126 MB L2, before each batch
+        flush_buf.fill_(1)
+        torch.cuda.synchronize(local)
+
+    pol = P.Policy.load(P.BATCHED_PATH)
+    graphs = []
+    for scale in w["scales"]:
+        for seed in w["seeds"]:
+            g = bd.Graph.rmat(scale, EDGE_FACTOR, 0.57, 0.19, 0.19, 0.05, seed + 10 * scale,
+                              order=order)
+            learned, rule = bd.BatchedBFS(g, 64), bd.BatchedBFS(g, 64)
+            pol.install(learned)
+            graphs.append((g, g.pick_roots(seed, 64), learned, rule))
+    totals = {"batched": [0.0, 0], "batched_rule": [0.0, 0]}
+    dirs = {}
+    with ClockSampler(local) as clocks:
+        for step in range(args.warmup + args.steps):
+            for g, roots, learned, rule in graphs:
+                for name, h in (("batched", learned), ("batched_rule", rule)):
+                    flush_l2()
+                    st = h.run(roots)
+                    if step >= args.warmup:
+                        totals[name][0] += st.ms
+                        totals[name][1] += int(h.counts()[0].sum())
+                        dirs.setdefault(name, []).append(h.directions())
+    modes = {k: {"gteps": e / (ms * 1e-3) / 1e9, "ms_per_step": ms / args.steps}
+             for k, (ms, e) in totals.items()}
+    line = {
+        "metric": "aggregate GTEPS, 64-root batches on 9 held-out RMAT graphs (scales 16-18), "
+                  "learned push/pull policy vs rule, 1 B200",
+        "value": modes["batched"]["gteps"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": modes["batched"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "scales": list(w["scales"]),
+                   "graph_seeds": [s + 10 * sc for sc in w["scales"] for s in w["seeds"]],
+                   "roots": 64, "adjacency_order": args.order,
+                   "l2": "L2 flushed (512 MB write) before each batch", "parallelism": "1 GPU"},
+        "modes": modes,
+        "directions": {k: sorted(set(v)) for k, v in dirs.items()},
+        "gpu_launches": args.steps * 2 * len(graphs) * 3,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    for g, _, learned, rule in graphs:
+        learned.close()
+        rule.close()
+        g.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -343,6 +407,10 @@ def main():
         if world > 1:
             raise SystemExit("packed512 runs on one GPU")
         return bench_packed(args, w, bd, order, local)
+    if w["kind"] == "policy_set":
+        if world > 1:
+            raise SystemExit("policy16-18 runs on one GPU")
+        return bench_policy_set(args, w, bd, order, local)
     num_roots = w["roots"]
     t_gen = time.time()
     if w["kind"] == "rmat":
