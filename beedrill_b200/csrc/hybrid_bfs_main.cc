@@ -20,6 +20,9 @@
 //                      first (results are unchanged)
 //   --hub_layout       --degree_order, and the traversal runs on vertices
 //                      renumbered by degree (results in the file's ids)
+//   --tuning_file F    launch parameters from the autotuner (default:
+//                      ../tuning/b200.json beside this binary's directory,
+//                      when present)
 // Algorithms: the reference's four names plus top_down, bottom_up, learned.
 #include <getopt.h>
 #include <unistd.h>
@@ -61,6 +64,7 @@ const struct option long_options[] = {
     {"batched", no_argument, nullptr, 0},
     {"degree_order", no_argument, nullptr, 0},
     {"hub_layout", no_argument, nullptr, 0},
+    {"tuning_file", required_argument, nullptr, 0},
     {nullptr, 0, nullptr, 0},
 };
 
@@ -91,6 +95,7 @@ void print_help(const char *argv0)
     printf("\t--batched            Run all trials' roots together (64 per group)\n");
     printf("\t--degree_order       Order neighbour lists by neighbour degree\n");
     printf("\t--hub_layout         Traverse with vertices renumbered by degree\n");
+    printf("\t--tuning_file FILE   Launch parameters from the autotuner\n");
     printf("\t--version            Print version info\n");
     printf("\t--help               Print command line help\n");
 }
@@ -117,6 +122,7 @@ struct bfs_args {
     bool batched = false;
     bool degree_order = false;
     bool hub_layout = false;
+    const char *tuning_file = nullptr;
 };
 
 bfs_args parse(int argc, char **argv)
@@ -153,6 +159,7 @@ bfs_args parse(int argc, char **argv)
         else if (name == "batched") { a.batched = true; }
         else if (name == "degree_order") { a.degree_order = true; }
         else if (name == "hub_layout") { a.hub_layout = true; }
+        else if (name == "tuning_file") { a.tuning_file = optarg; }
         else if (name == "version") {
             printf("%s\n", bd_version());
             exit(0);
@@ -183,19 +190,36 @@ int alg_code(const char *name)
     return -1;
 }
 
-// The trained policy beside this binary (beedrill_b200/bin -> beedrill_b200/policy).
-std::string default_policy(bool batched)
+// Directory of this binary (beedrill_b200/bin).
+std::string binary_dir()
 {
     char exe[4096];
     const ssize_t len = readlink("/proc/self/exe", exe, sizeof(exe) - 1);
-    std::string dir = ".";
-    if (len > 0) {
-        exe[len] = '\0';
-        dir = exe;
-        const size_t slash = dir.rfind('/');
-        dir = slash == std::string::npos ? "." : dir.substr(0, slash);
+    if (len <= 0) { return "."; }
+    exe[len] = '\0';
+    std::string dir = exe;
+    const size_t slash = dir.rfind('/');
+    return slash == std::string::npos ? "." : dir.substr(0, slash);
+}
+
+// The autotuner's launch parameters for a graph of n vertices, if any.
+bool find_tuning(const bfs_args &args, long n, beedrill::tuning *t)
+{
+    const std::string path =
+        args.tuning_file ? args.tuning_file : binary_dir() + "/../tuning/b200.json";
+    if (access(path.c_str(), R_OK) != 0) {
+        if (args.tuning_file) { throw beedrill::error(BD_ERR_IO, "tuning file " + path); }
+        return false;
     }
-    return dir + (batched ? "/../policy/learned_policy_batched.json" : "/../policy/learned_policy.json");
+    *t = beedrill::load_tuning(path, n);
+    return true;
+}
+
+// The trained policy beside this binary (beedrill_b200/bin -> beedrill_b200/policy).
+std::string default_policy(bool batched)
+{
+    return binary_dir() +
+           (batched ? "/../policy/learned_policy_batched.json" : "/../policy/learned_policy.json");
 }
 
 // Loads the policy for --algorithm learned; without a file the rule decides.
@@ -237,6 +261,8 @@ bool run_batched(const bfs_args &args, beedrill::graph &g, int alg, const std::v
     bool success = true;
     bd_msbfs_opts opts;
     bd_msbfs_default_opts(&opts);
+    beedrill::tuning tn;
+    if (find_tuning(args, g.num_vertices(), &tn)) { tn.apply(&opts); }
     if (alg == BD_ALG_TOP_DOWN) { opts.force_dir = 0; }
     if (alg == BD_ALG_BOTTOM_UP) { opts.force_dir = 1; }
     beedrill::batched_bfs bfs(g, (int32_t)roots.size(), &opts);
@@ -325,6 +351,8 @@ int main(int argc, char **argv)
         opts.alpha = args.alpha;
         opts.beta = args.beta;
         opts.min_parent = args.min_parent ? 1 : 0;
+        beedrill::tuning tn;
+        if (find_tuning(args, g.num_vertices(), &tn)) { tn.apply(&opts); }
         beedrill::hybrid_bfs bfs(g, &opts);
         beedrill::policy pol;
         if (alg == BD_ALG_LEARNED && find_policy(args, &pol)) { bfs.set_policy(pol); }

@@ -9,10 +9,14 @@
 //     only when asked for (depths(), parents(), check(), print_tree()).
 #pragma once
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -93,6 +97,172 @@ inline policy load_policy(const std::string &path)
         throw error(BD_ERR_FORMAT, "policy file " + path);
     }
     return pol;
+}
+
+// Launch parameters chosen by the autotuner (beedrill_b200/autotune.py) for
+// this GPU, read from its JSON file: the entry tuned at the graph scale
+// nearest log2(n).  No counterpart in the reference.
+struct tuning {
+    std::map<std::string, double> single, batched;
+    // Fills the fields an application left at 0 (library default) with the
+    // tuned values; the batched rule's alpha is taken whenever it is tuned.
+    void apply(bd_bfs_opts *o) const
+    {
+        set(single, "block_size", &o->block_size);
+        set(single, "large_degree", &o->large_degree);
+        set(single, "chunk_edges", &o->chunk_edges);
+        set(single, "bu_prefix", &o->bu_prefix);
+        set(single, "bu_words", &o->bu_words);
+        set(single, "bu_sparse_words", &o->bu_sparse_words);
+    }
+    void apply(bd_msbfs_opts *o) const
+    {
+        auto a = batched.find("alpha");
+        if (a != batched.end()) { o->alpha = (int64_t)a->second; }
+        set(batched, "block_size", &o->block_size);
+        set(batched, "large_degree", &o->large_degree);
+        set(batched, "chunk_edges", &o->chunk_edges);
+        set(batched, "pull_prefix", &o->pull_prefix);
+        set(batched, "heavy_degree", &o->heavy_degree);
+        set(batched, "heavy_chunk", &o->heavy_chunk);
+    }
+
+private:
+    static void set(const std::map<std::string, double> &m, const char *k, int32_t *f)
+    {
+        auto it = m.find(k);
+        if (it != m.end() && *f == 0) { *f = (int32_t)it->second; }
+    }
+};
+
+namespace detail {
+// A small JSON reader for the tuning file (objects, arrays, numbers,
+// strings, true / false / null).
+struct jvalue {
+    enum kind_t { NUL, NUM, STR, ARR, OBJ, BOOL } kind = NUL;
+    double num = 0;
+    std::string str;
+    std::vector<jvalue> arr;
+    std::vector<std::pair<std::string, jvalue>> obj;
+    const jvalue *get(const std::string &k) const
+    {
+        for (const auto &kv : obj) {
+            if (kv.first == k) { return &kv.second; }
+        }
+        return nullptr;
+    }
+};
+
+struct jparser {
+    const char *p;
+    void ws()
+    {
+        while (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t') { ++p; }
+    }
+    [[noreturn]] void fail() { throw error(BD_ERR_FORMAT, "tuning file"); }
+    std::string string()
+    {
+        if (*p != '"') { fail(); }
+        std::string out;
+        for (++p; *p && *p != '"'; ++p) {
+            if (*p == '\\' && p[1]) { ++p; }
+            out += *p;
+        }
+        if (*p != '"') { fail(); }
+        ++p;
+        return out;
+    }
+    jvalue value()
+    {
+        ws();
+        jvalue v;
+        if (*p == '{') {
+            v.kind = jvalue::OBJ;
+            ++p;
+            ws();
+            while (*p != '}') {
+                ws();
+                std::string k = string();
+                ws();
+                if (*p != ':') { fail(); }
+                ++p;
+                v.obj.emplace_back(k, value());
+                ws();
+                if (*p == ',') { ++p; } else if (*p != '}') { fail(); }
+            }
+            ++p;
+        } else if (*p == '[') {
+            v.kind = jvalue::ARR;
+            ++p;
+            ws();
+            while (*p != ']') {
+                v.arr.push_back(value());
+                ws();
+                if (*p == ',') { ++p; } else if (*p != ']') { fail(); }
+            }
+            ++p;
+        } else if (*p == '"') {
+            v.kind = jvalue::STR;
+            v.str = string();
+        } else if (!strncmp(p, "true", 4) || !strncmp(p, "false", 5)) {
+            v.kind = jvalue::BOOL;
+            v.num = *p == 't';
+            p += *p == 't' ? 4 : 5;
+        } else if (!strncmp(p, "null", 4)) {
+            p += 4;
+        } else {
+            char *end = nullptr;
+            v.num = strtod(p, &end);
+            if (end == p) { fail(); }
+            v.kind = jvalue::NUM;
+            p = end;
+        }
+        return v;
+    }
+};
+
+inline void numbers_of(const jvalue *o, std::map<std::string, double> *out)
+{
+    if (!o || o->kind != jvalue::OBJ) { return; }
+    for (const auto &kv : o->obj) {
+        if (kv.second.kind == jvalue::NUM) { (*out)[kv.first] = kv.second.num; }
+    }
+}
+}  // namespace detail
+
+// Reads the autotuner's file; the entry of the scale nearest log2(n) (ties
+// go to the larger scale), or the file's default entry.
+inline tuning load_tuning(const std::string &path, long num_vertices)
+{
+    FILE *fp = fopen(path.c_str(), "rb");
+    if (!fp) { throw error(BD_ERR_IO, "tuning file " + path); }
+    std::string text;
+    char buf[65536];
+    size_t got;
+    while ((got = fread(buf, 1, sizeof(buf), fp)) > 0) { text.append(buf, got); }
+    fclose(fp);
+    detail::jparser jp{text.c_str()};
+    const detail::jvalue root = jp.value();
+    const detail::jvalue *entry = &root;
+    const detail::jvalue *by = root.get("by_scale");
+    if (by && by->kind == detail::jvalue::OBJ && !by->obj.empty() && num_vertices > 0) {
+        const double scale = std::log2((double)std::max(num_vertices, 2L));
+        double best = 1e300;
+        int best_key = 0;
+        for (const auto &kv : by->obj) {
+            const int key = atoi(kv.first.c_str());
+            const double d = std::fabs(key - scale);
+            if (d < best || (d == best && key > best_key)) {
+                best = d;
+                best_key = key;
+                entry = &kv.second;
+            }
+        }
+    }
+    tuning t;
+    detail::numbers_of(entry->get("single"), &t.single);
+    detail::numbers_of(entry->get("batched"), &t.batched);
+    return t;
 }
 
 // The graph (graph_base.h): a CSR in HBM.

@@ -98,3 +98,37 @@ def test_cpp_facade_reads_the_trained_policies(tmp_path):
         assert abs(float(out[5]) - sum(d["params"])) <= 1e-3 * max(1.0, sum(abs(v) for v in d["params"]))
         assert abs(float(out[6]) - d["inv_std"][3]) <= 1e-6 * abs(d["inv_std"][3])
         assert out[7] == "-3"  # BD_ERR_FORMAT
+
+
+def test_cpp_facade_reads_the_tuning_file(tmp_path):
+    """The C++ facade's reader of the autotuner's file (used by the CLI)
+    picks the same entry, with the same values, as the Python binding."""
+    import subprocess
+    src = tmp_path / "tune.cc"
+    src.write_text(
+        '#include "beedrill/hybrid_bfs.hpp"\n'
+        'int main(int argc, char **argv) {\n'
+        '  beedrill::tuning t = beedrill::load_tuning(argv[1], atol(argv[2]));\n'
+        '  bd_bfs_opts o; memset(&o, 0, sizeof o); t.apply(&o);\n'
+        '  bd_msbfs_opts m; memset(&m, 0, sizeof m); m.alpha = 4; t.apply(&m);\n'
+        '  printf("%d %d %d %d %d %d %lld %d %d %d %d %d %d\\n", o.block_size, o.large_degree,\n'
+        '         o.chunk_edges, o.bu_prefix, o.bu_words, o.bu_sparse_words, (long long)m.alpha,\n'
+        '         m.block_size, m.large_degree, m.chunk_edges, m.pull_prefix, m.heavy_degree,\n'
+        '         m.heavy_chunk);\n'
+        '  return 0; }\n')
+    exe = tmp_path / "tune"
+    lib_dir = os.path.dirname(bd.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", lib_dir, "-lbeedrill_b200", f"-Wl,-rpath,{lib_dir}"], check=True)
+    path = os.path.join(ROOT, "beedrill_b200", "tuning", "b200.json")
+    if not os.path.exists(path):
+        pytest.skip("no tuning file committed")
+    for n in (1 << 16, 1 << 20, 1 << 21, 1 << 23, 1 << 24, 1 << 26):
+        out = [int(x) for x in subprocess.run([str(exe), path, str(n)], check=True,
+                                               stdout=subprocess.PIPE, text=True).stdout.split()]
+        s, b = bd.tuned_options("single", n), bd.tuned_options("batched", n)
+        want = [s.get(k, 0) for k in ("block_size", "large_degree", "chunk_edges", "bu_prefix",
+                                      "bu_words", "bu_sparse_words")] + \
+               [b.get("alpha", 4)] + [b.get(k, 0) for k in ("block_size", "large_degree", "chunk_edges",
+                                                             "pull_prefix", "heavy_degree", "heavy_chunk")]
+        assert out == want, (n, out, want)
