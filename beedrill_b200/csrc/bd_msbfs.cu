@@ -25,9 +25,17 @@
 //   done    uint32[n/32]   vertices every lane has reached, and isolated ones:
 //                          pull steps skip them by the word, push steps
 //                          drop arcs into them before touching seen
-//   depth   int32[n][R]    vertex-major, so a vertex's lanes share sectors
-//   parent  uint32[n][R]   vertex-major; widened to the reference's int64
-//                          encoding when copied out
+//   drec    16 B [n][16]   delivery records of pull steps: {lane mask lo,
+//                          hi, provider, level}, one store for all the
+//                          lanes one neighbour delivered (drec_cnt[n] counts
+//                          them)
+//   depth   int32[n][R]    per-lane rows, vertex-major (a vertex's lanes share
+//   parent  uint32[n][R]   sectors): push deliveries, and pull deliveries
+//                          past a vertex's 16 records; widened to the
+//                          reference's int64 encoding when copied out
+//   fb[3]   uint32[n/32]   bit v set iff F[.][v] != 0
+// The kernel leaves F and fb zero when it ends (it clears the last
+// frontier's words), so a call needs no memsets of them.
 #include <algorithm>
 #include <cstring>
 #include <vector>
