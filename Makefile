@@ -11,7 +11,8 @@ ARCH := -gencode arch=compute_100a,code=sm_100a
 NVFLAGS := -O3 -std=c++17 $(ARCH) -lineinfo -Xcompiler -fPIC -Xcompiler -Wall \
            -Iinclude -Ibeedrill_b200/csrc --expt-relaxed-constexpr
 CSRC := beedrill_b200/csrc
-CU_SRCS := $(CSRC)/bd_common.cu $(CSRC)/bd_graph.cu $(CSRC)/bd_bfs.cu $(CSRC)/bd_policy.cu $(CSRC)/bd_msbfs.cu
+CU_SRCS := $(CSRC)/bd_common.cu $(CSRC)/bd_graph.cu $(CSRC)/bd_bfs.cu $(CSRC)/bd_policy.cu $(CSRC)/bd_msbfs.cu \
+           $(CSRC)/bd_check.cu
 CU_OBJS := $(patsubst $(CSRC)/%.cu,beedrill_b200/_build/%.o,$(CU_SRCS))
 HDRS := include/beedrill_b200.h $(CSRC)/bd_internal.h $(CSRC)/bd_bfs_device.cuh $(CSRC)/bd_device_util.cuh \
         $(CSRC)/bd_policy.cuh

@@ -146,6 +146,7 @@ def lib() -> ctypes.CDLL:
         "bd_graph_copy_edges": (c_int, [c_void_p, i64p, i64p]),
         "bd_graph_write_el64": (c_int, [c_void_p, c_char_p]),
         "bd_graph_check": (c_int, [c_void_p, i32p]),
+        "bd_graph_check_parents": (c_int, [c_void_p, c_int64, i64p, i32p, i64p]),
         "bd_graph_pick_roots": (c_int, [c_void_p, c_uint64, c_int64, i64p]),
         "bd_graph_device_csr": (c_int, [c_void_p, vpp, vpp]),
         "bd_graph_destroy": (c_int, [c_void_p]),
@@ -316,6 +317,20 @@ class Graph:
         ok = c_int32()
         _check(lib().bd_graph_check(self._h, byref(ok)), "graph check")
         return bool(ok.value)
+
+    # hybrid_bfs::check (hybrid_bfs.cc:281-379) of any parent array, on the device
+    def check_parents(self, source: int, parent: np.ndarray) -> tuple[bool, int]:
+        """(passes, lowest failing vertex or -1) for a parent array of n
+        entries in the reference's encoding (source -> source, unreached
+        vertices negative)."""
+        par = np.ascontiguousarray(parent, dtype=np.int64)
+        n = self.num_vertices()
+        if par.shape != (n,):
+            raise ValueError(f"parent array of shape {par.shape} for {n} vertices")
+        ok, bad = c_int32(), c_int64()
+        _check(lib().bd_graph_check_parents(self._h, source, _ptr(par, c_int64), byref(ok),
+                                            byref(bad)), "check_parents")
+        return bool(ok.value), int(bad.value)
 
     def pick_roots(self, seed: int, k: int) -> np.ndarray:
         roots = np.empty(k, np.int64)

@@ -1486,14 +1486,15 @@ bd_status bd_bfs_count_traversed_edges(bd_bfs *b, int64_t *out)
     return BD_OK;
 }
 
-// hybrid_bfs::check (hybrid_bfs.cc:281-379), on the host (bd::check_parents).
+// hybrid_bfs::check (hybrid_bfs.cc:281-379), on the device (bd_check.cu),
+// of the parents the last run left in HBM.
 bd_status bd_bfs_check(bd_bfs *b, int64_t source, int32_t *ok)
 {
     if (!b || !ok) { return BD_ERR_INVALID; }
     if (source < 0 || source >= b->g->n) { return BD_ERR_RANGE; }
-    std::vector<int64_t> parent(b->g->n);
-    BD_TRY(bd_bfs_get_parents(b, parent.data()));
-    return check_parents(b->g, source, parent.data(), ok);
+    const int64_t *parent = nullptr;
+    BD_TRY(bd_bfs_device_ptrs(b, nullptr, &parent));
+    return check_parents_device(b->g, source, parent, ok, nullptr);
 }
 
 bd_status bd_bfs_get_steps(bd_bfs *b, bd_step *steps, int64_t capacity, int64_t *count)

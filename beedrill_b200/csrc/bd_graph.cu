@@ -1198,53 +1198,3 @@ bd_status bd_graph_destroy(bd_graph *g)
 }
 
 }  // extern "C"
-
-namespace bd {
-
-// hybrid_bfs::check (hybrid_bfs.cc:281-379) on the host: a serial queue BFS
-// for depths, then every reached vertex must have its parent in its
-// adjacency list exactly one level up, and reachability must agree.
-bd_status check_parents(const bd_graph *g, int64_t source, const int64_t *parent, int32_t *ok)
-{
-    const int64_t n = g->n;
-    std::vector<int64_t> off(n + 1);
-    std::vector<uint32_t> adj(g->arcs);
-    BD_TRY(bd_graph_copy_csr(g, off.data(), adj.data()));
-    std::vector<int64_t> depth(n, -1), q;
-    q.reserve(n);
-    q.push_back(source);
-    depth[source] = 0;
-    for (size_t h = 0; h < q.size(); ++h) {
-        int64_t u = q[h];
-        for (int64_t e = off[u]; e < off[u + 1]; ++e) {
-            int64_t v = adj[e];
-            if (depth[v] == -1) {
-                depth[v] = depth[u] + 1;
-                q.push_back(v);
-            }
-        }
-    }
-    *ok = 1;
-    for (int64_t u = 0; u < n; ++u) {
-        if (depth[u] >= 0 && parent[u] >= 0) {
-            if (u == source) {
-                if (!(parent[u] == u && depth[u] == 0)) { *ok = 0; break; }
-                continue;
-            }
-            bool found = false;
-            for (int64_t e = off[u]; e < off[u + 1]; ++e) {
-                if ((int64_t)adj[e] == parent[u]) {
-                    found = depth[parent[u]] == depth[u] - 1;
-                    break;
-                }
-            }
-            if (!found) { *ok = 0; break; }
-        } else if ((depth[u] < 0) != (parent[u] < 0)) {
-            *ok = 0;
-            break;
-        }
-    }
-    return BD_OK;
-}
-
-}  // namespace bd

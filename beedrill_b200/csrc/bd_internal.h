@@ -80,9 +80,12 @@ struct PolicyBlob;
 // Host-side PolicyBlob from the ABI's arrays (bd_policy.cu).
 bd_status policy_blob(const float *params, const float *mean, const float *inv_std,
                       const float *lo, const float *hi, float margin, PolicyBlob *blob);
-// hybrid_bfs::check on the host for a parent array in the reference's
-// encoding; *ok = 1 when it passes.
-bd_status check_parents(const bd_graph *g, int64_t source, const int64_t *parent, int32_t *ok);
+// hybrid_bfs::check on the device (bd_check.cu) for a parent array in
+// device memory, in the reference's encoding and the caller's vertex ids;
+// *ok = 1 when it passes, *bad_vertex (may be null) gets the lowest failing
+// vertex or -1.
+bd_status check_parents_device(const bd_graph *g, int64_t source, const int64_t *d_parent,
+                               int32_t *ok, int64_t *bad_vertex);
 // BD_ORDER_HUB: builds the renumbered traversal CSR of a finished graph.
 bd_status graph_build_hub(bd_graph *g, cudaStream_t s);
 // Fills d_isolated from d_off.

@@ -1257,22 +1257,30 @@ bd_status ms_check_root(bd_msbfs *b, int32_t root_index)
     return BD_OK;
 }
 
+// One root's depths or parents (caller ids, reference encoding) into a
+// device buffer of n entries, queued on the handle's stream.
+cudaError_t ms_extract_async(bd_msbfs *b, int32_t root_index, int32_t *d_depth, int64_t *d_parent)
+{
+    const int64_t n = b->g->n;
+    const int group = root_index / 64, lane = root_index % 64;
+    const int64_t slice = n * (int64_t)b->R;
+    ms_extract_kernel<<<ms_grid_for(n), 256, 0, b->stream>>>(
+        b->depth + group * slice, b->parent + group * slice, b->drec + group * n * (int64_t)kRecSlots,
+        b->drec_cnt + group * n, b->seen + group * n, b->g->d_off, n, b->R, lane, b->g->d_perm,
+        b->g->d_iperm, d_depth, d_parent);
+    return cudaGetLastError();
+}
+
 bd_status ms_extract(bd_msbfs *b, int32_t root_index, int32_t *depth, int64_t *parent)
 {
     BD_TRY(ms_check_root(b, root_index));
     BD_CUDA(cudaSetDevice(b->device));
     const int64_t n = b->g->n;
-    const int group = root_index / 64, lane = root_index % 64;
-    const int64_t slice = n * (int64_t)b->R;
     void *tmp = nullptr;
     const size_t bytes = depth ? sizeof(int32_t) * n : sizeof(int64_t) * n;
     BD_CUDA(cudaMalloc(&tmp, bytes));
-    ms_extract_kernel<<<ms_grid_for(n), 256, 0, b->stream>>>(
-        b->depth + group * slice, b->parent + group * slice, b->drec + group * n * (int64_t)kRecSlots,
-        b->drec_cnt + group * n, b->seen + group * n, b->g->d_off, n, b->R, lane, b->g->d_perm,
-        b->g->d_iperm, depth ? static_cast<int32_t *>(tmp) : nullptr,
-        parent ? static_cast<int64_t *>(tmp) : nullptr);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = ms_extract_async(b, root_index, depth ? static_cast<int32_t *>(tmp) : nullptr,
+                                     parent ? static_cast<int64_t *>(tmp) : nullptr);
     if (e == cudaSuccess) {
         e = cudaMemcpyAsync(depth ? (void *)depth : (void *)parent, tmp, bytes,
                             cudaMemcpyDeviceToHost, b->stream);
@@ -1446,13 +1454,22 @@ bd_status bd_msbfs_get_parents(bd_msbfs *b, int32_t root_index, int64_t *parent)
     return ms_extract(b, root_index, nullptr, parent);
 }
 
+// hybrid_bfs::check of one root's parents, extracted and checked in HBM
+// (bd_check.cu).
 bd_status bd_msbfs_check(bd_msbfs *b, int32_t root_index, int32_t *ok)
 {
     if (!b || !ok) { return BD_ERR_INVALID; }
     BD_TRY(ms_check_root(b, root_index));
-    std::vector<int64_t> parent(b->g->n);
-    BD_TRY(ms_extract(b, root_index, nullptr, parent.data()));
-    return check_parents(b->g, b->sources[root_index], parent.data(), ok);
+    BD_CUDA(cudaSetDevice(b->device));
+    int64_t *parent = nullptr;
+    BD_CUDA(cudaMalloc(&parent, sizeof(int64_t) * b->g->n));
+    cudaError_t e = ms_extract_async(b, root_index, nullptr, parent);
+    if (e == cudaSuccess) { e = cudaStreamSynchronize(b->stream); }
+    const bd_status st = e == cudaSuccess
+                             ? check_parents_device(b->g, b->sources[root_index], parent, ok, nullptr)
+                             : cuda_fail(e, "msbfs extract", __FILE__, __LINE__);
+    cudaFree(parent);
+    return st;
 }
 
 bd_status bd_msbfs_count_traversed_edges(bd_msbfs *b, int32_t root_index, int64_t *edges,

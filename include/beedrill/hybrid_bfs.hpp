@@ -315,6 +315,21 @@ public:
         throw_if(bd_graph_check(h_, &ok), "check_graph");
         return ok != 0;
     }
+    // hybrid_bfs::check (hybrid_bfs.cc:281-379) of any parent array (n entries,
+    // the reference's encoding), on the device; *bad_vertex gets the lowest
+    // failing vertex or -1.
+    bool check_parents(int64_t source, const std::vector<int64_t> &parent,
+                       int64_t *bad_vertex = nullptr) const
+    {
+        if ((long)parent.size() != num_vertices()) {
+            throw error(BD_ERR_INVALID, "check_parents: parent array size");
+        }
+        int32_t ok = 0;
+        int64_t bad = -1;
+        throw_if(bd_graph_check_parents(h_, source, parent.data(), &ok, &bad), "check_parents");
+        if (bad_vertex) { *bad_vertex = bad; }
+        return ok != 0;
+    }
     // pick_random_vertex with lcg(seed) (hybrid_bfs_main.cc:136-144)
     std::vector<int64_t> pick_roots(uint64_t seed, int64_t k) const
     {

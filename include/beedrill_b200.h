@@ -23,7 +23,8 @@
  *   run_with_migrating_threads / run_with_remote_writes
  *     (hybrid_bfs.cc:196-235)                               -> bd_bfs_run_top_down
  *   run_with_remote_writes_hybrid (hybrid_bfs.cc:243-277)   -> bd_bfs_run_beamer
- *   hybrid_bfs::check (hybrid_bfs.cc:281-379)               -> bd_bfs_check
+ *   hybrid_bfs::check (hybrid_bfs.cc:281-379)               -> bd_bfs_check,
+ *                                                              bd_graph_check_parents
  *   hybrid_bfs::count_num_traversed_edges (:401-414)        -> bd_bfs_count_traversed_edges
  *   hybrid_bfs::print_tree (hybrid_bfs.cc:381-399)          -> bd_bfs_get_parents (+ host printing)
  */
@@ -155,6 +156,14 @@ bd_status bd_graph_write_el64(const bd_graph *g, const char *path);
 /* graph::check: every edge present in both lists, no adjacent duplicates.
  * ok receives 1 (pass) or 0. */
 bd_status bd_graph_check(const bd_graph *g, int32_t *ok);
+/* hybrid_bfs::check (hybrid_bfs.cc:281-379) of a caller's parent array
+ * (host, n entries, the reference's encoding: the source is its own parent,
+ * unreached vertices negative), run on the device against depths from an
+ * independent device BFS from source.  ok receives 1 (pass) or 0;
+ * bad_vertex (may be NULL) receives the lowest failing vertex -- the one
+ * the reference's loop stops at -- or -1. */
+bd_status bd_graph_check_parents(const bd_graph *g, int64_t source, const int64_t *parent,
+                                 int32_t *ok, int64_t *bad_vertex);
 /* Roots as hybrid_bfs_main.cc:136-144 with lcg(seed). */
 bd_status bd_graph_pick_roots(const bd_graph *g, uint64_t seed, int64_t k, int64_t *roots);
 /* Device pointers of the CSR (borrowed, valid until bd_graph_destroy). */

@@ -206,15 +206,17 @@ void or_bfs_depth(int64_t n, const int64_t *offsets, const uint32_t *adj,
     free(q);
 }
 
-/* hybrid_bfs.cc:281-379.  Stops at the first failure, like the reference. */
-int or_check(int64_t n, const int64_t *offsets, const uint32_t *adj,
-             int64_t source, const int64_t *parent, int32_t *depth)
+/* hybrid_bfs.cc:281-379.  Returns the vertex u at which the reference's
+ * ascending loop stops (the u its LOG lines name), or -1 when the check
+ * passes. */
+int64_t or_check_first_bad(int64_t n, const int64_t *offsets, const uint32_t *adj,
+                           int64_t source, const int64_t *parent, int32_t *depth)
 {
     or_bfs_depth(n, offsets, adj, source, depth);
     for (int64_t u = 0; u < n; ++u) {
         if (depth[u] >= 0 && parent[u] >= 0) {
             if (u == source) {
-                if (!(parent[u] == u && depth[u] == 0)) { return 0; }
+                if (!(parent[u] == u && depth[u] == 0)) { return u; }
                 continue;
             }
             int found = 0;
@@ -226,12 +228,19 @@ int or_check(int64_t n, const int64_t *offsets, const uint32_t *adj,
                     break;
                 }
             }
-            if (!found) { return 0; }
+            if (!found) { return u; }
         } else if ((depth[u] < 0) != (parent[u] < 0)) {
-            return 0;
+            return u;
         }
     }
-    return 1;
+    return -1;
+}
+
+/* hybrid_bfs::check's verdict: 1 = pass. */
+int or_check(int64_t n, const int64_t *offsets, const uint32_t *adj,
+             int64_t source, const int64_t *parent, int32_t *depth)
+{
+    return or_check_first_bad(n, offsets, adj, source, parent, depth) < 0;
 }
 
 void or_min_parent(int64_t n, const int64_t *offsets, const uint32_t *adj,

@@ -52,6 +52,10 @@ void or_bfs_depth(int64_t n, const int64_t *offsets, const uint32_t *adj,
  * is int32[n]; on return it holds the serial BFS depths. */
 int or_check(int64_t n, const int64_t *offsets, const uint32_t *adj,
              int64_t source, const int64_t *parent, int32_t *depth_scratch);
+/* The same check; returns the vertex at which the reference's loop stops
+ * (the one its LOG lines name), or -1 on PASS. */
+int64_t or_check_first_bad(int64_t n, const int64_t *offsets, const uint32_t *adj,
+                           int64_t source, const int64_t *parent, int32_t *depth_scratch);
 /* Deterministic tree: parent(v) = min{u in N(v) : depth[u] == depth[v]-1},
  * parent(source) = source, unreached -> reference encoding. */
 void or_min_parent(int64_t n, const int64_t *offsets, const uint32_t *adj,

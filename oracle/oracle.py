@@ -48,6 +48,8 @@ def lib() -> ctypes.CDLL:
         L.or_bfs_depth.argtypes = [c_int64, i64p, u32p, c_int64, i32p]
         L.or_bfs_depth.restype = None
         L.or_check.argtypes = [c_int64, i64p, u32p, c_int64, i64p, i32p]
+        L.or_check_first_bad.argtypes = [c_int64, i64p, u32p, c_int64, i64p, i32p]
+        L.or_check_first_bad.restype = c_int64
         L.or_min_parent.argtypes = [c_int64, i64p, u32p, c_int64, i32p, i64p]
         L.or_min_parent.restype = None
         L.or_count_traversed.argtypes = [c_int64, i64p, i64p]
@@ -142,6 +144,14 @@ def check(off, adj, source: int, parent: np.ndarray) -> bool:
     scratch = np.empty(len(off) - 1, np.int32)
     return bool(lib().or_check(len(off) - 1, _p(off, c_int64), _p(adj, c_uint32), source,
                                _p(parent, c_int64), _p(scratch, ctypes.c_int32)))
+
+
+def check_first_bad(off, adj, source: int, parent: np.ndarray) -> int:
+    """The vertex at which hybrid_bfs::check stops (hybrid_bfs.cc:331-376), or -1."""
+    parent = np.ascontiguousarray(parent, np.int64)
+    scratch = np.empty(len(off) - 1, np.int32)
+    return int(lib().or_check_first_bad(len(off) - 1, _p(off, c_int64), _p(adj, c_uint32), source,
+                                        _p(parent, c_int64), _p(scratch, ctypes.c_int32)))
 
 
 def min_parent(off, adj, source: int, depth: np.ndarray) -> np.ndarray:

@@ -2,7 +2,8 @@
 one edge, an isolated source, a star (one vertex adjacent to all), a long
 path, several components, and a source in a small component; for each
 direction policy, each adjacency order including the hub layout, min-parent
-trees, and the batched kernel.  Expected values come from the oracle."""
+trees, and the batched kernel.  Expected values come from the oracle; the
+device check() must pass every tree the oracle's check passes."""
 import numpy as np
 import pytest
 
@@ -69,6 +70,7 @@ def test_single_source_every_policy(name, order):
             assert np.array_equal(bfs.depths(), depth), (name, order, alg, s)
             par = bfs.parents()
             assert O.check(off, adj, s, par), (name, order, alg, s)
+            assert bfs.check(s) and g.check_parents(s, par) == (True, -1), (name, order, alg, s)
             assert bfs.count_num_traversed_edges() == O.count_traversed(off, par)
         bfs.close()
     g.close()
@@ -94,5 +96,6 @@ def test_min_parent_and_batched(name, order):
         assert np.array_equal(ms.depths(i), depth), (name, order, s)
         par = ms.parents(i)
         assert O.check(off, adj, s, par)
+        assert ms.check(i), (name, order, s)
         assert m_c[i] == O.count_traversed(off, par) and n_c[i] == int((depth >= 0).sum())
     g.close()

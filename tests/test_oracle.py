@@ -149,20 +149,31 @@ def test_check_rejects_planted_mistakes(scale10):
     non_nbrs = np.setdiff1d(np.arange(n), adj[off[v]:off[v + 1]])
     bad[v] = int(non_nbrs[non_nbrs != v][0])
     assert not O.check(off, adj, root, bad)
+    assert O.check_first_bad(off, adj, root, bad) == v
     # neighbour at the wrong depth
     same = [u for u in adj[off[v]:off[v + 1]] if depth[u] == depth[v]]
     if same:
         bad = good.copy()
         bad[v] = int(same[0])
         assert not O.check(off, adj, root, bad)
+        assert O.check_first_bad(off, adj, root, bad) == v
     # reachable vertex left without a parent
     bad = good.copy()
     bad[v] = -1
     assert not O.check(off, adj, root, bad)
+    assert O.check_first_bad(off, adj, root, bad) == v
     # source not its own parent
     bad = good.copy()
     bad[root] = int(adj[off[root]])
     assert not O.check(off, adj, root, bad)
+    assert O.check_first_bad(off, adj, root, bad) == root
+    # two mistakes: the check stops at the lower vertex
+    w = int(rng.choice(reached[reached != v]))
+    bad = good.copy()
+    bad[v] = -1
+    bad[w] = -1
+    assert O.check_first_bad(off, adj, root, bad) == min(v, w)
+    assert O.check_first_bad(off, adj, root, good) == -1
 
 
 def test_el64_header_rules(tmp_path):
