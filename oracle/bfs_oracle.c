@@ -273,6 +273,107 @@ int64_t or_count_traversed(int64_t n, const int64_t *offsets, const int64_t *par
     return sum / 2;
 }
 
+/* ---- connected components ------------------------------------------------ */
+
+/* components::run (components.cc:38-118) as its serial elision executes
+ * it.  Every vertex starts as its own component; a pass visits every arc
+ * (src, dst) and lowers component[src] to component[dst] when that is
+ * smaller; then each vertex's label is replaced by its label's label until
+ * it is a fixed point (pointer jumping); passes repeat until one changes
+ * nothing.  The worklist pushes each vertex at its head (worklist.h
+ * append), so a pass visits vertices in descending order; pointer jumping
+ * runs in ascending order.  Returns the number of passes (the last, which
+ * changed nothing, included) -- the `num_iters` the reference prints. */
+int64_t or_components(int64_t n, const int64_t *offsets, const uint32_t *adj,
+                      int64_t *component, int64_t *size, int64_t *num_components)
+{
+    for (int64_t v = 0; v < n; ++v) {
+        component[v] = v;
+        size[v] = 0;
+    }
+    int64_t iters;
+    for (iters = 1;; ++iters) {
+        int changed = 0;
+        for (int64_t s = n - 1; s >= 0; --s) {
+            for (int64_t e = offsets[s]; e < offsets[s + 1]; ++e) {
+                int64_t d = adj[e];
+                if (component[d] < component[s]) {
+                    component[s] = component[d];
+                    changed = 1;
+                }
+            }
+        }
+        if (!changed) { break; }
+        for (int64_t v = 0; v < n; ++v) {
+            while (component[v] != component[component[v]]) {
+                component[v] = component[component[v]];
+            }
+        }
+    }
+    int64_t count = 0;
+    for (int64_t v = 0; v < n; ++v) { size[component[v]] += 1; }
+    for (int64_t v = 0; v < n; ++v) { count += size[v] > 0; }
+    *num_components = count;
+    return iters;
+}
+
+typedef struct {
+    int64_t label, vertex;
+} or_label_pair;
+
+static int or_label_cmp(const void *a, const void *b)
+{
+    const or_label_pair *x = a, *y = b;
+    if (x->label != y->label) { return x->label < y->label ? -1 : 1; }
+    return x->vertex < y->vertex ? -1 : (x->vertex > y->vertex);
+}
+
+/* components::check (components.cc:155-200): for each distinct label, a
+ * serial BFS from the last vertex carrying it (the label_to_source map is
+ * filled in ascending vertex order) must meet only that label, and every
+ * vertex must be visited by one of these searches.  Returns 1 = PASS. */
+int or_components_check(int64_t n, const int64_t *offsets, const uint32_t *adj,
+                        const int64_t *component)
+{
+    or_label_pair *pairs = malloc(sizeof(*pairs) * (n ? n : 1));
+    char *visited = calloc(n ? n : 1, 1);
+    int64_t *q = malloc(sizeof(int64_t) * (n ? n : 1));
+    for (int64_t v = 0; v < n; ++v) {
+        pairs[v].label = component[v];
+        pairs[v].vertex = v;
+    }
+    qsort(pairs, n, sizeof(*pairs), or_label_cmp);
+    int ok = 1;
+    for (int64_t i = 0; i < n && ok; ++i) {
+        if (i + 1 < n && pairs[i + 1].label == pairs[i].label) { continue; }
+        const int64_t label = pairs[i].label, source = pairs[i].vertex;
+        visited[source] = 1;
+        int64_t head = 0, tail = 0;
+        q[tail++] = source;
+        while (head < tail && ok) {
+            const int64_t u = q[head++];
+            for (int64_t e = offsets[u]; e < offsets[u + 1]; ++e) {
+                const int64_t v = adj[e];
+                if (component[v] != label) {
+                    ok = 0;
+                    break;
+                }
+                if (!visited[v]) {
+                    visited[v] = 1;
+                    q[tail++] = v;
+                }
+            }
+        }
+    }
+    for (int64_t v = 0; v < n && ok; ++v) {
+        if (!visited[v]) { ok = 0; }
+    }
+    free(pairs);
+    free(visited);
+    free(q);
+    return ok;
+}
+
 /* run_beamer's control flow (hybrid_bfs.cc:152-191) over a level profile.
  * Both step kinds discover exactly the next BFS level, so the per-level
  * vertex counts and degree sums fix every decision:

@@ -60,6 +60,13 @@ int64_t or_check_first_bad(int64_t n, const int64_t *offsets, const uint32_t *ad
  * parent(source) = source, unreached -> reference encoding. */
 void or_min_parent(int64_t n, const int64_t *offsets, const uint32_t *adj,
                    int64_t source, const int32_t *depth, int64_t *parent);
+/* components::run (components.cc:38-118), serial-elision order; returns
+ * the reference's num_iters.  component and size are int64[n]. */
+int64_t or_components(int64_t n, const int64_t *offsets, const uint32_t *adj,
+                      int64_t *component, int64_t *size, int64_t *num_components);
+/* components::check (components.cc:155-200).  Returns 1 = PASS. */
+int or_components_check(int64_t n, const int64_t *offsets, const uint32_t *adj,
+                        const int64_t *component);
 /* count_num_traversed_edges (hybrid_bfs.cc:401-414). */
 int64_t or_count_traversed(int64_t n, const int64_t *offsets, const int64_t *parent);
 

@@ -50,6 +50,9 @@ def lib() -> ctypes.CDLL:
         L.or_check.argtypes = [c_int64, i64p, u32p, c_int64, i64p, i32p]
         L.or_check_first_bad.argtypes = [c_int64, i64p, u32p, c_int64, i64p, i32p]
         L.or_check_first_bad.restype = c_int64
+        L.or_components.argtypes = [c_int64, i64p, u32p, i64p, i64p, i64p]
+        L.or_components.restype = c_int64
+        L.or_components_check.argtypes = [c_int64, i64p, u32p, i64p]
         L.or_min_parent.argtypes = [c_int64, i64p, u32p, c_int64, i32p, i64p]
         L.or_min_parent.restype = None
         L.or_count_traversed.argtypes = [c_int64, i64p, i64p]
@@ -152,6 +155,25 @@ def check_first_bad(off, adj, source: int, parent: np.ndarray) -> int:
     scratch = np.empty(len(off) - 1, np.int32)
     return int(lib().or_check_first_bad(len(off) - 1, _p(off, c_int64), _p(adj, c_uint32), source,
                                         _p(parent, c_int64), _p(scratch, ctypes.c_int32)))
+
+
+def components(off, adj):
+    """(labels, sizes, num_components, num_iters) of components::run
+    (components.cc:38-118) in its serial-elision order."""
+    n = len(off) - 1
+    comp = np.empty(n, np.int64)
+    size = np.empty(n, np.int64)
+    count = c_int64()
+    iters = lib().or_components(n, _p(off, c_int64), _p(adj, c_uint32), _p(comp, c_int64),
+                                _p(size, c_int64), ctypes.byref(count))
+    return comp, size, int(count.value), int(iters)
+
+
+def components_check(off, adj, labels: np.ndarray) -> bool:
+    """components::check (components.cc:155-200) of any labelling."""
+    labels = np.ascontiguousarray(labels, np.int64)
+    return bool(lib().or_components_check(len(off) - 1, _p(off, c_int64), _p(adj, c_uint32),
+                                          _p(labels, c_int64)))
 
 
 def min_parent(off, adj, source: int, depth: np.ndarray) -> np.ndarray:

@@ -17,6 +17,14 @@ What it writes, and where each number comes from:
 * ref_gen12.npz -- the same reference run on the project's seeded generator
   output at scale 12 (seed 12), so parents/levels can be compared at full
   detail on a graph the device generator must reproduce byte for byte.
+* ref_components.npz -- oracle/_ref/components (the reference's
+  connected-components CLI) with --check_results --dump_results on three
+  graphs: graph500-scale10.el64, a sparse project-generated RMAT graph
+  (scale 12, edge factor 2, seed 5) and a 48 x 48 grid with 30 % of its
+  edges deleted (seed 3).  Per graph: the CSR, the labels parsed from the
+  reference's dump, its component count, iteration count and check()
+  verdict.  `python tests/golden/make_golden.py --components` rewrites
+  only this file.
 * golden.json -- hashes and per-root summaries: sha256 of the generator's
   el64 files (scale 12 and 16), and for scale 16 (seed 16, 8 roots of lcg(0))
   the reference's m_c, per-step discovered counts, per-level directions and
@@ -27,6 +35,7 @@ from __future__ import annotations
 import hashlib
 import json
 import os
+import re
 import subprocess
 import sys
 import tempfile
@@ -87,8 +96,52 @@ def pack_roots(d):
     }
 
 
+def ref_components(el64, n):
+    """Labels, component count, iteration count and check() verdict printed
+    by the reference's components CLI (components_main.cc:164-196)."""
+    out = subprocess.run([os.path.join(O.REF_DIR, "components"), "--graph_filename", el64,
+                          "--check_results", "--dump_results"], check=True,
+                         stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True).stdout
+    labels = np.full(n, -1, np.int64)
+    count = iters = None
+    passed = None
+    for line in out.splitlines():
+        m = re.match(r"Found (\d+) components in (\d+) iterations", line)
+        if m:
+            count, iters = int(m.group(1)), int(m.group(2))
+        if line.startswith("Checking results..."):
+            passed = line.endswith("PASS")
+        m = re.match(r"Component (\d+): (.*)$", line)
+        if m:
+            c = int(m.group(1))
+            for part in m.group(2).split(", "):
+                lo, _, hi = part.partition("-")
+                labels[int(lo): int(hi or lo) + 1] = c
+    assert (labels >= 0).all() and count is not None and passed is not None
+    return labels, count, iters, passed
+
+
+def components_fixture(tmp):
+    graphs = {"scale10": O.el64_load(os.path.join(HERE, "graph500-scale10.el64")),
+              "rmat12_ef2": O.rmat_graph(12, edge_factor=2, seed=5),
+              "grid48": O.grid_graph(48, 48, 0.3, seed=3)}
+    arrays = {}
+    for name, (n, src, dst) in graphs.items():
+        el = os.path.join(tmp, name + ".el64")
+        O.el64_write(el, n, src, dst)
+        off, adj = O.csr_build(n, src, dst)
+        labels, count, iters, passed = ref_components(el, n)
+        arrays.update({f"{name}.offsets": off, f"{name}.adj": adj, f"{name}.labels": labels,
+                       f"{name}.summary": np.array([count, iters, int(passed)], np.int64)})
+    np.savez_compressed(os.path.join(HERE, "ref_components.npz"), **arrays)
+
+
 def main():
     O.build()
+    if "--components" in sys.argv[1:]:
+        with tempfile.TemporaryDirectory() as tmp:
+            components_fixture(tmp)
+        return
     if not os.path.exists(os.path.join(O.REF_DIR, "ref_dump")):
         sys.exit("reference builds missing: the reference sources are needed")
     golden = {"generator": {"a": 0.57, "b": 0.19, "c": 0.19, "d": 0.05, "edge_factor": 16}}
@@ -147,6 +200,7 @@ def main():
                                          + adj.astype("<u4").tobytes()).hexdigest(),
             "alpha": 15, "beta": 18, "roots": roots,
         }
+        components_fixture(tmp)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
         f.write("\n")

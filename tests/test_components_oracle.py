@@ -1,0 +1,63 @@
+"""The connected-components oracle against the reference's own build.
+
+tests/golden/ref_components.npz holds what the reference's components CLI
+(components_main.cc, built from its sources by oracle/Makefile) printed on
+three graphs: labels (from --dump_results), component count, iteration
+count and its check() verdict.  The oracle's restatement of
+components::run must reproduce all of them, and its restatement of
+components::check must accept exactly the labellings the reference's rule
+accepts.  CPU only.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+NAMES = ["scale10", "rmat12_ef2", "grid48"]
+
+
+@pytest.fixture(scope="module")
+def ref():
+    O.build()
+    return np.load(os.path.join(HERE, "golden", "ref_components.npz"))
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_components_match_the_reference(ref, name):
+    off, adj = ref[f"{name}.offsets"], ref[f"{name}.adj"]
+    count, iters, passed = ref[f"{name}.summary"].tolist()
+    labels, sizes, k, it = O.components(off, adj)
+    assert np.array_equal(labels, ref[f"{name}.labels"])
+    assert (k, it) == (count, iters)
+    assert passed == 1 and O.components_check(off, adj, labels)
+    assert sizes.sum() == len(labels) and int((sizes > 0).sum()) == k
+    assert np.array_equal(np.flatnonzero(sizes), np.unique(labels))
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_check_rule(ref, name):
+    """components::check accepts any labelling that gives each component one
+    label of its own, and nothing else."""
+    off, adj = ref[f"{name}.offsets"], ref[f"{name}.adj"]
+    good = ref[f"{name}.labels"]
+    uniq, counts = np.unique(good, return_counts=True)
+    big = int(uniq[np.argmax(counts)])
+    other = int(uniq[uniq != big][0])
+    members = np.flatnonzero(good == big)
+    # one vertex of a component relabelled: its edges cross labels
+    bad = good.copy()
+    bad[members[len(members) // 2]] = -7
+    assert not O.components_check(off, adj, bad)
+    # two components share one label: the second is never visited
+    bad = good.copy()
+    bad[good == other] = big
+    assert not O.components_check(off, adj, bad)
+    # arbitrary but distinct labels per component pass
+    relabel = good * 3 + (1 << 40)
+    assert O.components_check(off, adj, relabel)
+    swapped = good.copy()
+    swapped[good == big], swapped[good == other] = other, big
+    assert O.components_check(off, adj, swapped)
