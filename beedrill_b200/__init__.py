@@ -25,7 +25,7 @@ from ctypes import (POINTER, Structure, byref, c_char_p, c_double, c_float, c_in
 
 import numpy as np
 
-__all__ = ["BeedrillError", "Graph", "HybridBFS", "BatchedBFS", "Step", "ALGORITHMS", "lib", "LIB_PATH",
+__all__ = ["BeedrillError", "Graph", "HybridBFS", "BatchedBFS", "Components", "Step", "ALGORITHMS", "lib", "LIB_PATH",
            "tuned_options",
            "policy_forward", "policy_loss_grad", "policy_train"]
 
@@ -96,6 +96,10 @@ class RunStats(Structure):
     ]
 
 
+class ComponentsStats(Structure):
+    _fields_ = [("num_components", c_int64), ("num_iters", c_int64), ("ms", c_double)]
+
+
 _lib = None
 TUNING_PATH = os.path.join(HERE, "tuning", "b200.json")
 
@@ -147,6 +151,15 @@ def lib() -> ctypes.CDLL:
         "bd_graph_write_el64": (c_int, [c_void_p, c_char_p]),
         "bd_graph_check": (c_int, [c_void_p, i32p]),
         "bd_graph_check_parents": (c_int, [c_void_p, c_int64, i64p, i32p, i64p]),
+        "bd_graph_check_components": (c_int, [c_void_p, i64p, i32p, i64p]),
+        "bd_components_create": (c_int, [c_void_p, vpp]),
+        "bd_components_clear": (c_int, [c_void_p]),
+        "bd_components_run": (c_int, [c_void_p, POINTER(ComponentsStats)]),
+        "bd_components_get_labels": (c_int, [c_void_p, i64p]),
+        "bd_components_get_sizes": (c_int, [c_void_p, i64p]),
+        "bd_components_device_labels": (c_int, [c_void_p, vpp]),
+        "bd_components_check": (c_int, [c_void_p, i32p]),
+        "bd_components_destroy": (c_int, [c_void_p]),
         "bd_graph_pick_roots": (c_int, [c_void_p, c_uint64, c_int64, i64p]),
         "bd_graph_device_csr": (c_int, [c_void_p, vpp, vpp]),
         "bd_graph_destroy": (c_int, [c_void_p]),
@@ -330,6 +343,19 @@ class Graph:
         ok, bad = c_int32(), c_int64()
         _check(lib().bd_graph_check_parents(self._h, source, _ptr(par, c_int64), byref(ok),
                                             byref(bad)), "check_parents")
+        return bool(ok.value), int(bad.value)
+
+    # components::check (components.cc:155-200) of any labelling, on the device
+    def check_components(self, labels: np.ndarray) -> tuple[bool, int]:
+        """(passes, lowest vertex breaking the rule or -1) for int64 labels of
+        every vertex."""
+        lab = np.ascontiguousarray(labels, dtype=np.int64)
+        n = self.num_vertices()
+        if lab.shape != (n,):
+            raise ValueError(f"label array of shape {lab.shape} for {n} vertices")
+        ok, bad = c_int32(), c_int64()
+        _check(lib().bd_graph_check_components(self._h, _ptr(lab, c_int64), byref(ok), byref(bad)),
+               "check_components")
         return bool(ok.value), int(bad.value)
 
     def pick_roots(self, seed: int, k: int) -> np.ndarray:
@@ -597,6 +623,51 @@ class BatchedBFS:
     def close(self) -> None:
         if self._h is not None and self._h.value:
             lib().bd_msbfs_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Components:
+    """Connected components (components.h): every vertex labelled with the
+    smallest vertex id of its component, as the reference's run() leaves
+    component_; sizes per label as component_size_."""
+
+    def __init__(self, graph: Graph):
+        self.graph = graph
+        self._h = c_void_p()
+        self.last_stats = ComponentsStats()
+        _check(lib().bd_components_create(graph._h, byref(self._h)), "components")
+
+    def clear(self) -> None:
+        _check(lib().bd_components_clear(self._h), "clear")
+
+    def run(self) -> ComponentsStats:
+        _check(lib().bd_components_run(self._h, byref(self.last_stats)), "components run")
+        return self.last_stats
+
+    def labels(self) -> np.ndarray:
+        out = np.empty(self.graph.num_vertices(), np.int64)
+        _check(lib().bd_components_get_labels(self._h, _ptr(out, c_int64)), "labels")
+        return out
+
+    def sizes(self) -> np.ndarray:
+        out = np.empty(self.graph.num_vertices(), np.int64)
+        _check(lib().bd_components_get_sizes(self._h, _ptr(out, c_int64)), "sizes")
+        return out
+
+    def check(self) -> bool:
+        ok = c_int32()
+        _check(lib().bd_components_check(self._h, byref(ok)), "components check")
+        return bool(ok.value)
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            lib().bd_components_destroy(self._h)
         self._h = None
 
     def __del__(self):

@@ -663,6 +663,7 @@ bd_status graph_from_device_edges(int64_t n, int64_t m, int64_t *d_src, int64_t 
     g->m = m;
     g->arcs = 2 * m;
     g->order = order;
+    g->symmetric = true;  // every edge is stored in both directions
     g->d_src = d_src;
     g->d_dst = d_dst;
     cudaStream_t s = 0;
@@ -1049,6 +1050,8 @@ bd_status bd_graph_concat(bd_graph *const *graphs, int64_t count, bd_graph **out
     g->arcs = arcs;
     g->m = m;
     g->order = graphs[0]->order;
+    g->symmetric = true;
+    for (int64_t i = 0; i < count; ++i) { g->symmetric = g->symmetric && graphs[i]->symmetric; }
     if (cudaMalloc(&g->d_off, sizeof(int64_t) * (n + 1)) != cudaSuccess ||
         cudaMalloc(&g->d_adj, sizeof(uint32_t) * (arcs ? arcs : 1)) != cudaSuccess) {
         graph_free(g);

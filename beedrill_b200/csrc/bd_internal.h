@@ -44,6 +44,9 @@ struct bd_graph {
     int64_t arcs = 0;       // entries of the adjacency array
     int64_t n_live = 0;     // vertices of nonzero degree
     int32_t order = BD_ORDER_INSERTION;
+    // Every arc u->v has its reverse v->u (graphs built from edge lists, and
+    // unions of them); not assumed for a caller's CSR.
+    bool symmetric = false;
     int64_t *d_off = nullptr;     // [n + 1]
     uint32_t *d_adj = nullptr;    // [arcs]
     uint32_t *d_isolated = nullptr;  // [words(n)]
@@ -86,6 +89,12 @@ bd_status policy_blob(const float *params, const float *mean, const float *inv_s
 // vertex or -1.
 bd_status check_parents_device(const bd_graph *g, int64_t source, const int64_t *d_parent,
                                int32_t *ok, int64_t *bad_vertex);
+// components::check on the device (bd_check.cu) for labels in device
+// memory (int64[n]); *ok = 1 when it passes, *bad_vertex (may be null) gets
+// the lowest vertex that is unreached from its label's representative or
+// has an arc to another label, or -1.
+bd_status check_components_device(const bd_graph *g, const int64_t *d_label, int32_t *ok,
+                                  int64_t *bad_vertex);
 // BD_ORDER_HUB: builds the renumbered traversal CSR of a finished graph.
 bd_status graph_build_hub(bd_graph *g, cudaStream_t s);
 // Fills d_isolated from d_off.

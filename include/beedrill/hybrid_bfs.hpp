@@ -523,4 +523,78 @@ private:
     bd_run_stats stats_{};
 };
 
+// The reference's `components` class (components.h:6-33): run() labels
+// every vertex with the smallest id of its component.
+class components {
+public:
+    using stats = bd_components_stats;
+    explicit components(graph &g) : g_(g)
+    {
+        throw_if(bd_components_create(g.handle(), &h_), "components");
+    }
+    components(const components &) = delete;
+    components &operator=(const components &) = delete;
+    ~components()
+    {
+        if (h_) { bd_components_destroy(h_); }
+    }
+    void clear() { throw_if(bd_components_clear(h_), "clear"); }
+    stats run()
+    {
+        throw_if(bd_components_run(h_, &stats_), "run");
+        return stats_;
+    }
+    bool check()
+    {
+        int32_t ok = 0;
+        throw_if(bd_components_check(h_, &ok), "check");
+        return ok != 0;
+    }
+    // component_ and component_size_ (components.h:13-15)
+    std::vector<int64_t> component()
+    {
+        std::vector<int64_t> c(g_.num_vertices());
+        throw_if(bd_components_get_labels(h_, c.data()), "component");
+        return c;
+    }
+    std::vector<int64_t> component_size()
+    {
+        std::vector<int64_t> s(g_.num_vertices());
+        throw_if(bd_components_get_sizes(h_, s.data()), "component_size");
+        return s;
+    }
+    // components::dump (components.cc:120-152): per label, its vertices as ranges.
+    void dump()
+    {
+        const std::vector<int64_t> c = component();
+        std::vector<std::vector<int64_t>> members(c.size());
+        for (size_t v = 0; v < c.size(); ++v) { members[(size_t)c[v]].push_back((int64_t)v); }
+        for (size_t l = 0; l < members.size(); ++l) {
+            const std::vector<int64_t> &m = members[l];
+            if (m.empty()) { continue; }
+            printf("Component %zu: ", l);
+            for (size_t i = 0; i < m.size();) {
+                size_t j = i;
+                while (j + 1 < m.size() && m[j + 1] == m[j] + 1) { ++j; }
+                if (i) { printf(", "); }
+                if (j == i) {
+                    printf("%li", (long)m[i]);
+                } else {
+                    printf("%li-%li", (long)m[i], (long)m[j]);
+                }
+                i = j + 1;
+            }
+            printf("\n");
+        }
+        fflush(stdout);
+    }
+    const stats &last_stats() const { return stats_; }
+    bd_components *handle() const { return h_; }
+
+private:
+    graph &g_;
+    bd_components *h_ = nullptr;
+    stats stats_{};
+};
+
 }  // namespace beedrill

@@ -27,6 +27,12 @@
  *                                                              bd_graph_check_parents
  *   hybrid_bfs::count_num_traversed_edges (:401-414)        -> bd_bfs_count_traversed_edges
  *   hybrid_bfs::print_tree (hybrid_bfs.cc:381-399)          -> bd_bfs_get_parents (+ host printing)
+ *   components::components(graph&) (components.cc:13-22)   -> bd_components_create
+ *   components::run (components.cc:38-118)                  -> bd_components_run
+ *   components::component_, component_size_ (components.h:13-15)
+ *                                                           -> bd_components_get_labels, _get_sizes
+ *   components::check (components.cc:155-200)               -> bd_components_check,
+ *                                                              bd_graph_check_components
  */
 #ifndef BEEDRILL_B200_H
 #define BEEDRILL_B200_H
@@ -279,6 +285,42 @@ bd_status bd_msbfs_set_policy(bd_msbfs *b, const float *params, const float *mea
                               const float *inv_std, const float *lo, const float *hi,
                               float margin);
 bd_status bd_msbfs_destroy(bd_msbfs *b);
+
+/* ---- connected components ------------------------------------------------- */
+/* Labels every vertex with the smallest vertex id of its component -- the
+ * labelling the reference's label propagation converges to, so labels,
+ * sizes and the component count equal the reference's exactly.  One pass
+ * over the arcs builds a union-find forest on the device (num_iters = 1;
+ * the reference counts its label-propagation passes).  On a CSR that does
+ * not hold every edge in both directions the components are those of the
+ * undirected graph its arcs form; check() follows arcs as stored, like the
+ * reference's, so it is meaningful for symmetric graphs only. */
+typedef struct bd_components bd_components;
+typedef struct bd_components_stats {
+    int64_t num_components; /* isolated vertices count as one component each */
+    int64_t num_iters;      /* passes over the arcs */
+    double ms;              /* device time of run() */
+} bd_components_stats;
+bd_status bd_components_create(bd_graph *g, bd_components **out);
+/* components::clear is empty in the reference; run() starts over. */
+bd_status bd_components_clear(bd_components *cc);
+bd_status bd_components_run(bd_components *cc, bd_components_stats *stats);
+/* component_ / component_size_ (host int64[n]; size is indexed by label,
+ * 0 for ids that label nothing). */
+bd_status bd_components_get_labels(bd_components *cc, int64_t *component);
+bd_status bd_components_get_sizes(bd_components *cc, int64_t *component_size);
+/* Labels in device memory (borrowed, valid until the next run or destroy). */
+bd_status bd_components_device_labels(bd_components *cc, const int64_t **component);
+/* components::check of the last run's labels, on the device. */
+bd_status bd_components_check(bd_components *cc, int32_t *ok);
+bd_status bd_components_destroy(bd_components *cc);
+/* components::check (components.cc:155-200) of any labelling (host int64[n]):
+ * passes when every edge joins two vertices of one label and no label spans
+ * two components.  bad_vertex (may be NULL) receives the lowest vertex that
+ * breaks the rule (an edge to another label, or not reached from its
+ * label's representative), or -1. */
+bd_status bd_graph_check_components(const bd_graph *g, const int64_t *component, int32_t *ok,
+                                    int64_t *bad_vertex);
 
 /* ---- learned direction policy -------------------------------------------- */
 /* An fp32 MLP 8 -> 32 (ReLU) -> 32 (ReLU) -> 2 that picks the direction of
