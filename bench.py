@@ -45,6 +45,7 @@ EDGE_FACTOR = 16
 GRAPH_SEED = 24
 NUM_ROOTS = 64
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "hybrid_bfs")
+REF_CC_BIN = os.path.join(ROOT, "oracle", "_ref", "components")
 
 
 def hmean(x):
@@ -211,6 +212,8 @@ WORKLOADS = {
     "grid4096": {"kind": "grid", "rows": 4096, "cols": 4096, "delete": 0.01, "roots": 64},
     # 512 independent RMAT graphs (scales 10-18, edge factors 4-32), one root each
     "packed512": {"kind": "packed", "graphs": 512},
+    # connected components (components.cc) on the same RMAT scale-24 graph
+    "components24": {"kind": "components", "scale": 24, "cpu_scale": 20},
 }
 
 
@@ -307,6 +310,109 @@ def bench_packed(args, w, bd, order, local):
     multi.close()
     for h in singles:
         h.close()
+    return 0
+
+
+def reference_components_run(el64_path: str, trials: int, timeout: float):
+    """Runs the reference's components CLI (serial elision, one pinned core)
+    and returns per-trial (components, iterations, ms) (components_main.cc:180-181)."""
+    cmd = ["taskset", "-c", str(max(0, (os.cpu_count() or 1) - 1)), REF_CC_BIN,
+           "--graph_filename", el64_path, "--num_trials", str(trials)]
+    try:
+        out = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                             timeout=timeout).stdout
+    except (subprocess.TimeoutExpired, FileNotFoundError, OSError) as e:
+        return None, str(e)
+    rows = [(int(a), int(b), float(c)) for a, b, c in
+            re.findall(r"Found (\d+) components in (\d+) iterations \(([0-9.]+) ms", out)]
+    return rows, out[-400:]
+
+
+def bench_components(args, w, bd, local):
+    """Connected components of the RMAT scale-24 graph.  One step = one
+    components run (labels, sizes, count).  GTEPS = iterations x edges / time
+    as the reference prints it (components_main.cc:179); one iteration here.
+    The CPU baseline is the reference's own components build on a scale-20
+    graph of the same generator (its label propagation would take minutes at
+    scale 24 on one core)."""
+    import torch
+    scale = args.scale or w["scale"]
+    t_gen = time.time()
+    g = bd.Graph.rmat(scale, EDGE_FACTOR, seed=GRAPH_SEED if scale == SCALE else scale)
+    gen_s = time.time() - t_gen
+    n, m = g.num_vertices(), g.num_edges()
+    cc = bd.Components(g)
+    flush_buf = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def flush_l2():  # > the 126 MB L2 before every timed run
+        flush_buf.fill_(1)
+        torch.cuda.synchronize(local)
+
+    labels = np.empty(n, np.int64)
+    lab_ptr = labels.ctypes.data_as(bd.ctypes.POINTER(bd.ctypes.c_int64))
+    for _ in range(args.warmup):
+        flush_l2()
+        cc.run()
+    ok = cc.check()
+    ms, wall, counts = [], [], set()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush_l2()
+            t0 = time.perf_counter()
+            st = cc.run()
+            if bd.lib().bd_components_get_labels(cc._h, lab_ptr) != 0:
+                raise RuntimeError("label copy failed")
+            wall.append((time.perf_counter() - t0) * 1e3)
+            ms.append(st.ms)
+            counts.add(st.num_components)
+    if not ok or len(counts) != 1:
+        raise RuntimeError("components check failed or counts differ between runs")
+    ms_step = float(np.mean(ms))
+    value = m / (ms_step * 1e-3) / 1e9
+    e2e = m / (float(np.mean(wall)) * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    b_alg = 8.0 * (n + 1) + 8.0 * m + 4.0 * n + 16.0 * n
+    achieved = b_alg / (ms_step * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline and os.path.exists(REF_CC_BIN):
+        cs = w["cpu_scale"]
+        gs = bd.Graph.rmat(cs, EDGE_FACTOR, seed=cs)
+        ms_cpu = None
+        with tempfile.TemporaryDirectory(dir=os.environ.get("BD_TMP", None)) as tmp:
+            path = os.path.join(tmp, f"rmat{cs}.el64")
+            gs.write_el64(path)
+            rows, _ = reference_components_run(path, 2, timeout=600)
+        if rows:
+            ms_cpu = rows[-1][2]
+            cpu = {"value": gs.num_edges() / (ms_cpu * 1e-3) / 1e9, "unit": UNIT, "cores": 1,
+                   "kind": "reference",
+                   "sample": f"reference components build (serial elision, 1 pinned core) on "
+                             f"RMAT scale {cs} (seed {cs}): {rows[-1][0]} components, "
+                             f"{rows[-1][1]} label-propagation iterations, {ms_cpu:.0f} ms; "
+                             f"value = edges / time (its own printout multiplies by iterations)"}
+        gs.close()
+    line = {
+        "metric": f"connected components, edges / run time, RMAT scale {scale}, 1 B200",
+        "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": args.workload, "scale": scale, "edge_factor": EDGE_FACTOR,
+                   "num_vertices": n, "num_edges": m, "components": counts.pop(),
+                   "l2": "flushed (512 MB write) before every run; CSR %.2f GB" %
+                         ((8 * (n + 1) + 8 * m) / 1e9),
+                   "graph_build_s": round(gen_s, 2), "check": ok, "parallelism": "1 GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "note": "B_alg = 8(n+1) + 4*2m + 4n (forest) + 16n (labels, sizes) per run"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8 * n,
+                "note": "public API per step: run, then the int64 labels copied to the host"},
+        "cpu_baseline": cpu,
+        "gpu_launches": 4 * args.steps,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    cc.close()
+    g.close()
     return 0
 
 
@@ -411,6 +517,10 @@ def main():
         if world > 1:
             raise SystemExit("policy16-18 runs on one GPU")
         return bench_policy_set(args, w, bd, order, local)
+    if w["kind"] == "components":
+        if world > 1:
+            raise SystemExit("components24 runs on one GPU")
+        return bench_components(args, w, bd, local)
     num_roots = w["roots"]
     t_gen = time.time()
     if w["kind"] == "rmat":
