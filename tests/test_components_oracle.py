@@ -61,3 +61,37 @@ def test_check_rule(ref, name):
     swapped = good.copy()
     swapped[good == big], swapped[good == other] = other, big
     assert O.components_check(off, adj, swapped)
+
+
+def _random_graph(rng, n, m):
+    src = rng.integers(0, n, m)
+    dst = rng.integers(0, n, m)
+    keep = src != dst
+    pairs = np.unique(np.sort(np.stack([src[keep], dst[keep]], 1), axis=1), axis=0)
+    return O.csr_build(n, pairs[:, 0].astype(np.int64), pairs[:, 1].astype(np.int64))
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_components_against_scipy(seed):
+    """Labels equal the minimum vertex id of each component as scipy's
+    connected_components finds them, on sparse random graphs."""
+    sp = pytest.importorskip("scipy.sparse")
+    csgraph = pytest.importorskip("scipy.sparse.csgraph")
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(1, 3000))
+    off, adj = _random_graph(rng, n, int(rng.integers(0, 2 * n)))
+    mat = sp.csr_matrix((np.ones(len(adj)), adj.astype(np.int64), off), shape=(n, n))
+    k, comp = csgraph.connected_components(mat, directed=False)
+    first = np.full(k, n, np.int64)
+    np.minimum.at(first, comp, np.arange(n))
+    labels, sizes, count, iters = O.components(off, adj)
+    assert count == k and iters >= 1
+    assert np.array_equal(labels, first[comp])
+    assert np.array_equal(sizes[first], np.bincount(comp, minlength=k))
+    # any one-to-one relabelling of the components passes the check
+    perm = rng.permutation(k)
+    assert O.components_check(off, adj, perm[comp] * 7 - 3)
+    if k > 1:
+        merged = comp.copy()
+        merged[comp == 1] = 0
+        assert not O.components_check(off, adj, merged)
