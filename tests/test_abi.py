@@ -61,6 +61,11 @@ def test_invalid_arguments_rejected_without_device():
     assert L.bd_graph_rmat(0, 16, 0.57, 0.19, 0.19, 0.05, 0, 0, ctypes.byref(h)) == -1
     assert L.bd_graph_rmat(10, 16, 0.57, 0.19, 0.19, 0.05, 0, 7, ctypes.byref(h)) == -1
     assert L.bd_bfs_create(None, None, ctypes.byref(h)) == -1
+    assert L.bd_components_create(None, ctypes.byref(h)) == -1
+    assert L.bd_components_run(None, None) == -1
+    ok, bad = ctypes.c_int32(), ctypes.c_int64()
+    assert L.bd_graph_check_parents(None, 0, None, ctypes.byref(ok), ctypes.byref(bad)) == -1
+    assert L.bd_graph_check_components(None, None, ctypes.byref(ok), ctypes.byref(bad)) == -1
 
 
 def test_cpp_facade_reads_the_trained_policies(tmp_path):
@@ -132,3 +137,21 @@ def test_cpp_facade_reads_the_tuning_file(tmp_path):
                [b.get("alpha", 4)] + [b.get(k, 0) for k in ("block_size", "large_degree", "chunk_edges",
                                                              "pull_prefix", "heavy_degree", "heavy_chunk")]
         assert out == want, (n, out, want)
+
+
+def test_clis_fail_loudly_without_a_device():
+    """Both CLIs exit non-zero with the library's no-device status: there is
+    no CPU path behind them."""
+    import subprocess
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    for name in ("hybrid_bfs", "components"):
+        cli = os.path.join(ROOT, "beedrill_b200", "bin", name)
+        if not os.path.exists(cli):
+            pytest.skip("CLIs not built")
+        out = subprocess.run([cli, "--rmat_scale", "8"], stdout=subprocess.PIPE,
+                             stderr=subprocess.STDOUT, text=True, timeout=120)
+        assert out.returncode != 0, (name, out.stdout)
+        assert "device" in out.stdout.lower(), (name, out.stdout)
+        assert "Found" not in out.stdout and "Traversed" not in out.stdout
