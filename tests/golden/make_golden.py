@@ -23,8 +23,12 @@ What it writes, and where each number comes from:
   (scale 12, edge factor 2, seed 5) and a 48 x 48 grid with 30 % of its
   edges deleted (seed 3).  Per graph: the CSR, the labels parsed from the
   reference's dump, its component count, iteration count and check()
-  verdict.  `python tests/golden/make_golden.py --components` rewrites
-  only this file.
+  verdict; and a set of planted labellings (a vertex relabelled, two
+  components merged under one label, arbitrary distinct labels, two labels
+  swapped, one label for all, an isolated vertex given a used label) with
+  the verdict of the reference's own components::check on each
+  (oracle/_ref/ref_components_check).  `python tests/golden/make_golden.py
+  --components` rewrites only this file.
 * golden.json -- hashes and per-root summaries: sha256 of the generator's
   el64 files (scale 12 and 16), and for scale 16 (seed 16, 8 roots of lcg(0))
   the reference's m_c, per-step discovered counts, per-level directions and
@@ -121,6 +125,45 @@ def ref_components(el64, n):
     return labels, count, iters, passed
 
 
+def planted_labellings(off, good):
+    """Correct and wrong labellings of one graph, made from its labels."""
+    uniq, counts = np.unique(good, return_counts=True)
+    big = int(uniq[np.argmax(counts)])
+    other = int(uniq[uniq != big][0])
+    members = np.flatnonzero(good == big)
+    out = [good.copy()]
+    bad = good.copy()
+    bad[members[len(members) // 2]] = -7
+    out.append(bad)
+    bad = good.copy()
+    bad[good == other] = big
+    out.append(bad)
+    out.append(good * 3 + (1 << 40))
+    bad = good.copy()
+    bad[good == big], bad[good == other] = other, big
+    out.append(bad)
+    out.append(np.zeros_like(good))
+    isolated = np.flatnonzero(np.diff(off) == 0)
+    if len(isolated):
+        bad = good.copy()
+        bad[isolated[-1]] = big
+        out.append(bad)
+    return np.stack(out)
+
+
+def ref_components_check(el64, planted, tmp):
+    path = os.path.join(tmp, "planted.bin")
+    with open(path, "wb") as f:
+        f.write(np.array(planted.shape, np.int64).tobytes())
+        f.write(np.ascontiguousarray(planted, np.int64).tobytes())
+    out = subprocess.run([os.path.join(O.REF_DIR, "ref_components_check"), "--graph_filename",
+                          el64, "--labels", path], check=True, stdout=subprocess.PIPE,
+                         stderr=subprocess.DEVNULL, text=True).stdout
+    verdicts = [int(v) for v in re.findall(r"VERDICT (\d)", out)]
+    assert len(verdicts) == len(planted)
+    return np.array(verdicts, np.int64)
+
+
 def components_fixture(tmp):
     graphs = {"scale10": O.el64_load(os.path.join(HERE, "graph500-scale10.el64")),
               "rmat12_ef2": O.rmat_graph(12, edge_factor=2, seed=5),
@@ -131,8 +174,11 @@ def components_fixture(tmp):
         O.el64_write(el, n, src, dst)
         off, adj = O.csr_build(n, src, dst)
         labels, count, iters, passed = ref_components(el, n)
+        planted = planted_labellings(off, labels)
         arrays.update({f"{name}.offsets": off, f"{name}.adj": adj, f"{name}.labels": labels,
-                       f"{name}.summary": np.array([count, iters, int(passed)], np.int64)})
+                       f"{name}.summary": np.array([count, iters, int(passed)], np.int64),
+                       f"{name}.planted": planted,
+                       f"{name}.planted_verdict": ref_components_check(el, planted, tmp)})
     np.savez_compressed(os.path.join(HERE, "ref_components.npz"), **arrays)
 
 

@@ -4,7 +4,8 @@ Labels must equal the reference's exactly (each vertex labelled with the
 smallest id of its component): against the reference's own output on the
 fixture graphs (tests/golden/ref_components.npz), and against the oracle's
 restatement of components::run elsewhere.  The device check() must give the
-oracle's verdict on correct and planted-wrong labellings.  At RMAT scale 24
+reference's own verdict on the fixtures' planted labellings and the
+oracle's elsewhere, on correct and wrong labellings alike.  At RMAT scale 24
 size-independent properties stand in: labels are minimum ids and fixed
 points, sizes add up, the count equals the number of distinct labels,
 check() passes, and a BFS from any vertex reaches exactly its label's
@@ -52,6 +53,9 @@ def test_labels_equal_the_reference(name):
         assert np.array_equal(labels, want), name
         assert k == count and ok
         assert np.array_equal(sizes, np.bincount(want, minlength=len(want)))
+        # the reference's own check() verdicts on planted labellings
+        for i, (lab, v) in enumerate(zip(ref[f"{name}.planted"], ref[f"{name}.planted_verdict"])):
+            assert g.check_components(lab)[0] == bool(v), (name, i)
         g.close()
 
 

@@ -3,10 +3,11 @@
 tests/golden/ref_components.npz holds what the reference's components CLI
 (components_main.cc, built from its sources by oracle/Makefile) printed on
 three graphs: labels (from --dump_results), component count, iteration
-count and its check() verdict.  The oracle's restatement of
+count and its check() verdict, plus the verdicts of the reference's own
+components::check on planted labellings.  The oracle's restatement of
 components::run must reproduce all of them, and its restatement of
-components::check must accept exactly the labellings the reference's rule
-accepts.  CPU only.
+components::check must give the reference's verdict on every labelling.
+CPU only.
 """
 import os
 
@@ -35,6 +36,17 @@ def test_components_match_the_reference(ref, name):
     assert passed == 1 and O.components_check(off, adj, labels)
     assert sizes.sum() == len(labels) and int((sizes > 0).sum()) == k
     assert np.array_equal(np.flatnonzero(sizes), np.unique(labels))
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_check_verdicts_equal_the_reference(ref, name):
+    """The oracle's components::check gives the reference's own verdict
+    (oracle/_ref/ref_components_check) on every planted labelling."""
+    off, adj = ref[f"{name}.offsets"], ref[f"{name}.adj"]
+    planted, want = ref[f"{name}.planted"], ref[f"{name}.planted_verdict"]
+    assert len(planted) >= 6 and want.min() == 0 and want.max() == 1
+    for i, (lab, v) in enumerate(zip(planted, want)):
+        assert O.components_check(off, adj, lab) == bool(v), i
 
 
 @pytest.mark.parametrize("name", NAMES)
