@@ -29,6 +29,16 @@ What it writes, and where each number comes from:
   the verdict of the reference's own components::check on each
   (oracle/_ref/ref_components_check).  `python tests/golden/make_golden.py
   --components` rewrites only this file.
+* ref_check.npz -- hybrid_bfs::check run by the reference itself
+  (oracle/_ref/ref_check) on parent arrays of graph500-scale10.el64: the
+  reference's beamer_hybrid tree of each of its 8 roots, and for each root
+  the same tree with planted mistakes (a parent that is no neighbour, a
+  neighbour on the same level or one level down, a reached vertex without a
+  parent, a vertex its own parent, parent ids past n, an unreached vertex
+  with a parent, a source that is not its own parent, two mistakes at
+  once).  Per record: source, parents, the reference's verdict and the
+  vertex its LOG lines name (where its loop stops; -1 on PASS).
+  `python tests/golden/make_golden.py --check` rewrites only this file.
 * golden.json -- hashes and per-root summaries: sha256 of the generator's
   el64 files (scale 12 and 16), and for scale 16 (seed 16, 8 roots of lcg(0))
   the reference's m_c, per-step discovered counts, per-level directions and
@@ -125,6 +135,87 @@ def ref_components(el64, n):
     return labels, count, iters, passed
 
 
+def planted_parents(off, adj, root, good, rng):
+    """The reference tree of one root and copies with mistakes planted."""
+    n = len(off) - 1
+    depth = O.bfs_depth(off, adj, root)
+    reached = np.flatnonzero(depth > 1)
+    v = int(rng.choice(reached))
+    nbrs = adj[off[v]:off[v + 1]].astype(np.int64)
+    out = [good.copy()]
+
+    def plant(changes):
+        bad = good.copy()
+        for u, p in changes:
+            bad[u] = p
+        out.append(bad)
+
+    non = np.setdiff1d(np.arange(n), nbrs)
+    plant([(v, int(non[non != v][0]))])
+    for d in (depth[v], depth[v] + 1):
+        cand = nbrs[depth[nbrs] == d]
+        if len(cand):
+            plant([(v, int(cand[0]))])
+    plant([(v, -1)])
+    plant([(v, v)])
+    plant([(v, n + 5)])
+    unreached = np.flatnonzero(depth < 0)
+    if len(unreached):
+        plant([(int(unreached[-1]), root)])
+    plant([(root, int(adj[off[root]]))])
+    w = int(rng.choice(reached[reached != v]))
+    plant([(v, -1), (w, -1)])
+    return out
+
+
+def ref_check(el64, sources, parents, tmp):
+    """Verdict and stopping vertex of the reference's own check() per record."""
+    path = os.path.join(tmp, "parents.bin")
+    n = parents.shape[1]
+    with open(path, "wb") as f:
+        f.write(np.array([len(sources), n], np.int64).tobytes())
+        for s, p in zip(sources, parents):
+            f.write(np.int64(s).tobytes())
+            f.write(np.ascontiguousarray(p, np.int64).tobytes())
+    out = subprocess.run([os.path.join(O.REF_DIR, "ref_check"), "--graph_filename", el64,
+                          "--parents", path], check=True, stdout=subprocess.PIPE,
+                         stderr=subprocess.DEVNULL, text=True).stdout
+    verdict, stop = [], []
+    for i, block in enumerate(out.split("BEGIN ")[1:]):
+        m = re.search(r"VERDICT (\d+) (\d)", block)
+        assert m and int(m.group(1)) == i
+        ok = int(m.group(2))
+        where = -1
+        if not ok:
+            if "Source wrong" in block:
+                where = int(sources[i])
+            else:
+                e = re.search(r"Couldn't find edge from -?\d+ to (\d+)", block)
+                r = re.search(r"Reachability mismatch: depth\[(\d+)\]", block)
+                where = int((e or r).group(1))
+        verdict.append(ok)
+        stop.append(where)
+    assert len(verdict) == len(sources)
+    return np.array(verdict, np.int64), np.array(stop, np.int64)
+
+
+def check_fixture(tmp):
+    el10 = os.path.join(HERE, "graph500-scale10.el64")
+    ref = np.load(os.path.join(HERE, "ref_scale10.npz"))
+    off, adj = ref["offsets"], ref["adj"].astype(np.uint32)
+    rng = np.random.default_rng(281)
+    sources, parents = [], []
+    for root, good in zip(ref["beamer_hybrid.roots"], ref["beamer_hybrid.parent"]):
+        for p in planted_parents(off, adj, int(root), good, rng):
+            sources.append(int(root))
+            parents.append(p)
+    sources = np.array(sources, np.int64)
+    parents = np.stack(parents)
+    verdict, stop = ref_check(el10, sources, parents, tmp)
+    np.savez_compressed(os.path.join(HERE, "ref_check.npz"), sources=sources, parents=parents,
+                        verdict=verdict, stop=stop)
+
+
 def planted_labellings(off, good):
     """Correct and wrong labellings of one graph, made from its labels."""
     uniq, counts = np.unique(good, return_counts=True)
@@ -184,9 +275,12 @@ def components_fixture(tmp):
 
 def main():
     O.build()
-    if "--components" in sys.argv[1:]:
+    if "--components" in sys.argv[1:] or "--check" in sys.argv[1:]:
         with tempfile.TemporaryDirectory() as tmp:
-            components_fixture(tmp)
+            if "--components" in sys.argv[1:]:
+                components_fixture(tmp)
+            if "--check" in sys.argv[1:]:
+                check_fixture(tmp)
         return
     if not os.path.exists(os.path.join(O.REF_DIR, "ref_dump")):
         sys.exit("reference builds missing: the reference sources are needed")
@@ -247,6 +341,7 @@ def main():
             "alpha": 15, "beta": 18, "roots": roots,
         }
         components_fixture(tmp)
+        check_fixture(tmp)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
         f.write("\n")

@@ -74,6 +74,19 @@ def test_check_parents_matches_the_serial_check(order):
     g.close()
 
 
+def test_check_parents_equals_the_reference_check():
+    """The reference's own check() (tests/golden/ref_check.npz) on its trees
+    of graph500-scale10 and on copies with planted mistakes: same verdict,
+    and the reported vertex is the one its LOG lines name."""
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    d = np.load(os.path.join(here, "golden", "ref_check.npz"))
+    g = bd.Graph.from_el64(os.path.join(here, "golden", "graph500-scale10.el64"))
+    for i, (s, p, v, w) in enumerate(zip(d["sources"], d["parents"], d["verdict"], d["stop"])):
+        assert g.check_parents(int(s), p) == (bool(v), int(w)), i
+    g.close()
+
+
 def test_check_parents_small_graphs():
     # no edges: only the source is reached
     g = bd.Graph.from_edges(5, np.zeros(0, np.int64), np.zeros(0, np.int64))

@@ -135,6 +135,18 @@ def test_scale16_depths_and_sequences(golden):
         assert O.count_traversed(off, mp) == r["m_c"]
 
 
+def test_check_equals_the_reference_check_on_planted_trees(scale10, golden_dir):
+    """Verdict and stopping vertex of the oracle's check() equal the
+    reference's own check() (oracle/_ref/ref_check, its LOG lines) on the
+    reference's trees and on 63 copies with planted mistakes."""
+    n, src, dst, off, adj, ref = scale10
+    d = np.load(os.path.join(golden_dir, "ref_check.npz"))
+    assert len(d["sources"]) > 60 and d["verdict"].sum() == 8
+    for i, (s, p, v, w) in enumerate(zip(d["sources"], d["parents"], d["verdict"], d["stop"])):
+        assert O.check(off, adj, int(s), p) == bool(v), i
+        assert O.check_first_bad(off, adj, int(s), p) == w, i
+
+
 def test_check_rejects_planted_mistakes(scale10):
     """Mistakes planted in a parent array on the CPU must fail check()."""
     n, src, dst, off, adj, ref = scale10
