@@ -523,6 +523,35 @@ private:
     bd_run_stats stats_{};
 };
 
+namespace detail {
+// components::dump's text (components.cc:120-152): for each label in
+// ascending order, "Component <label>: " and its vertices as ranges
+// ("a-b" or "a"), comma separated.  Labels must lie in [0, n).
+inline void print_components(const std::vector<int64_t> &c, FILE *out)
+{
+    std::vector<std::vector<int64_t>> members(c.size());
+    for (size_t v = 0; v < c.size(); ++v) { members[(size_t)c[v]].push_back((int64_t)v); }
+    for (size_t l = 0; l < members.size(); ++l) {
+        const std::vector<int64_t> &m = members[l];
+        if (m.empty()) { continue; }
+        fprintf(out, "Component %zu: ", l);
+        for (size_t i = 0; i < m.size();) {
+            size_t j = i;
+            while (j + 1 < m.size() && m[j + 1] == m[j] + 1) { ++j; }
+            if (i) { fprintf(out, ", "); }
+            if (j == i) {
+                fprintf(out, "%li", (long)m[i]);
+            } else {
+                fprintf(out, "%li-%li", (long)m[i], (long)m[j]);
+            }
+            i = j + 1;
+        }
+        fprintf(out, "\n");
+    }
+    fflush(out);
+}
+}  // namespace detail
+
 // The reference's `components` class (components.h:6-33): run() labels
 // every vertex with the smallest id of its component.
 class components {
@@ -564,30 +593,7 @@ public:
         return s;
     }
     // components::dump (components.cc:120-152): per label, its vertices as ranges.
-    void dump()
-    {
-        const std::vector<int64_t> c = component();
-        std::vector<std::vector<int64_t>> members(c.size());
-        for (size_t v = 0; v < c.size(); ++v) { members[(size_t)c[v]].push_back((int64_t)v); }
-        for (size_t l = 0; l < members.size(); ++l) {
-            const std::vector<int64_t> &m = members[l];
-            if (m.empty()) { continue; }
-            printf("Component %zu: ", l);
-            for (size_t i = 0; i < m.size();) {
-                size_t j = i;
-                while (j + 1 < m.size() && m[j + 1] == m[j] + 1) { ++j; }
-                if (i) { printf(", "); }
-                if (j == i) {
-                    printf("%li", (long)m[i]);
-                } else {
-                    printf("%li-%li", (long)m[i], (long)m[j]);
-                }
-                i = j + 1;
-            }
-            printf("\n");
-        }
-        fflush(stdout);
-    }
+    void dump() { detail::print_components(component(), stdout); }
     const stats &last_stats() const { return stats_; }
     bd_components *handle() const { return h_; }
 

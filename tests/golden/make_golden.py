@@ -23,7 +23,7 @@ What it writes, and where each number comes from:
   (scale 12, edge factor 2, seed 5) and a 48 x 48 grid with 30 % of its
   edges deleted (seed 3).  Per graph: the CSR, the labels parsed from the
   reference's dump, its component count, iteration count and check()
-  verdict; and a set of planted labellings (a vertex relabelled, two
+  verdict, the text of its --dump_results; and a set of planted labellings (a vertex relabelled, two
   components merged under one label, arbitrary distinct labels, two labels
   swapped, one label for all, an isolated vertex given a used label) with
   the verdict of the reference's own components::check on each
@@ -132,7 +132,8 @@ def ref_components(el64, n):
                 lo, _, hi = part.partition("-")
                 labels[int(lo): int(hi or lo) + 1] = c
     assert (labels >= 0).all() and count is not None and passed is not None
-    return labels, count, iters, passed
+    dump = "".join(line + "\n" for line in out.splitlines() if line.startswith("Component "))
+    return labels, count, iters, passed, dump
 
 
 def planted_parents(off, adj, root, good, rng):
@@ -264,10 +265,11 @@ def components_fixture(tmp):
         el = os.path.join(tmp, name + ".el64")
         O.el64_write(el, n, src, dst)
         off, adj = O.csr_build(n, src, dst)
-        labels, count, iters, passed = ref_components(el, n)
+        labels, count, iters, passed, dump = ref_components(el, n)
         planted = planted_labellings(off, labels)
         arrays.update({f"{name}.offsets": off, f"{name}.adj": adj, f"{name}.labels": labels,
                        f"{name}.summary": np.array([count, iters, int(passed)], np.int64),
+                       f"{name}.dump": np.frombuffer(dump.encode(), np.uint8),
                        f"{name}.planted": planted,
                        f"{name}.planted_verdict": ref_components_check(el, planted, tmp)})
     np.savez_compressed(os.path.join(HERE, "ref_components.npz"), **arrays)

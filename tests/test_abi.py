@@ -155,3 +155,32 @@ def test_clis_fail_loudly_without_a_device():
         assert out.returncode != 0, (name, out.stdout)
         assert "device" in out.stdout.lower(), (name, out.stdout)
         assert "Found" not in out.stdout and "Traversed" not in out.stdout
+
+
+def test_cpp_facade_dump_text_equals_the_reference(tmp_path):
+    """components::dump text (the CLI's --dump_results) from the facade's
+    printer equals, byte for byte, what the reference's own components CLI
+    printed for the same labels (tests/golden/ref_components.npz)."""
+    import subprocess
+    import numpy as np
+    src = tmp_path / "dump.cc"
+    src.write_text(
+        '#include "beedrill/hybrid_bfs.hpp"\n'
+        'int main(int argc, char **argv) {\n'
+        '  FILE *f = fopen(argv[1], "rb"); int64_t n = 0;\n'
+        '  if (!f || fread(&n, 8, 1, f) != 1) return 2;\n'
+        '  std::vector<int64_t> c(n);\n'
+        '  if (fread(c.data(), 8, n, f) != (size_t)n) return 2;\n'
+        '  fclose(f); beedrill::detail::print_components(c, stdout); return 0; }\n')
+    exe = tmp_path / "dump"
+    lib_dir = os.path.dirname(bd.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe), "-L", lib_dir, "-lbeedrill_b200",
+                    f"-Wl,-rpath,{lib_dir}"], check=True)
+    ref = np.load(os.path.join(ROOT, "tests", "golden", "ref_components.npz"))
+    for name in ("scale10", "rmat12_ef2", "grid48"):
+        labels = ref[f"{name}.labels"]
+        path = tmp_path / f"{name}.bin"
+        path.write_bytes(np.int64(len(labels)).tobytes() + labels.astype(np.int64).tobytes())
+        out = subprocess.run([str(exe), str(path)], check=True, stdout=subprocess.PIPE).stdout
+        assert out == bytes(ref[f"{name}.dump"]), name

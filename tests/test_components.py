@@ -167,3 +167,5 @@ def test_cli_matches_the_reference_output():
                 lo, _, hi = part.partition("-")
                 labels[int(lo): int(hi or lo) + 1] = int(m.group(1))
     assert np.array_equal(labels, ref["scale10.labels"])
+    dump = "".join(line + "\n" for line in text.splitlines() if line.startswith("Component "))
+    assert dump.encode() == bytes(ref["scale10.dump"])
