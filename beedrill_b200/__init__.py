@@ -26,7 +26,7 @@ from ctypes import (POINTER, Structure, byref, c_char_p, c_double, c_float, c_in
 import numpy as np
 
 __all__ = ["BeedrillError", "Graph", "HybridBFS", "BatchedBFS", "Components", "Step", "ALGORITHMS", "lib", "LIB_PATH",
-           "tuned_options",
+           "tuned_options", "format_tree",
            "policy_forward", "policy_loss_grad", "policy_train"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -499,18 +499,7 @@ class HybridBFS:
 
     # hybrid_bfs::print_tree (hybrid_bfs.cc:381-399)
     def print_tree(self) -> None:
-        parent = self.parents()
-        for v in range(len(parent)):
-            p = int(parent[v])
-            if p < 0:
-                continue
-            line = f"{v:4d}"
-            while True:
-                line += f" <- {p:4d}"
-                if p == -1 or p == parent[p]:
-                    break
-                p = int(parent[p])
-            print(line)
+        print(format_tree(self.parents()), end="")
 
     def set_policy(self, params, mean, inv_std, margin: float = 0.0, lo=None, hi=None) -> None:
         """Install the learned direction policy used by alg="learned"
@@ -630,6 +619,26 @@ class BatchedBFS:
             self.close()
         except Exception:
             pass
+
+
+def format_tree(parent) -> str:
+    """hybrid_bfs::print_tree's text (hybrid_bfs.cc:381-399) for a parent
+    array in the reference's encoding: each vertex with a parent and its
+    ancestors up to the root, "%4li <- %4li <- ..." per line."""
+    n = len(parent)
+    lines = []
+    for v in range(n):
+        p = int(parent[v])
+        if p < 0:
+            continue
+        line = f"{v:4d}"
+        while True:
+            line += f" <- {p:4d}"
+            if p < 0 or p >= n or p == parent[p]:
+                break
+            p = int(parent[p])
+        lines.append(line + "\n")
+    return "".join(lines)
 
 
 class Components:

@@ -354,6 +354,57 @@ private:
     bd_graph *h_ = nullptr;
 };
 
+namespace detail {
+// hybrid_bfs::print_tree's text (hybrid_bfs.cc:381-399): for each vertex
+// with a parent, the vertex and its ancestors up to the root,
+// "%4li <- %4li <- ...".  A chain that meets a negative entry stops there
+// (the reference would index with it).
+inline void print_tree(const std::vector<int64_t> &p, FILE *out)
+{
+    const long n = (long)p.size();
+    for (long v = 0; v < n; ++v) {
+        long parent = (long)p[v];
+        if (parent < 0) { continue; }
+        fprintf(out, "%4li", v);
+        while (true) {
+            fprintf(out, " <- %4li", parent);
+            if (parent < 0 || parent >= n) { break; }
+            if (parent == p[parent]) { break; }
+            parent = (long)p[parent];
+        }
+        fprintf(out, "\n");
+    }
+    fflush(out);
+}
+
+// components::dump's text (components.cc:120-152): for each label in
+// ascending order, "Component <label>: " and its vertices as ranges
+// ("a-b" or "a"), comma separated.  Labels must lie in [0, n).
+inline void print_components(const std::vector<int64_t> &c, FILE *out)
+{
+    std::vector<std::vector<int64_t>> members(c.size());
+    for (size_t v = 0; v < c.size(); ++v) { members[(size_t)c[v]].push_back((int64_t)v); }
+    for (size_t l = 0; l < members.size(); ++l) {
+        const std::vector<int64_t> &m = members[l];
+        if (m.empty()) { continue; }
+        fprintf(out, "Component %zu: ", l);
+        for (size_t i = 0; i < m.size();) {
+            size_t j = i;
+            while (j + 1 < m.size() && m[j + 1] == m[j] + 1) { ++j; }
+            if (i) { fprintf(out, ", "); }
+            if (j == i) {
+                fprintf(out, "%li", (long)m[i]);
+            } else {
+                fprintf(out, "%li-%li", (long)m[i], (long)m[j]);
+            }
+            i = j + 1;
+        }
+        fprintf(out, "\n");
+    }
+    fflush(out);
+}
+}  // namespace detail
+
 // hybrid_bfs (hybrid_bfs.h:11-47).
 class hybrid_bfs {
 public:
@@ -415,23 +466,7 @@ public:
         return (long)m;
     }
     // print_tree (hybrid_bfs.cc:381-399)
-    void print_tree()
-    {
-        std::vector<int64_t> p = parents();
-        for (size_t v = 0; v < p.size(); ++v) {
-            long parent = (long)p[v];
-            if (parent < 0) { continue; }
-            printf("%4zu", v);
-            while (true) {
-                printf(" <- %4li", parent);
-                if (parent == -1) { break; }
-                if (parent == p[parent]) { break; }
-                parent = (long)p[parent];
-            }
-            printf("\n");
-        }
-        fflush(stdout);
-    }
+    void print_tree() { detail::print_tree(parents(), stdout); }
     std::vector<int32_t> depths()
     {
         std::vector<int32_t> d(g_.num_vertices());
@@ -522,35 +557,6 @@ private:
     bd_msbfs *h_ = nullptr;
     bd_run_stats stats_{};
 };
-
-namespace detail {
-// components::dump's text (components.cc:120-152): for each label in
-// ascending order, "Component <label>: " and its vertices as ranges
-// ("a-b" or "a"), comma separated.  Labels must lie in [0, n).
-inline void print_components(const std::vector<int64_t> &c, FILE *out)
-{
-    std::vector<std::vector<int64_t>> members(c.size());
-    for (size_t v = 0; v < c.size(); ++v) { members[(size_t)c[v]].push_back((int64_t)v); }
-    for (size_t l = 0; l < members.size(); ++l) {
-        const std::vector<int64_t> &m = members[l];
-        if (m.empty()) { continue; }
-        fprintf(out, "Component %zu: ", l);
-        for (size_t i = 0; i < m.size();) {
-            size_t j = i;
-            while (j + 1 < m.size() && m[j + 1] == m[j] + 1) { ++j; }
-            if (i) { fprintf(out, ", "); }
-            if (j == i) {
-                fprintf(out, "%li", (long)m[i]);
-            } else {
-                fprintf(out, "%li-%li", (long)m[i], (long)m[j]);
-            }
-            i = j + 1;
-        }
-        fprintf(out, "\n");
-    }
-    fflush(out);
-}
-}  // namespace detail
 
 // The reference's `components` class (components.h:6-33): run() labels
 // every vertex with the smallest id of its component.

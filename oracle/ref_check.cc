@@ -9,12 +9,14 @@
 // ref_dump.cc, the reference's headers are included with `private` opened
 // for writing the array before check() runs.
 //
-//   ref_check --graph_filename G --parents P
+//   ref_check --graph_filename G --parents P [--print_tree]
 //
 // P (little endian): int64 k, int64 n, then k records of int64 source and
 // int64 parent[n].  For record i the output is the line "BEGIN i", whatever
 // the reference's check() logs (its LOG lines name the vertex it stops at),
-// then "VERDICT i <0|1>".
+// then "VERDICT i <0|1>".  With --print_tree, print_tree()
+// (hybrid_bfs.cc:381-399) runs instead of check(): "BEGIN i", the tree's
+// text, "END i".
 #include <getopt.h>
 
 #include <algorithm>
@@ -47,9 +49,11 @@ int main(int argc, char **argv)
 {
     const char *graph_path = nullptr;
     const char *parents_path = nullptr;
+    bool tree = false;
     static const struct option opts[] = {
         {"graph_filename", required_argument, nullptr, 'g'},
         {"parents", required_argument, nullptr, 'p'},
+        {"print_tree", no_argument, nullptr, 't'},
         {nullptr, 0, nullptr, 0},
     };
     int c, idx;
@@ -57,6 +61,7 @@ int main(int argc, char **argv)
         switch (c) {
             case 'g': graph_path = optarg; break;
             case 'p': parents_path = optarg; break;
+            case 't': tree = true; break;
             default: die("bad arguments");
         }
     }
@@ -83,6 +88,12 @@ int main(int argc, char **argv)
         for (long v = 0; v < n; ++v) { bfs->parent_[v] = parent[v]; }
         printf("BEGIN %ld\n", (long)i);
         fflush(stdout);
+        if (tree) {
+            bfs->print_tree();
+            printf("END %ld\n", (long)i);
+            fflush(stdout);
+            continue;
+        }
         const bool ok = bfs->check(source);
         printf("VERDICT %ld %d\n", (long)i, ok ? 1 : 0);
         fflush(stdout);

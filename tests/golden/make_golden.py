@@ -37,7 +37,8 @@ What it writes, and where each number comes from:
   parent, a vertex its own parent, parent ids past n, an unreached vertex
   with a parent, a source that is not its own parent, two mistakes at
   once).  Per record: source, parents, the reference's verdict and the
-  vertex its LOG lines name (where its loop stops; -1 on PASS).
+  vertex its LOG lines name (where its loop stops; -1 on PASS); and the
+  text of the reference's print_tree() for each of the 8 trees.
   `python tests/golden/make_golden.py --check` rewrites only this file.
 * golden.json -- hashes and per-root summaries: sha256 of the generator's
   el64 files (scale 12 and 16), and for scale 16 (seed 16, 8 roots of lcg(0))
@@ -169,15 +170,32 @@ def planted_parents(off, adj, root, good, rng):
     return out
 
 
-def ref_check(el64, sources, parents, tmp):
-    """Verdict and stopping vertex of the reference's own check() per record."""
-    path = os.path.join(tmp, "parents.bin")
-    n = parents.shape[1]
+def write_parents(path, sources, parents):
     with open(path, "wb") as f:
-        f.write(np.array([len(sources), n], np.int64).tobytes())
+        f.write(np.array([len(sources), parents.shape[1]], np.int64).tobytes())
         for s, p in zip(sources, parents):
             f.write(np.int64(s).tobytes())
             f.write(np.ascontiguousarray(p, np.int64).tobytes())
+
+
+def ref_print_tree(el64, sources, parents, tmp):
+    """The text of the reference's own print_tree() for each parent array."""
+    path = os.path.join(tmp, "trees.bin")
+    write_parents(path, sources, parents)
+    out = subprocess.run([os.path.join(O.REF_DIR, "ref_check"), "--graph_filename", el64,
+                          "--parents", path, "--print_tree"], check=True, stdout=subprocess.PIPE,
+                         stderr=subprocess.DEVNULL, text=True).stdout
+    texts = []
+    for i in range(len(sources)):
+        head, tail = f"BEGIN {i}\n", f"END {i}\n"
+        texts.append(out[out.index(head) + len(head): out.index(tail)])
+    return texts
+
+
+def ref_check(el64, sources, parents, tmp):
+    """Verdict and stopping vertex of the reference's own check() per record."""
+    path = os.path.join(tmp, "parents.bin")
+    write_parents(path, sources, parents)
     out = subprocess.run([os.path.join(O.REF_DIR, "ref_check"), "--graph_filename", el64,
                           "--parents", path], check=True, stdout=subprocess.PIPE,
                          stderr=subprocess.DEVNULL, text=True).stdout
@@ -213,8 +231,12 @@ def check_fixture(tmp):
     sources = np.array(sources, np.int64)
     parents = np.stack(parents)
     verdict, stop = ref_check(el10, sources, parents, tmp)
+    trees = ref_print_tree(el10, ref["beamer_hybrid.roots"], ref["beamer_hybrid.parent"], tmp)
+    tree_bytes = [t.encode() for t in trees]
     np.savez_compressed(os.path.join(HERE, "ref_check.npz"), sources=sources, parents=parents,
-                        verdict=verdict, stop=stop)
+                        verdict=verdict, stop=stop,
+                        tree_text=np.frombuffer(b"".join(tree_bytes), np.uint8),
+                        tree_offsets=np.cumsum([0] + [len(b) for b in tree_bytes]).astype(np.int64))
 
 
 def planted_labellings(off, good):

@@ -184,3 +184,45 @@ def test_cpp_facade_dump_text_equals_the_reference(tmp_path):
         path.write_bytes(np.int64(len(labels)).tobytes() + labels.astype(np.int64).tobytes())
         out = subprocess.run([str(exe), str(path)], check=True, stdout=subprocess.PIPE).stdout
         assert out == bytes(ref[f"{name}.dump"]), name
+
+
+def test_cpp_facade_print_tree_equals_the_reference(tmp_path):
+    """hybrid_bfs::print_tree text from the facade's printer equals, byte for
+    byte, the reference's own print_tree() on its 8 scale-10 trees
+    (tests/golden/ref_check.npz)."""
+    import subprocess
+    import numpy as np
+    src = tmp_path / "tree.cc"
+    src.write_text(
+        '#include "beedrill/hybrid_bfs.hpp"\n'
+        'int main(int argc, char **argv) {\n'
+        '  FILE *f = fopen(argv[1], "rb"); int64_t n = 0;\n'
+        '  if (!f || fread(&n, 8, 1, f) != 1) return 2;\n'
+        '  std::vector<int64_t> p(n);\n'
+        '  if (fread(p.data(), 8, n, f) != (size_t)n) return 2;\n'
+        '  fclose(f); beedrill::detail::print_tree(p, stdout); return 0; }\n')
+    exe = tmp_path / "tree"
+    lib_dir = os.path.dirname(bd.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe), "-L", lib_dir, "-lbeedrill_b200",
+                    f"-Wl,-rpath,{lib_dir}"], check=True)
+    golden = os.path.join(ROOT, "tests", "golden")
+    trees = np.load(os.path.join(golden, "ref_scale10.npz"))["beamer_hybrid.parent"]
+    d = np.load(os.path.join(golden, "ref_check.npz"))
+    text, off = bytes(d["tree_text"]), d["tree_offsets"]
+    assert len(off) == len(trees) + 1
+    for i, parent in enumerate(trees):
+        path = tmp_path / f"p{i}.bin"
+        path.write_bytes(np.int64(len(parent)).tobytes() + parent.astype(np.int64).tobytes())
+        out = subprocess.run([str(exe), str(path)], check=True, stdout=subprocess.PIPE).stdout
+        assert out == text[off[i]:off[i + 1]], i
+
+
+def test_python_print_tree_text_equals_the_reference():
+    import numpy as np
+    golden = os.path.join(ROOT, "tests", "golden")
+    trees = np.load(os.path.join(golden, "ref_scale10.npz"))["beamer_hybrid.parent"]
+    d = np.load(os.path.join(golden, "ref_check.npz"))
+    text, off = bytes(d["tree_text"]), d["tree_offsets"]
+    for i, parent in enumerate(trees):
+        assert bd.format_tree(parent).encode() == text[off[i]:off[i + 1]], i
