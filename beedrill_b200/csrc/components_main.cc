@@ -10,6 +10,7 @@
 // (one iteration here: a single pass over the arcs).
 #include <getopt.h>
 
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -107,6 +108,18 @@ components_args parse(int argc, char **argv)
     return a;
 }
 
+// The reference's load line (hybrid_bfs_main.cc:175-178, components_main.cc:
+// 133-136): edges, time, and MB/s of 16-byte edges; here the time covers
+// reading or generating the edges and building the CSR on the device.
+void print_loaded(const beedrill::graph &g, std::chrono::steady_clock::time_point t0)
+{
+    const double ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    const long m = g.num_edges();
+    printf("Loaded %li edges in %3.2f ms, %3.2f MB/s\n", m, ms, (1e-6 * m * 16) / (1e-3 * ms));
+    printf("Graph has %li vertices\n", g.num_vertices());
+}
+
 }  // namespace
 
 int main(int argc, char **argv)
@@ -114,10 +127,11 @@ int main(int argc, char **argv)
     bool success = true;
     const components_args args = parse(argc, argv);
     try {
+        const auto t_load = std::chrono::steady_clock::now();
         beedrill::graph g = args.rmat_scale > 0
                                 ? beedrill::graph::rmat(args.rmat_scale, args.edge_factor, args.seed)
                                 : beedrill::graph::from_el64(args.graph_filename);
-        printf("Loaded %li edges, %li vertices\n", g.num_edges(), g.num_vertices());
+        print_loaded(g, t_load);
         if (args.dump_edge_list || args.dump_graph) {
             std::vector<int64_t> off;
             std::vector<uint32_t> adj;
