@@ -624,20 +624,26 @@ class BatchedBFS:
 def format_tree(parent) -> str:
     """hybrid_bfs::print_tree's text (hybrid_bfs.cc:381-399) for a parent
     array in the reference's encoding: each vertex with a parent and its
-    ancestors up to the root, "%4li <- %4li <- ..." per line."""
+    ancestors up to the root, "%4li <- %4li <- ..." per line.  A chain that
+    meets a negative or out-of-range entry stops there (the reference would
+    index with it); a chain that climbs n times without reaching a root is
+    a cycle (the reference would loop forever) and its line ends with
+    " <- (cycle)"."""
     n = len(parent)
     lines = []
     for v in range(n):
         p = int(parent[v])
         if p < 0:
             continue
-        line = f"{v:4d}"
-        while True:
-            line += f" <- {p:4d}"
+        parts = [f"{v:4d}"]
+        for _ in range(n + 1):
+            parts.append(f" <- {p:4d}")
             if p < 0 or p >= n or p == parent[p]:
                 break
             p = int(parent[p])
-        lines.append(line + "\n")
+        else:
+            parts.append(" <- (cycle)")
+        lines.append("".join(parts) + "\n")
     return "".join(lines)
 
 

@@ -1531,18 +1531,19 @@ bd_status bd_bfs_destroy(bd_bfs *b)
 // temporary (control block, the two visited bitmaps, the frontier queues)
 // lives in one file-scope device array of fixed size, so graphs are limited
 // to BD_NOALLOC_MAX_VERTICES vertices.  Each GPU that loads this library
-// holds that array (about 4.9 MB) until the process exits.
+// holds that array (about 7.2 MB) until the process exits.
 // ---------------------------------------------------------------------------
 namespace bd {
 namespace {
 
 constexpr int64_t kNaMaxVertices = BD_NOALLOC_MAX_VERTICES;
 constexpr int64_t kNaWords = kNaMaxVertices / 32;
-constexpr int64_t kNaLarge = 1 << 15;  // slots for large-degree frontier vertices
+constexpr int64_t kNaLarge = 1 << 17;  // slots for large-degree frontier vertices
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t kNaOffCtrl = 0;
 constexpr size_t kNaOffSource = align256(kNaOffCtrl + sizeof(Ctrl));
-constexpr size_t kNaOffVis = align256(kNaOffSource + sizeof(int64_t));
+constexpr size_t kNaOffLive = kNaOffSource + sizeof(int64_t);  // vertices of nonzero degree
+constexpr size_t kNaOffVis = align256(kNaOffLive + sizeof(unsigned long long));
 constexpr size_t kNaOffQs = align256(kNaOffVis + 2 * sizeof(uint32_t) * kNaWords);
 constexpr size_t kNaOffQl = align256(kNaOffQs + 2 * sizeof(uint32_t) * kNaMaxVertices);
 constexpr size_t kNaOffQlb = align256(kNaOffQl + 2 * sizeof(uint32_t) * kNaLarge);
@@ -1580,14 +1581,17 @@ bd_status noalloc_setup(int dev, unsigned char **base, int *grid)
     return BD_OK;
 }
 
-// depth = -1; vis[0] = degree-zero and padding bits; the source id.
+// depth = -1; vis[0] = degree-zero and padding bits; the source id; the
+// count of vertices of nonzero degree added into *live (zeroed before).
 __global__ void noalloc_prepare_kernel(const int64_t *off, int64_t n, int32_t *depth,
-                                       uint32_t *vis0, int64_t source, int64_t *source_slot)
+                                       uint32_t *vis0, int64_t source, int64_t *source_slot,
+                                       unsigned long long *live)
 {
     const int64_t words = (n + 31) / 32;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     for (int64_t v = t; v < n; v += stride) { depth[v] = -1; }
+    unsigned long long nz = 0;
     for (int64_t w = t; w < words; w += stride) {
         uint32_t b = 0;
         for (int k = 0; k < 32; ++k) {
@@ -1595,7 +1599,10 @@ __global__ void noalloc_prepare_kernel(const int64_t *off, int64_t n, int32_t *d
             if (v >= n || off[v + 1] == off[v]) { b |= 1u << k; }
         }
         vis0[w] = b;
+        nz += 32 - __popc(b);
     }
+    nz = dev::warp_sum(nz);
+    if (dev::lane_id() == 0 && nz) { atomicAdd(live, nz); }
     if (t == 0) { *source_slot = source; }
 }
 
@@ -1632,9 +1639,9 @@ extern "C" bd_status bd_bfs_run_noalloc(const int64_t *d_offsets, const uint32_t
     p.depth = d_depth;
     p.parent = d_parent;
     p.words = bitmap_words(num_vertices);
-    p.n_live = num_vertices;
     Ctrl *ctrl = reinterpret_cast<Ctrl *>(base + kNaOffCtrl);
     int64_t *source_slot = reinterpret_cast<int64_t *>(base + kNaOffSource);
+    unsigned long long *live = reinterpret_cast<unsigned long long *>(base + kNaOffLive);
     for (int i = 0; i < 2; ++i) {
         p.vis[i] = reinterpret_cast<uint32_t *>(base + kNaOffVis) + i * kNaWords;
         p.qs[i] = reinterpret_cast<uint32_t *>(base + kNaOffQs) + i * kNaMaxVertices;
@@ -1647,19 +1654,29 @@ extern "C" bd_status bd_bfs_run_noalloc(const int64_t *d_offsets, const uint32_t
     p.alg = BD_ALG_BEAMER;
     p.alpha = alpha;
     p.beta = beta;
-    // Large-degree slots: at most num_arcs / large_deg vertices qualify.
-    p.large_deg = (uint32_t)std::max<int64_t>(1024, num_arcs / kNaLarge + 1);
-    p.chunk = 1024;
+    // The regular handle's defaults (bd_bfs_create), except that the
+    // large-degree threshold rises above them on graphs of more than
+    // 32 x kNaLarge arcs: at most num_arcs / large_deg vertices qualify, and
+    // the array holds kNaLarge of them.
+    p.large_deg = (uint32_t)std::max<int64_t>(32, num_arcs / kNaLarge + 1);
+    p.chunk = 256;
     p.bu_prefix = 32;
     p.spin_limit = kDefaultSpin;
     p.expected_ctas = (unsigned)grid;
     p.policy = nullptr;
 
-    // The control block, source slot and vis[0] are rewritten here; the
-    // queues and vis[1] are written before they are read within a run.
+    // The control block, source slot, live count and vis[0] are rewritten
+    // here; the queues and vis[1] are written before they are read within a
+    // run.  The live count (vertices of nonzero degree) decides the
+    // bottom-up layout switch, so it is read back before the launch.
+    BD_CUDA(cudaMemsetAsync(live, 0, sizeof(unsigned long long), s));
     noalloc_prepare_kernel<<<grid_for(std::max<int64_t>(num_vertices, 1)), 256, 0, s>>>(
-        d_offsets, num_vertices, d_depth, p.vis[0], source, source_slot);
+        d_offsets, num_vertices, d_depth, p.vis[0], source, source_slot, live);
     BD_CUDA(cudaGetLastError());
+    unsigned long long n_live = 0;
+    BD_CUDA(cudaMemcpyAsync(&n_live, live, sizeof(n_live), cudaMemcpyDeviceToHost, s));
+    BD_CUDA(cudaStreamSynchronize(s));
+    p.n_live = (int64_t)n_live;
     init_sources_kernel<<<1, 32, 0, s>>>(p, source_slot, 1, 0);
     BD_CUDA(cudaGetLastError());
     KernelChoice kc = pick_kernel(512);

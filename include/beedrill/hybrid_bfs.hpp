@@ -357,8 +357,10 @@ private:
 namespace detail {
 // hybrid_bfs::print_tree's text (hybrid_bfs.cc:381-399): for each vertex
 // with a parent, the vertex and its ancestors up to the root,
-// "%4li <- %4li <- ...".  A chain that meets a negative entry stops there
-// (the reference would index with it).
+// "%4li <- %4li <- ...".  A chain that meets a negative or out-of-range
+// entry stops there (the reference would index with it); a chain that climbs
+// n times without reaching a root is a cycle (the reference would loop
+// forever), and its line ends with " <- (cycle)".
 inline void print_tree(const std::vector<int64_t> &p, FILE *out)
 {
     const long n = (long)p.size();
@@ -366,12 +368,16 @@ inline void print_tree(const std::vector<int64_t> &p, FILE *out)
         long parent = (long)p[v];
         if (parent < 0) { continue; }
         fprintf(out, "%4li", v);
-        while (true) {
+        bool ended = false;
+        for (long climb = 0; climb <= n && !ended; ++climb) {
             fprintf(out, " <- %4li", parent);
-            if (parent < 0 || parent >= n) { break; }
-            if (parent == p[parent]) { break; }
-            parent = (long)p[parent];
+            if (parent < 0 || parent >= n || parent == p[parent]) {
+                ended = true;
+            } else {
+                parent = (long)p[parent];
+            }
         }
+        if (!ended) { fprintf(out, " <- (cycle)"); }
         fprintf(out, "\n");
     }
     fflush(out);
@@ -379,15 +385,21 @@ inline void print_tree(const std::vector<int64_t> &p, FILE *out)
 
 // components::dump's text (components.cc:120-152): for each label in
 // ascending order, "Component <label>: " and its vertices as ranges
-// ("a-b" or "a"), comma separated.  Labels must lie in [0, n).
+// ("a-b" or "a"), comma separated, then a newline.  The reference ends a
+// line only after a range that closed before the last vertex, so a label
+// whose vertices form one range ending at vertex n-1 gets no newline (with
+// minimum-id labels, that is the last line when vertex n-1's component is
+// one contiguous run).  Labels must lie in [0, n).
 inline void print_components(const std::vector<int64_t> &c, FILE *out)
 {
     std::vector<std::vector<int64_t>> members(c.size());
     for (size_t v = 0; v < c.size(); ++v) { members[(size_t)c[v]].push_back((int64_t)v); }
+    const int64_t last_vertex = (int64_t)c.size() - 1;
     for (size_t l = 0; l < members.size(); ++l) {
         const std::vector<int64_t> &m = members[l];
         if (m.empty()) { continue; }
         fprintf(out, "Component %zu: ", l);
+        bool closed_early = false;  // a range ended before the last vertex
         for (size_t i = 0; i < m.size();) {
             size_t j = i;
             while (j + 1 < m.size() && m[j + 1] == m[j] + 1) { ++j; }
@@ -397,9 +409,10 @@ inline void print_components(const std::vector<int64_t> &c, FILE *out)
             } else {
                 fprintf(out, "%li-%li", (long)m[i], (long)m[j]);
             }
+            if (m[j] != last_vertex) { closed_early = true; }
             i = j + 1;
         }
-        fprintf(out, "\n");
+        if (closed_early) { fprintf(out, "\n"); }
     }
     fflush(out);
 }

@@ -221,17 +221,24 @@ bd_status bd_bfs_destroy(bd_bfs *b);
  * default stream), and returns after the stream has finished.
  * traversed_edges (host, may be NULL) gets count_num_traversed_edges().
  *
- * All temporaries live in one fixed device array inside the library, so:
+ * All temporaries live in one fixed device array inside the library (about
+ * 7.2 MB on every GPU that loads it, held until the process exits), so:
  *   - num_vertices must not exceed BD_NOALLOC_MAX_VERTICES (else
  *     BD_ERR_LIMIT, nothing launched);
- *   - the first call on a device looks the array up on that device
- *     (cudaGetSymbolAddress); make that first call before any stream
- *     capture;
+ *   - the first call on a device looks the array's device address up on
+ *     that device (cudaGetSymbolAddress) and keeps it for the life of the
+ *     process: after a cudaDeviceReset of that device the kept address is
+ *     stale, so do not call this entry point again in that process;
+ *   - every call waits for `stream` twice (it reads two counters back), so
+ *     no call may be made while a stream capture is under way;
  *   - every call shares the array: calls that overlap on the GPU (other
  *     streams, other host threads) race and corrupt each other.  Serialise
  *     them.
- * Nothing is allocated or freed; the call uses the device current on the
- * calling thread. */
+ * Launch parameters are the regular handle's defaults (bd_bfs_create),
+ * except that on graphs of more than 4,194,304 arcs the large-degree
+ * threshold rises above 32 (to num_arcs / 131072 + 1) so that its queue fits
+ * the array.  Nothing is allocated or freed; the call uses the device
+ * current on the calling thread. */
 #define BD_NOALLOC_MAX_VERTICES 524288
 bd_status bd_bfs_run_noalloc(const int64_t *d_offsets, const uint32_t *d_adjacency,
                              int64_t num_vertices, int64_t num_arcs, int64_t source,

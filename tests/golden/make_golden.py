@@ -18,12 +18,15 @@ What it writes, and where each number comes from:
   output at scale 12 (seed 12), so parents/levels can be compared at full
   detail on a graph the device generator must reproduce byte for byte.
 * ref_components.npz -- oracle/_ref/components (the reference's
-  connected-components CLI) with --check_results --dump_results on three
+  connected-components CLI) with --check_results --dump_results on five
   graphs: graph500-scale10.el64, a sparse project-generated RMAT graph
-  (scale 12, edge factor 2, seed 5) and a 48 x 48 grid with 30 % of its
-  edges deleted (seed 3).  Per graph: the CSR, the labels parsed from the
-  reference's dump, its component count, iteration count and check()
-  verdict, the text of its --dump_results; and a set of planted labellings (a vertex relabelled, two
+  (scale 12, edge factor 2, seed 5), a 48 x 48 grid with 30 % of its
+  edges deleted (seed 3), and two graphs whose last component is one run
+  of vertices ending at n-1 (a scale-10 RMAT graph plus one isolated
+  vertex; graph500-scale10 plus a 3-vertex path), where the reference's
+  dump ends without a newline.  Per graph: the CSR, the labels parsed from
+  the reference's dump, its component count, iteration count and check()
+  verdict, the raw text of its --dump_results; and a set of planted labellings (a vertex relabelled, two
   components merged under one label, arbitrary distinct labels, two labels
   swapped, one label for all, an isolated vertex given a used label) with
   the verdict of the reference's own components::check on each
@@ -133,7 +136,10 @@ def ref_components(el64, n):
                 lo, _, hi = part.partition("-")
                 labels[int(lo): int(hi or lo) + 1] = c
     assert (labels >= 0).all() and count is not None and passed is not None
-    dump = "".join(line + "\n" for line in out.splitlines() if line.startswith("Component "))
+    # the dump is the last thing the CLI prints, right after the check's
+    # verdict; kept byte for byte (a line may lack its newline)
+    verdict = "Checking results...PASS\n" if passed else "Checking results...FAIL\n"
+    dump = out[out.rindex(verdict) + len(verdict):]
     return labels, count, iters, passed, dump
 
 
@@ -278,10 +284,21 @@ def ref_components_check(el64, planted, tmp):
     return np.array(verdicts, np.int64)
 
 
+def with_tail(graph, k):
+    """The graph with k new vertices at the end joined as a path (k = 1: one
+    isolated vertex), so the last component is one run ending at vertex
+    n-1: the reference's dump prints no newline after that line."""
+    n, src, dst = graph
+    extra = np.arange(n, n + k - 1, dtype=np.int64)
+    return n + k, np.concatenate([src, extra]), np.concatenate([dst, extra + 1])
+
+
 def components_fixture(tmp):
     graphs = {"scale10": O.el64_load(os.path.join(HERE, "graph500-scale10.el64")),
               "rmat12_ef2": O.rmat_graph(12, edge_factor=2, seed=5),
-              "grid48": O.grid_graph(48, 48, 0.3, seed=3)}
+              "grid48": O.grid_graph(48, 48, 0.3, seed=3),
+              "tail_isolated": with_tail(O.rmat_graph(10, edge_factor=4, seed=9), 1),
+              "tail_path": with_tail(O.el64_load(os.path.join(HERE, "graph500-scale10.el64")), 3)}
     arrays = {}
     for name, (n, src, dst) in graphs.items():
         el = os.path.join(tmp, name + ".el64")

@@ -178,7 +178,7 @@ def test_cpp_facade_dump_text_equals_the_reference(tmp_path):
                     str(src), "-o", str(exe), "-L", lib_dir, "-lbeedrill_b200",
                     f"-Wl,-rpath,{lib_dir}"], check=True)
     ref = np.load(os.path.join(ROOT, "tests", "golden", "ref_components.npz"))
-    for name in ("scale10", "rmat12_ef2", "grid48"):
+    for name in ("scale10", "rmat12_ef2", "grid48", "tail_isolated", "tail_path"):
         labels = ref[f"{name}.labels"]
         path = tmp_path / f"{name}.bin"
         path.write_bytes(np.int64(len(labels)).tobytes() + labels.astype(np.int64).tobytes())
@@ -226,3 +226,14 @@ def test_python_print_tree_text_equals_the_reference():
     text, off = bytes(d["tree_text"]), d["tree_offsets"]
     for i, parent in enumerate(trees):
         assert bd.format_tree(parent).encode() == text[off[i]:off[i + 1]], i
+
+
+def test_format_tree_stops_on_a_cycle():
+    """A planted parent cycle (0 -> 1 -> 2 -> 1) ends its lines with a cycle
+    mark instead of climbing forever, as the reference would."""
+    import numpy as np
+    text = bd.format_tree(np.array([1, 2, 1, -1], np.int64))
+    lines = text.splitlines()
+    assert len(lines) == 3
+    assert all(line.endswith(" <- (cycle)") for line in lines)
+    assert lines[0].startswith("   0 <-    1 <-    2 <-    1")

@@ -39,7 +39,7 @@ def _run(g):
     return out
 
 
-@pytest.mark.parametrize("name", ["scale10", "rmat12_ef2", "grid48"])
+@pytest.mark.parametrize("name", ["scale10", "rmat12_ef2", "grid48", "tail_isolated", "tail_path"])
 def test_labels_equal_the_reference(name):
     ref = np.load(os.path.join(HERE, "golden", "ref_components.npz"))
     off, adj = ref[f"{name}.offsets"], ref[f"{name}.adj"]
@@ -145,27 +145,39 @@ def test_scale24_properties():
     g.close()
 
 
-def test_cli_matches_the_reference_output():
+@pytest.mark.parametrize("name", ["scale10", "tail_path"])
+def test_cli_matches_the_reference_output(name, tmp_path):
+    """The components CLI on a fixture graph: counts, check() and the
+    --dump_results text byte for byte as the reference's CLI printed it
+    (on tail_path the last line has no newline, as in the reference)."""
     import re
     import subprocess
     cli = os.path.join(os.path.dirname(HERE), "beedrill_b200", "bin", "components")
     if not os.path.exists(cli):
         pytest.skip("CLI not built")
     ref = np.load(os.path.join(HERE, "golden", "ref_components.npz"))
-    out = subprocess.run([cli, "--graph_filename", os.path.join(HERE, "golden", "graph500-scale10.el64"),
+    if name == "scale10":
+        path = os.path.join(HERE, "golden", "graph500-scale10.el64")
+    else:
+        off, adj = ref[f"{name}.offsets"], ref[f"{name}.adj"]
+        src, dst = _edges_from_csr(off, adj)
+        path = str(tmp_path / f"{name}.el64")
+        O.el64_write(path, len(off) - 1, src, dst)
+    count = int(ref[f"{name}.summary"][0])
+    out = subprocess.run([cli, "--graph_filename", path,
                           "--num_trials", "3", "--check_results", "--dump_results"],
                          stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, timeout=120)
     assert out.returncode == 0, out.stdout
     text = out.stdout
-    assert text.count("Found 138 components in 1 iterations") == 3
+    assert text.count(f"Found {count} components in 1 iterations") == 3
     assert "Checking results...PASS" in text
-    labels = np.full(1024, -1, np.int64)
-    for line in text.splitlines():
-        m = re.match(r"Component (\d+): (.*)$", line)
-        if m:
-            for part in m.group(2).split(", "):
-                lo, _, hi = part.partition("-")
-                labels[int(lo): int(hi or lo) + 1] = int(m.group(1))
-    assert np.array_equal(labels, ref["scale10.labels"])
-    dump = "".join(line + "\n" for line in text.splitlines() if line.startswith("Component "))
-    assert dump.encode() == bytes(ref["scale10.dump"])
+    n = len(ref[f"{name}.labels"])
+    labels = np.full(n, -1, np.int64)
+    for m in re.finditer(r"Component (\d+): ((?:\d+(?:-\d+)?)(?:, \d+(?:-\d+)?)*)", text):
+        for part in m.group(2).split(", "):
+            lo, _, hi = part.partition("-")
+            labels[int(lo): int(hi or lo) + 1] = int(m.group(1))
+    assert np.array_equal(labels, ref[f"{name}.labels"])
+    verdict = "Checking results...PASS\n"
+    dump = text[text.rindex(verdict) + len(verdict):]
+    assert dump.encode() == bytes(ref[f"{name}.dump"])

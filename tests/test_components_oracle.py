@@ -17,7 +17,7 @@ import pytest
 from oracle import oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-NAMES = ["scale10", "rmat12_ef2", "grid48"]
+NAMES = ["scale10", "rmat12_ef2", "grid48", "tail_isolated", "tail_path"]
 
 
 @pytest.fixture(scope="module")

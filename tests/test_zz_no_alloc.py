@@ -9,8 +9,11 @@ CSR and the output arrays.
 This file is collected last on purpose.  The test calls the new entry point
 through the C ABI twice in a row (different roots, so stale scratch from the
 first call would show) and compares each result with the regular entry point
-(bd_bfs_run on a HybridBFS handle) on the same graph and root: depths
-bit-exact, m_c equal, and the parent tree must pass the reference's check().
+(bd_bfs_run on a HybridBFS handle) and with the oracle on the same graph and
+root: depths bit-exact against both, m_c equal, and the parent tree must
+pass the reference's check().  The device's free memory must be the same
+before and after the second call (the first one only looks the scratch
+array up).
 """
 import ctypes
 
@@ -59,15 +62,20 @@ def test_noalloc_matches_regular_entry_point(scale):
     parent = torch.empty(n, dtype=torch.int64, device="cuda:0")
     regular = bd.HybridBFS(g, alg="beamer_hybrid")
     run = _fn()
-    for root in g.pick_roots(5, 2):  # two calls in a row
+    for i, root in enumerate(g.pick_roots(5, 2)):  # two calls in a row
         root = int(root)
         torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(0)[0]
         edges = ctypes.c_int64(-1)
         st = run(d_off, d_adj, n, len(adj), root, 15, 18, depth.data_ptr(), parent.data_ptr(),
                  None, ctypes.byref(edges))
         assert st == 0, bd.lib().bd_status_string(st)
+        torch.cuda.synchronize()
+        if i == 1:
+            assert torch.cuda.mem_get_info(0)[0] == free_before, "the call allocated device memory"
         got_depth = depth.cpu().numpy()
         got_parent = parent.cpu().numpy()
+        assert np.array_equal(got_depth, O.bfs_depth(off, adj, root))
         regular.clear()
         stats = regular.run(root)
         assert np.array_equal(got_depth, regular.depths())
