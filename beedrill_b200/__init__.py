@@ -85,7 +85,7 @@ class MsBfsOpts(Structure):
         ("alpha", c_int64), ("force_dir", c_int32), ("block_size", c_int32),
         ("large_degree", c_int32), ("chunk_edges", c_int32), ("pull_prefix", c_int32),
         ("use_graph", c_int32), ("spin_limit", c_int64), ("heavy_degree", c_int32),
-        ("heavy_chunk", c_int32),
+        ("heavy_chunk", c_int32), ("materialize", c_int32), ("min_parent", c_int32),
     ]
 
 
@@ -143,6 +143,8 @@ def lib() -> ctypes.CDLL:
         "bd_graph_from_csr": (c_int, [c_int64, c_int64, i64p, u32p, vpp]),
         "bd_graph_rmat": (c_int, [c_int32, c_int64, c_double, c_double, c_double, c_double,
                                   c_uint64, c_int32, vpp]),
+        "bd_graph_rmat_stream": (c_int, [c_int32, c_int64, c_double, c_double, c_double, c_double,
+                                         ctypes.c_uint32, c_int32, c_uint64, c_int32, vpp]),
         "bd_graph_concat": (c_int, [vpp, c_int64, vpp, i64p]),
         "bd_graph_grid": (c_int, [c_int64, c_int64, c_double, c_uint64, c_int32, vpp]),
         "bd_graph_info": (c_int, [c_void_p, i64p, i64p]),
@@ -173,6 +175,8 @@ def lib() -> ctypes.CDLL:
         "bd_bfs_run_multi": (c_int, [c_void_p, i64p, c_int64, POINTER(RunStats)]),
         "bd_bfs_run_many": (c_int, [c_void_p, i64p, c_int64, POINTER(c_double), i64p, i64p,
                                     POINTER(c_double)]),
+        "bd_bfs_run_many_into": (c_int, [c_void_p, i64p, c_int64, c_void_p, c_void_p,
+                                         POINTER(c_double), i64p, i64p, POINTER(c_double)]),
         "bd_bfs_get_depths": (c_int, [c_void_p, i32p]),
         "bd_bfs_get_parents": (c_int, [c_void_p, i64p]),
         "bd_bfs_device_ptrs": (c_int, [c_void_p, vpp, vpp]),
@@ -189,6 +193,7 @@ def lib() -> ctypes.CDLL:
         "bd_msbfs_count_traversed_edges": (c_int, [c_void_p, c_int32, i64p, i64p]),
         "bd_msbfs_get_steps": (c_int, [c_void_p, POINTER(Step), c_int64, i64p]),
         "bd_msbfs_check": (c_int, [c_void_p, c_int32, POINTER(c_int32)]),
+        "bd_msbfs_device_results": (c_int, [c_void_p, c_int32, vpp, vpp]),
         "bd_msbfs_destroy": (c_int, [c_void_p]),
         "bd_msbfs_set_policy": (c_int, [c_void_p, f32p, f32p, f32p, f32p, f32p, c_float]),
         "bd_policy_forward": (c_int, [f32p, f32p, c_int64, f32p]),
@@ -278,6 +283,20 @@ class Graph:
         h = c_void_p()
         _check(lib().bd_graph_rmat(scale, edge_factor, a, b, c, d, seed, order, byref(h)),
                f"rmat(scale={scale})")
+        return cls(h)
+
+    @classmethod
+    def rmat_stream(cls, scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19,
+                    c: float = 0.19, d: float = 0.05, stream_seed: int = 0, permute: bool = False,
+                    permute_seed: int = 0, order: int = ORDER_INSERTION) -> "Graph":
+        """RMAT edges drawn exactly as the reference's generator draws them
+        (its sitmo stream, rmat_generator.h:70-193), flipped, sorted and
+        deduplicated; permute=False keeps the generator's ids and the sorted
+        order, permute=True applies the seeded relabel and shuffle of rmat()."""
+        h = c_void_p()
+        _check(lib().bd_graph_rmat_stream(scale, edge_factor, a, b, c, d, stream_seed,
+                                          int(bool(permute)), permute_seed, order, byref(h)),
+               f"rmat_stream(scale={scale})")
         return cls(h)
 
     @classmethod
@@ -465,6 +484,23 @@ class HybridBFS:
             return ms, edges, reached, e2e.value
         return ms, edges, e2e.value
 
+    def run_many_into(self, sources, d_depth: int, d_parent: int):
+        """run_many, and root i's depths and parents (caller ids, the
+        reference's encoding) written inside its timed region to the device
+        arrays at d_depth + i*n (int32) and d_parent + i*n (int64), each of
+        len(sources) x n entries.  Returns per-root ms, m_c, n_c and the
+        device time of the whole call."""
+        src = np.ascontiguousarray(sources, np.int64)
+        ms = np.empty(len(src), np.float64)
+        edges = np.empty(len(src), np.int64)
+        reached = np.empty(len(src), np.int64)
+        e2e = c_double()
+        _check(lib().bd_bfs_run_many_into(self._h, _ptr(src, c_int64), len(src), c_void_p(d_depth),
+                                          c_void_p(d_parent), _ptr(ms, c_double),
+                                          _ptr(edges, c_int64), _ptr(reached, c_int64), byref(e2e)),
+               "run_many_into")
+        return ms, edges, reached, e2e.value
+
     # hybrid_bfs::check (hybrid_bfs.cc:281-379)
     def check(self, source: int) -> bool:
         ok = c_int32()
@@ -527,7 +563,8 @@ class BatchedBFS:
     def __init__(self, graph: Graph, max_roots: int = 64, alpha: int = 0, force_dir: int = -1,
                  use_graph: bool = True, block_size: int = 0, large_degree: int = 0,
                  chunk_edges: int = 0, pull_prefix: int = 0, spin_limit: int = 0,
-                 heavy_degree: int = 0, heavy_chunk: int = 0, tuned: bool = True):
+                 heavy_degree: int = 0, heavy_chunk: int = 0, tuned: bool = True,
+                 materialize: bool = False, min_parent: bool = False):
         if tuned:
             t = tuned_options("batched", graph.num_vertices())
             alpha = alpha or t.get("alpha", 0)
@@ -547,6 +584,7 @@ class BatchedBFS:
         o.block_size, o.large_degree, o.chunk_edges = block_size, large_degree, chunk_edges
         o.pull_prefix, o.spin_limit = pull_prefix, spin_limit
         o.heavy_degree, o.heavy_chunk = heavy_degree, heavy_chunk
+        o.materialize, o.min_parent = int(bool(materialize)), int(bool(min_parent))
         self.max_roots = max_roots
         self._h = c_void_p()
         _check(lib().bd_msbfs_create(graph._h, max_roots, byref(o), byref(self._h)), "msbfs")
@@ -569,6 +607,12 @@ class BatchedBFS:
         _check(lib().bd_msbfs_get_parents(self._h, i, _ptr(p, c_int64)), "msbfs parents")
         return p
 
+    def parents_to(self, i: int, host_addr: int) -> None:
+        """Root i's parents into caller-owned host memory at host_addr (n
+        int64 entries; pinned memory copies fastest)."""
+        _check(lib().bd_msbfs_get_parents(self._h, i, ctypes.cast(host_addr, POINTER(c_int64))),
+               "msbfs parents")
+
     def count_num_traversed_edges(self, i: int) -> int:
         e = c_int64()
         _check(lib().bd_msbfs_count_traversed_edges(self._h, i, byref(e), None), "msbfs count")
@@ -584,6 +628,13 @@ class BatchedBFS:
         ok = c_int32()
         _check(lib().bd_msbfs_check(self._h, i, byref(ok)), "msbfs check")
         return bool(ok.value)
+
+    def device_results(self, i: int) -> tuple[int, int]:
+        """Device addresses of root i's materialized depths (int32[n]) and
+        parents (int64[n]); the handle must be made with materialize=True."""
+        d, p = c_void_p(), c_void_p()
+        _check(lib().bd_msbfs_device_results(self._h, i, byref(d), byref(p)), "msbfs results")
+        return d.value, p.value
 
     def counts(self):
         """(m_c, n_c) arrays over the roots of the last run."""

@@ -1130,10 +1130,31 @@ bd_status ensure_sources(bd_bfs *b, int64_t count)
     return BD_OK;
 }
 
+// Depths and parents in the caller's arrays with the reference's encoding
+// of unreached vertices (graphs without a hub numbering: the same ids).
+__global__ void copy_outputs_kernel(const int64_t *off, int64_t n, const int32_t *depth,
+                                    const int64_t *parent, int32_t *out_depth, int64_t *out_parent)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = depth[v];
+        out_depth[v] = d;
+        if (d >= 0) {
+            out_parent[v] = parent[v];
+        } else {
+            const int64_t deg = off[v + 1] - off[v];
+            out_parent[v] = deg != 0 ? -deg : -1;
+        }
+    }
+}
+
 // Enqueues init + the persistent kernel (+ min-parent pass) for either a
-// set of sources (index < 0) or source d_sources[index].
+// set of sources (index < 0) or source d_sources[index].  With out_depth /
+// out_parent (device, n entries each) the results are also written there
+// in the caller's ids and the reference's encoding, inside the timed region.
 bd_status enqueue_bfs(bd_bfs *b, int64_t count, int64_t index, cudaEvent_t start,
-                      cudaEvent_t stop)
+                      cudaEvent_t stop, int32_t *out_depth = nullptr,
+                      int64_t *out_parent = nullptr)
 {
     BfsParams p = make_params(b);
     // The timed region starts with the source setup, as run_beamer's does
@@ -1144,7 +1165,23 @@ bd_status enqueue_bfs(bd_bfs *b, int64_t count, int64_t index, cudaEvent_t start
     void *args[] = {&p};
     BD_CUDA(cudaLaunchCooperativeKernel((const void *)b->kernel, dim3(b->grid), dim3(b->block),
                                         args, 0, b->stream));
-    if (b->opts.min_parent) {
+    if (out_depth) {
+        const int64_t n = b->g->n;
+        if (b->g->d_perm) {
+            hub_outputs_kernel<<<grid_for(n), 256, 0, b->stream>>>(
+                b->g->d_perm, b->g->d_iperm, b->g->d_off, n, b->depth, b->parent, out_depth,
+                out_parent);
+        } else {
+            copy_outputs_kernel<<<grid_for(n), 256, 0, b->stream>>>(b->g->d_off, n, b->depth,
+                                                                   b->parent, out_depth, out_parent);
+        }
+        BD_CUDA(cudaGetLastError());
+        if (b->opts.min_parent) {
+            min_parent_kernel<<<grid_for(bitmap_words(n) * 32), 256, 0, b->stream>>>(
+                b->g->d_off, b->g->d_adj, n, out_depth, out_parent);
+            BD_CUDA(cudaGetLastError());
+        }
+    } else if (b->opts.min_parent) {
         // the smallest parent in the caller's numbering: on a hub graph, map
         // the outputs back first, then pick parents on the caller's CSR
         const int64_t n = b->g->n;
@@ -1253,6 +1290,14 @@ void bfs_free(bd_bfs *b)
 }
 
 }  // namespace
+
+cudaError_t launch_min_parent(const int64_t *off, const uint32_t *adj, int64_t n,
+                              const int32_t *depth, int64_t *parent, cudaStream_t s)
+{
+    min_parent_kernel<<<grid_for(bitmap_words(n) * 32), 256, 0, s>>>(off, adj, n, depth, parent);
+    return cudaGetLastError();
+}
+
 }  // namespace bd
 
 extern "C" {
@@ -1380,8 +1425,14 @@ bd_status bd_bfs_run_bottom_up(bd_bfs *b, int64_t source, bd_run_stats *stats)
     return run_with_alg(b, BD_ALG_BOTTOM_UP, b->opts.alpha, b->opts.beta, source, stats);
 }
 
-bd_status bd_bfs_run_many(bd_bfs *b, const int64_t *sources, int64_t k, double *ms_out,
-                          int64_t *edges_out, int64_t *reached_out, double *e2e_ms)
+}  // extern "C"
+
+namespace bd {
+namespace {
+
+bd_status run_many(bd_bfs *b, const int64_t *sources, int64_t k, int32_t *d_depth,
+                   int64_t *d_parent, double *ms_out, int64_t *edges_out, int64_t *reached_out,
+                   double *e2e_ms)
 {
     if (!b || !sources || k <= 0) { return BD_ERR_INVALID; }
     for (int64_t i = 0; i < k; ++i) {
@@ -1414,9 +1465,13 @@ bd_status bd_bfs_run_many(bd_bfs *b, const int64_t *sources, int64_t k, double *
         cleanup();
         return BD_ERR_CUDA;
     }
+    const int64_t n = b->g->n;
     for (int64_t i = 0; i < k && st == BD_OK; ++i) {
         st = enqueue_clear(b);
-        if (st == BD_OK) { st = enqueue_bfs(b, k, i, ev[2 * i], ev[2 * i + 1]); }
+        if (st == BD_OK) {
+            st = enqueue_bfs(b, k, i, ev[2 * i], ev[2 * i + 1], d_depth ? d_depth + i * n : nullptr,
+                             d_depth ? d_parent + i * n : nullptr);
+        }
         if (st == BD_OK) {
             save_result_kernel<<<1, 1, 0, b->stream>>>(b->ctrl, d_edges, i);
             if (cudaGetLastError() != cudaSuccess) { st = BD_ERR_CUDA; }
@@ -1445,6 +1500,25 @@ bd_status bd_bfs_run_many(bd_bfs *b, const int64_t *sources, int64_t k, double *
     }
     cleanup();
     return st;
+}
+
+}  // namespace
+}  // namespace bd
+
+extern "C" {
+
+bd_status bd_bfs_run_many(bd_bfs *b, const int64_t *sources, int64_t k, double *ms_out,
+                          int64_t *edges_out, int64_t *reached_out, double *e2e_ms)
+{
+    return run_many(b, sources, k, nullptr, nullptr, ms_out, edges_out, reached_out, e2e_ms);
+}
+
+bd_status bd_bfs_run_many_into(bd_bfs *b, const int64_t *sources, int64_t k, int32_t *d_depth,
+                               int64_t *d_parent, double *ms_out, int64_t *edges_out,
+                               int64_t *reached_out, double *e2e_ms)
+{
+    if (!d_depth || !d_parent) { return BD_ERR_INVALID; }
+    return run_many(b, sources, k, d_depth, d_parent, ms_out, edges_out, reached_out, e2e_ms);
 }
 
 bd_status bd_bfs_get_depths(bd_bfs *b, int32_t *depth)

@@ -9,30 +9,43 @@
 // id of its component -- so any algorithm that finds the components and
 // names each by its minimum id gives the reference's labels exactly.
 //
-// Here one pass over the arcs builds a union-find forest in HBM (one
-// uint32 parent per vertex; at scale 24 the 64 MB array stays in L2):
+// Here a union-find forest in HBM (one uint32 parent per vertex; at scale
+// 24 the 64 MB array stays in L2) is built by joins of arcs; joining links
+// the larger root under the smaller one with one atomicCAS on the larger
+// root's parent word, so every parent id is smaller than its child's and
+// every root is the minimum id of its tree: the final roots are exactly the
+// reference's labels.  Finds shorten paths as they walk (path splitting:
+// each visited vertex is pointed at its grandparent, an ancestor, so the
+// forest stays valid under concurrent finds and links).  Every loop ends: a
+// find walks strictly decreasing ids, and a join retries only after another
+// thread's link took its root, which happens at most n - 1 times in all.
 //
-//   cc_hook_kernel        one warp per vertex, lanes over its arcs; each
-//                         arc (u, v) with v < u joins the trees of u and v
-//                         (a symmetric CSR holds every edge twice, once in
-//                         each direction; any other CSR joins every arc).
-//                         Vertices of more than kHeavy arcs are listed
-//                         for the next kernel instead.
-//   cc_hook_heavy_kernel  the listed vertices, each one's arcs spread over
-//                         every thread of the grid.
-//   cc_compress_kernel    each vertex's label becomes its tree's root;
-//                         sizes per label and the count of roots.
-//
-// Joining links the larger root under the smaller one with one atomicCAS
-// on the larger root's parent word, so every parent id is smaller than its
-// child's and every root is the minimum id of its tree: the final roots
-// are exactly the reference's labels.  Finds shorten paths as they walk
-// (path splitting: each visited vertex is pointed at its grandparent, an
-// ancestor, so the forest stays valid under concurrent finds and links).
-// Every loop ends: a find walks strictly decreasing ids, and a join retries
-// only after another thread's link took its root, which happens at most
-// n - 1 times in all.
+// Which arcs are joined (symmetric CSR, every edge stored both ways), after
+// Sutton, Ben-Nun and Barak, "Optimizing Parallel Graph Connectivity
+// Computation via Subgraph Sampling" (IPDPS 2018, "Afforest"):
+//   cc_sample_kernel      every vertex joins its first kSampleArcs arcs,
+//                         one round per arc position, then every vertex is
+//                         pointed at its root (cc_flatten_kernel);
+//   the largest tree      found by sampling kProbe vertices' roots;
+//   cc_finish_kernel      every vertex OUTSIDE that tree joins the rest of
+//                         its arcs.  An edge between the largest tree and
+//                         another vertex is stored at that other vertex
+//                         too, and is joined from there, so skipping the
+//                         largest tree's own arcs loses no edge.  A warp
+//                         loads 32 vertices' roots at once and walks only
+//                         the lists of those with work; lists of more than
+//                         kHeavy arcs go to cc_finish_heavy_kernel, which
+//                         deals every listed vertex's arcs over the grid in
+//                         one flat range (a binary search per chunk).
+//   cc_compress_kernel    labels (each vertex's root), sizes per label
+//                         (one atomic per distinct label of a warp) and the
+//                         count of roots.
+// A CSR that does not hold every edge both ways takes every arc instead
+// (cc_hook_kernel / cc_hook_heavy_kernel, the same warp walk over all
+// vertices).
+#include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "bd_internal.h"
 
@@ -41,7 +54,10 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int64_t kHeavy = 4096;  // arcs above which a vertex is split over the grid
+constexpr int64_t kHeavy = 4096;    // arcs above which a vertex is split over the grid
+constexpr int kSampleArcs = 2;      // arc positions joined before the largest tree is found
+constexpr int kProbe = 1024;        // vertices whose roots vote for the largest tree
+constexpr int64_t kHeavyChunk = 1024;  // arcs per unit of the heavy pass
 
 int grid_for_warps(int64_t warps)
 {
@@ -91,42 +107,156 @@ __global__ void cc_init_kernel(uint32_t *parent, int64_t n, int64_t *size)
     }
 }
 
-__global__ void __launch_bounds__(kThreads) cc_hook_kernel(
-    const int64_t *off, const uint32_t *adj, int64_t n, int symmetric, uint32_t *parent,
-    uint32_t *heavy, unsigned long long *heavy_count)
+// Arc position `pos` of every vertex that has one.
+__global__ void cc_sample_kernel(const int64_t *off, const uint32_t *adj, int64_t n, int pos,
+                                 uint32_t *parent)
+{
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = off[u];
+        if (off[u + 1] - b > pos) { cc_join(parent, (uint32_t)u, __ldg(&adj[b + pos])); }
+    }
+}
+
+// Every vertex pointed at its root.
+__global__ void cc_flatten_kernel(uint32_t *parent, int64_t n)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = cc_find(parent, (uint32_t)v);
+        __stcg(&parent[v], r);
+    }
+}
+
+// Roots of kProbe vertices spread evenly over the ids.
+__global__ void cc_probe_kernel(uint32_t *parent, int64_t n, uint32_t *out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kProbe) {
+        const uint32_t v = (uint32_t)(((uint64_t)i * (uint64_t)n) / kProbe);
+        out[i] = cc_find(parent, v);
+    }
+}
+
+// Arcs [first, e) of the vertices of a warp's 32-vertex group that have
+// work: each such vertex's list is walked by the whole warp, 32 arcs a
+// round; lists longer than kHeavy are appended to `heavy` instead.
+// skip_root: vertices whose root is this id have no work (the largest
+// tree), or ~0u for none; first: arc position to start at; all_arcs: join
+// every arc (else only arcs to smaller ids: each edge once, from its larger
+// endpoint).
+__global__ void __launch_bounds__(kThreads) cc_walk_kernel(
+    const int64_t *off, const uint32_t *adj, int64_t n, uint32_t *parent, uint32_t skip_root,
+    int first, int all_arcs, uint32_t *heavy, unsigned long long *heavy_count)
 {
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * kWarps;
-    for (int64_t u = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32; u < n; u += warps) {
-        const int64_t b = off[u], e = off[u + 1];
-        if (e - b > kHeavy) {
-            if (lane == 0) { heavy[atomicAdd(heavy_count, 1ull)] = (uint32_t)u; }
-            continue;
+    const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = gw * 32; base < n; base += nw * 32) {
+        const int64_t u = base + lane;
+        int64_t b = 0, e = 0;
+        bool work = false;
+        if (u < n) {
+            b = off[u] + first;
+            e = off[u + 1];
+            work = b < e && (skip_root == ~0u || __ldcg(&parent[u]) != skip_root);
+            if (work && e - b > kHeavy) {
+                heavy[atomicAdd(heavy_count, 1ull)] = (uint32_t)u;
+                work = false;
+            }
         }
-        for (int64_t k = b + lane; k < e; k += 32) {
-            const uint32_t v = adj[k];
-            if (!symmetric || v < (uint32_t)u) { cc_join(parent, (uint32_t)u, v); }
+        unsigned todo = __ballot_sync(0xffffffffu, work);
+        while (todo) {
+            const int owner = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int64_t bb = __shfl_sync(0xffffffffu, b, owner);
+            const int64_t ee = __shfl_sync(0xffffffffu, e, owner);
+            const uint32_t uu = (uint32_t)(base + owner);
+            for (int64_t k = bb + lane; k < ee; k += 32) {
+                const uint32_t v = __ldg(&adj[k]);
+                if (all_arcs || v < uu) { cc_join(parent, uu, v); }
+            }
         }
     }
 }
 
-__global__ void __launch_bounds__(kThreads) cc_hook_heavy_kernel(
-    const int64_t *off, const uint32_t *adj, int symmetric, uint32_t *parent,
-    const uint32_t *heavy, const unsigned long long *heavy_count)
+// Chunk prefix of the heavy list: cbase[i] = chunks of heavy vertices < i.
+// One block of 1024 threads scans 1024 entries per round.
+__global__ void __launch_bounds__(1024) cc_heavy_chunks_kernel(
+    const int64_t *off, const uint32_t *heavy, const unsigned long long *heavy_count, int first,
+    unsigned long long *cbase)
 {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    __shared__ unsigned long long warp_tot[32];
+    __shared__ unsigned long long carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t count = (int64_t)*heavy_count;
-    for (int64_t i = 0; i < count; ++i) {
-        const uint32_t u = heavy[i];
-        const int64_t e = off[u + 1];
-        for (int64_t k = off[u] + t; k < e; k += stride) {
-            const uint32_t v = adj[k];
-            if (!symmetric || v < u) { cc_join(parent, u, v); }
+    if (threadIdx.x == 0) { carry = 0; }
+    __syncthreads();
+    for (int64_t base = 0; base < count; base += 1024) {
+        const int64_t i = base + threadIdx.x;
+        unsigned long long c = 0;
+        if (i < count) {
+            const uint32_t u = heavy[i];
+            const int64_t len = off[u + 1] - (off[u] + first);
+            c = (unsigned long long)((len + kHeavyChunk - 1) / kHeavyChunk);
+        }
+        unsigned long long incl = c;
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) { incl += y; }
+        }
+        if (lane == 31) { warp_tot[warp] = incl; }
+        __syncthreads();
+        if (warp == 0) {
+            unsigned long long t = warp_tot[lane];
+            for (int d = 1; d < 32; d <<= 1) {
+                const unsigned long long y = __shfl_up_sync(0xffffffffu, t, d);
+                if (lane >= d) { t += y; }
+            }
+            warp_tot[lane] = t;  // inclusive prefix over warps
+        }
+        __syncthreads();
+        const unsigned long long before = carry + (warp ? warp_tot[warp - 1] : 0ull);
+        if (i < count) { cbase[i] = before + incl - c; }
+        __syncthreads();
+        if (threadIdx.x == 1023) { carry = before + incl; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { cbase[count] = carry; }
+}
+
+// The heavy vertices' arcs as one flat range of kHeavyChunk-arc chunks dealt
+// to the warps of the grid (a warp per chunk, a binary search for its
+// vertex), so no thread walks one vertex's chunks after another.
+__global__ void __launch_bounds__(kThreads) cc_heavy_kernel(
+    const int64_t *off, const uint32_t *adj, uint32_t *parent, const uint32_t *heavy,
+    const unsigned long long *heavy_count, const unsigned long long *cbase, int first,
+    int all_arcs)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t count = (int64_t)*heavy_count;
+    if (count == 0) { return; }
+    const int64_t total = (int64_t)cbase[count];
+    for (int64_t c = gw; c < total; c += nw) {
+        int64_t lo = 0, hi = count - 1;  // last i with cbase[i] <= c
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) >> 1;
+            if ((int64_t)cbase[mid] <= c) { lo = mid; } else { hi = mid - 1; }
+        }
+        const uint32_t u = heavy[lo];
+        const int64_t b = off[u] + first + (c - (int64_t)cbase[lo]) * kHeavyChunk;
+        const int64_t e = min(off[u + 1], b + kHeavyChunk);
+        for (int64_t k = b + lane; k < e; k += 32) {
+            const uint32_t v = __ldg(&adj[k]);
+            if (all_arcs || v < u) { cc_join(parent, u, v); }
         }
     }
 }
 
+// Labels, sizes and roots.  Sizes: the lanes of a warp that share a label
+// add it once (the largest component's label is shared by most lanes).
 __global__ void cc_compress_kernel(uint32_t *parent, int64_t n, int64_t *label, int64_t *size,
                                    unsigned long long *roots)
 {
@@ -134,15 +264,19 @@ __global__ void cc_compress_kernel(uint32_t *parent, int64_t n, int64_t *label, 
     for (int64_t base = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; base < n;
          base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t v = base + lane;
-        bool root = false;
-        if (v < n) {
-            const uint32_t r = cc_find(parent, (uint32_t)v);
+        const bool valid = v < n;
+        uint32_t r = 0xFFFFFFFFu;
+        if (valid) {
+            r = cc_find(parent, (uint32_t)v);
             __stcg(&parent[v], r);
-            label[v] = r;
-            atomicAdd(reinterpret_cast<unsigned long long *>(&size[r]), 1ull);
-            root = r == (uint32_t)v;
+            __stcs(&label[v], (int64_t)r);
         }
-        const unsigned mask = __ballot_sync(0xffffffffu, root);
+        const unsigned same = __match_any_sync(0xffffffffu, r);
+        if (valid && lane == __ffs(same) - 1) {
+            atomicAdd(reinterpret_cast<unsigned long long *>(&size[r]),
+                      (unsigned long long)__popc(same));
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, valid && r == (uint32_t)v);
         if (lane == 0 && mask) { atomicAdd(roots, (unsigned long long)__popc(mask)); }
     }
 }
@@ -166,6 +300,8 @@ struct bd_components {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint32_t *parent = nullptr;            // [n] union-find forest
     uint32_t *heavy = nullptr;             // [arcs / kHeavy + 1] vertices split over the grid
+    unsigned long long *cbase = nullptr;   // [arcs / kHeavy + 2] their chunk prefix
+    uint32_t *probe = nullptr;             // [kProbe] sampled roots
     unsigned long long *counters = nullptr;  // [0] heavy vertices, [1] roots
     int64_t *label = nullptr;              // [n] component_ (components.h:13)
     int64_t *size = nullptr;               // [n] component_size_ (components.h:15)
@@ -182,6 +318,8 @@ void components_free(bd_components *c)
     if (c->stream) { cudaStreamSynchronize(c->stream); }
     cudaFree(c->parent);
     cudaFree(c->heavy);
+    cudaFree(c->cbase);
+    cudaFree(c->probe);
     cudaFree(c->counters);
     cudaFree(c->label);
     cudaFree(c->size);
@@ -209,6 +347,8 @@ bd_status bd_components_create(bd_graph *g, bd_components **out)
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
         cudaMalloc(&c->parent, sizeof(uint32_t) * (n ? n : 1)) != cudaSuccess ||
         cudaMalloc(&c->heavy, sizeof(uint32_t) * heavy_cap) != cudaSuccess ||
+        cudaMalloc(&c->cbase, sizeof(unsigned long long) * (heavy_cap + 1)) != cudaSuccess ||
+        cudaMalloc(&c->probe, sizeof(uint32_t) * bd::kProbe) != cudaSuccess ||
         cudaMalloc(&c->counters, sizeof(unsigned long long) * 2) != cudaSuccess ||
         cudaMalloc(&c->label, sizeof(int64_t) * (n ? n : 1)) != cudaSuccess ||
         cudaMalloc(&c->size, sizeof(int64_t) * (n ? n : 1)) != cudaSuccess) {
@@ -236,10 +376,40 @@ bd_status bd_components_run(bd_components *c, bd_components_stats *stats)
     BD_CUDA(cudaEventRecord(c->ev0, s));
     BD_CUDA(cudaMemsetAsync(c->counters, 0, sizeof(unsigned long long) * 2, s));
     bd::cc_init_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(c->parent, n, c->size);
-    bd::cc_hook_kernel<<<bd::grid_for_warps(n), bd::kThreads, 0, s>>>(
-        g->d_off, g->d_adj, n, g->symmetric ? 1 : 0, c->parent, c->heavy, c->counters);
-    bd::cc_hook_heavy_kernel<<<148 * 8, bd::kThreads, 0, s>>>(
-        g->d_off, g->d_adj, g->symmetric ? 1 : 0, c->parent, c->heavy, c->counters);
+    uint32_t skip = ~0u;
+    int first = 0;
+    if (g->symmetric) {
+        for (int pos = 0; pos < bd::kSampleArcs; ++pos) {
+            bd::cc_sample_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(g->d_off, g->d_adj, n,
+                                                                         pos, c->parent);
+        }
+        bd::cc_flatten_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(c->parent, n);
+        bd::cc_probe_kernel<<<(bd::kProbe + 255) / 256, 256, 0, s>>>(c->parent, n, c->probe);
+        BD_CUDA(cudaGetLastError());
+        std::vector<uint32_t> probe(bd::kProbe);
+        BD_CUDA(cudaMemcpyAsync(probe.data(), c->probe, sizeof(uint32_t) * bd::kProbe,
+                                cudaMemcpyDeviceToHost, s));
+        BD_CUDA(cudaStreamSynchronize(s));
+        // the most frequent root among the probes: the largest tree
+        std::sort(probe.begin(), probe.end());
+        size_t best = 0;
+        for (size_t i = 0, j = 0; i < probe.size(); i = j) {
+            for (j = i; j < probe.size() && probe[j] == probe[i]; ++j) {}
+            if (j - i > best) {
+                best = j - i;
+                skip = probe[i];
+            }
+        }
+        first = bd::kSampleArcs;
+    }
+    // symmetric: the rest of the arcs of vertices outside the largest tree;
+    // otherwise every arc of every vertex
+    bd::cc_walk_kernel<<<bd::grid_for_warps(n), bd::kThreads, 0, s>>>(
+        g->d_off, g->d_adj, n, c->parent, skip, first, 1, c->heavy, c->counters);
+    bd::cc_heavy_chunks_kernel<<<1, 1024, 0, s>>>(g->d_off, c->heavy, c->counters, first,
+                                                  c->cbase);
+    bd::cc_heavy_kernel<<<148 * 8, bd::kThreads, 0, s>>>(g->d_off, g->d_adj, c->parent, c->heavy,
+                                                        c->counters, c->cbase, first, 1);
     bd::cc_compress_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(c->parent, n, c->label,
                                                                     c->size, c->counters + 1);
     BD_CUDA(cudaGetLastError());

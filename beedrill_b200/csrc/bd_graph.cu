@@ -163,6 +163,218 @@ __global__ void rmat_keys_kernel(int scale, int64_t num_edges, double a, double 
     }
 }
 
+// ---------------------------------------------------------------------------
+// The reference generator's own random stream (generator/rmat_generator.h,
+// generator/prng_engine.hpp), so that edge streams can equal the
+// reference's bit for bit.
+//
+// sitmo::prng_engine (M.A. van den Berg, MIT licence, vendored by the
+// reference) is a counter-mode generator: 32-bit output t is half of
+// Threefish-256 (Skein 1.3 specification) reduced to 20 rounds, tweak zero,
+// key (seed, 0, 0, 0), applied to the 256-bit counter (t / 8, 0, 0, 0) --
+// the low half of 64-bit word (t % 8) / 2 when t is even, the high half when
+// odd.  Seeding encrypts counter 0, and discard(z) moves the counter, so
+// any position of the stream is reached directly.
+//
+// The reference draws its uniform doubles through libstdc++ (GCC 13)
+// std::uniform_real_distribution<double>(0, 1), which calls
+// std::generate_canonical<double, 53>: two engine outputs u0, u1 combined
+// as (u0 + u1 * 2^32) / 2^64 in double arithmetic (one rounding, at the
+// sum), with 1 - 2^-53 in place of a result of 1.
+// ---------------------------------------------------------------------------
+constexpr uint64_t kThreefishParity = 0x1BD11BDAA9FC1A22ull;
+
+__host__ __device__ __forceinline__ uint64_t rotl64(uint64_t x, int r)
+{
+    return (x << r) | (x >> (64 - r));
+}
+
+// Threefish-256, 20 rounds, zero tweak: the block of counter `ctr` under key
+// (key0, 0, 0, 0).  Rotation amounts of round r are kRot[r % 8]; words are
+// paired (0,1),(2,3) on even rounds and (0,3),(2,1) on odd rounds (the
+// Threefish-256 word permutation); subkey s is injected before rounds
+// 4s and after the last round.
+__device__ __forceinline__ void threefish20(uint64_t key0, uint64_t ctr, uint64_t o[4])
+{
+    const uint64_t k[5] = {key0, 0, 0, 0, kThreefishParity ^ key0};
+    const int rot[8][2] = {{14, 16}, {52, 57}, {23, 40}, {5, 37},
+                           {25, 33}, {46, 12}, {58, 22}, {32, 32}};
+    uint64_t x0 = ctr, x1 = 0, x2 = 0, x3 = 0;
+#pragma unroll
+    for (int r = 0; r < 20; ++r) {
+        if ((r & 3) == 0) {
+            const int sk = r >> 2;
+            x0 += k[sk % 5];
+            x1 += k[(sk + 1) % 5];
+            x2 += k[(sk + 2) % 5];
+            x3 += k[(sk + 3) % 5] + (uint64_t)sk;
+        }
+        if ((r & 1) == 0) {
+            x0 += x1;
+            x1 = rotl64(x1, rot[r & 7][0]) ^ x0;
+            x2 += x3;
+            x3 = rotl64(x3, rot[r & 7][1]) ^ x2;
+        } else {
+            x0 += x3;
+            x3 = rotl64(x3, rot[r & 7][0]) ^ x0;
+            x2 += x1;
+            x1 = rotl64(x1, rot[r & 7][1]) ^ x2;
+        }
+    }
+    o[0] = x0 + k[0];
+    o[1] = x1 + k[1];
+    o[2] = x2 + k[2];
+    o[3] = x3 + k[3] + 5;
+}
+
+// A reader of the stream from any position.
+struct SitmoStream {
+    uint64_t key0, block;
+    uint32_t word;  // next output within the block, 0..8
+    uint64_t o[4];
+    __device__ void seek(uint64_t t)
+    {
+        block = t >> 3;
+        word = (uint32_t)(t & 7);
+        threefish20(key0, block, o);
+    }
+    __device__ uint32_t next()
+    {
+        if (word == 8) {
+            ++block;
+            threefish20(key0, block, o);
+            word = 0;
+        }
+        const uint64_t w = o[word >> 1];
+        const uint32_t u = (word & 1) ? (uint32_t)(w >> 32) : (uint32_t)w;
+        ++word;
+        return u;
+    }
+    // generate_canonical<double, 53> over two outputs
+    __device__ double uniform()
+    {
+        const double lo = (double)next();
+        const double hi = (double)next();
+        const double sum = __dadd_rn(lo, __dmul_rn(hi, 4294967296.0));
+        const double r = __dmul_rn(sum, 5.42101086242752217e-20);  // 2^-64
+        return r >= 1.0 ? 0.99999999999999988898 : r;               // 1 - 2^-53
+    }
+};
+
+// Engine outputs per edge: next_edge draws 5 uniforms per level but the
+// last, which draws 1 (rmat_generator.h:80-89), two outputs per uniform.
+__host__ __device__ __forceinline__ uint64_t sitmo_outputs_per_edge(int scale)
+{
+    return 2ull * (5ull * (uint64_t)(scale - 1) + 1ull);
+}
+
+// next_edge (rmat_generator.h:91-140) on the reference stream: the same
+// quadrant recursion as rmat_attempt with the uniforms drawn from `rs`.
+__device__ void rmat_sitmo_edge(int scale, double a, double b, double c, double d,
+                                SitmoStream &rs, int64_t *src, int64_t *dst)
+{
+    double A = a, B = b, C = c, D = d;
+    int64_t si = 0, sj = 0;
+    int64_t bit = (int64_t)1 << (scale - 1);
+    for (;;) {
+        const double r = rs.uniform();
+        if (r > A) {
+            const double ab = __dadd_rn(A, B);
+            if (r <= ab) {
+                sj |= bit;
+            } else if (r <= __dadd_rn(ab, C)) {
+                si |= bit;
+            } else {
+                sj |= bit;
+                si |= bit;
+            }
+        }
+        if (bit == 1) { break; }
+        A = __dmul_rn(A, __ddiv_rn(__dadd_rn(9.5, rs.uniform()), 10.0));
+        B = __dmul_rn(B, __ddiv_rn(__dadd_rn(9.5, rs.uniform()), 10.0));
+        C = __dmul_rn(C, __ddiv_rn(__dadd_rn(9.5, rs.uniform()), 10.0));
+        D = __dmul_rn(D, __ddiv_rn(__dadd_rn(9.5, rs.uniform()), 10.0));
+        const double norm = __ddiv_rn(1.0, __dadd_rn(__dadd_rn(__dadd_rn(A, B), C), D));
+        A = __dmul_rn(A, norm);
+        B = __dmul_rn(B, norm);
+        C = __dmul_rn(C, norm);
+        D = __dsub_rn(1.0, __dadd_rn(__dadd_rn(A, B), C));
+        bit >>= 1;
+    }
+    *src = si;
+    *dst = sj;
+}
+
+// Edge i of rmat_fill (rmat_generator.h:145-175): drawn from stream position
+// i x outputs-per-edge, as the reference's discard() places it.  Self loops
+// are flagged for the serial re-roll.
+__global__ void rmat_sitmo_kernel(int scale, int64_t num_edges, double a, double b, double c,
+                                  double d, uint32_t seed, int64_t *src, int64_t *dst,
+                                  uint8_t *self_loop)
+{
+    const uint64_t per_edge = sitmo_outputs_per_edge(scale);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < num_edges;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        SitmoStream rs;
+        rs.key0 = seed;
+        rs.seek((uint64_t)i * per_edge);
+        int64_t s = 0, t = 0;
+        rmat_sitmo_edge(scale, a, b, c, d, rs, &s, &t);
+        src[i] = s;
+        dst[i] = t;
+        self_loop[i] = s == t ? 1 : 0;
+    }
+}
+
+// The serial re-roll of rmat_fill (rmat_generator.h:177-189): self loops in
+// edge order draw whole edges from the stream after the last generated edge
+// until they are not self loops.  One thread: the order is the point, and
+// self loops are few (about (a + d)^scale of the edges).  `list` holds the
+// self loops' edge indices in ascending order.
+__global__ void rmat_sitmo_reroll_kernel(int scale, int64_t num_edges, double a, double b,
+                                         double c, double d, uint32_t seed, const int64_t *list,
+                                         const int64_t *count, int64_t *src, int64_t *dst,
+                                         int *error)
+{
+    SitmoStream rs;
+    rs.key0 = seed;
+    rs.seek((uint64_t)num_edges * sitmo_outputs_per_edge(scale));
+    const int64_t total = *count;
+    uint64_t draws = 0;
+    for (int64_t k = 0; k < total; ++k) {
+        const int64_t i = list[k];
+        int64_t s = 0, t = 0;
+        do {
+            if (++draws > (uint64_t)kMaxAttempts * (uint64_t)(total + 1)) {
+                *error = 1;  // a degenerate A-D that only yields self loops
+                return;
+            }
+            rmat_sitmo_edge(scale, a, b, c, d, rs, &s, &t);
+        } while (s == t);
+        src[i] = s;
+        dst[i] = t;
+    }
+}
+
+// Generated edge k -> flipped (src < dst) packed key src << scale | dst.
+__global__ void flip_keys_kernel(const int64_t *src, const int64_t *dst, int64_t num_edges,
+                                 int scale, uint64_t *keys)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < num_edges;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t s = (uint64_t)src[i], t = (uint64_t)dst[i];
+        keys[i] = s < t ? (s << scale) | t : (t << scale) | s;
+    }
+}
+
+__global__ void iota_kernel(int64_t count, int64_t *out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        out[i] = i;
+    }
+}
+
 // Sort key of item idx in a permutation domain (vertex relabel / shuffle).
 __device__ __forceinline__ uint64_t perm_key(uint64_t seed, uint64_t idx, uint32_t tag)
 {
@@ -200,6 +412,8 @@ __global__ void scatter_rank_kernel(const uint32_t *sorted_v, int64_t n, uint32_
     }
 }
 
+// Packed key k -> edge (new_id of src, new_id of dst); new_id null: the
+// generator's own ids.
 __global__ void unpack_relabel_kernel(const uint64_t *packed, int64_t m, int scale,
                                       const uint32_t *new_id, int64_t *src, int64_t *dst)
 {
@@ -207,8 +421,8 @@ __global__ void unpack_relabel_kernel(const uint64_t *packed, int64_t m, int sca
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
          k += (int64_t)gridDim.x * blockDim.x) {
         uint64_t p = packed[k];
-        src[k] = new_id[p >> scale];
-        dst[k] = new_id[p & mask];
+        src[k] = new_id ? (int64_t)new_id[p >> scale] : (int64_t)(p >> scale);
+        dst[k] = new_id ? (int64_t)new_id[p & mask] : (int64_t)(p & mask);
     }
 }
 
@@ -893,8 +1107,13 @@ bd_status bd_graph_from_csr(int64_t num_vertices, int64_t num_arcs, const int64_
     return BD_OK;
 }
 
-bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, double c,
-                        double d, uint64_t seed, int32_t adjacency_order, bd_graph **out)
+}  // extern "C"
+
+namespace bd {
+namespace {
+
+bd_status check_rmat_args(int32_t scale, int64_t edge_factor, double a, double b, double c,
+                          double d, int32_t adjacency_order, bd_graph **out)
 {
     if (!out || scale < 1 || scale > 30 || edge_factor < 1 || edge_factor > 1024) {
         return BD_ERR_INVALID;
@@ -905,15 +1124,18 @@ bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, 
     if (adjacency_order < BD_ORDER_INSERTION || adjacency_order > BD_ORDER_HUB) {
         return BD_ERR_INVALID;
     }
-    BD_TRY(ensure_device());
+    return BD_OK;
+}
+
+// rmat_dataset_dump.cc:48-57 from flipped packed keys (keys.p, E of them):
+// sort + dedup, then either the seeded vertex relabel and edge shuffle
+// (permute) or the sorted list as it is, then the CSR.
+bd_status rmat_finish(int32_t scale, int64_t E, DevBuf<uint64_t> &keys,
+                      DevBuf<uint64_t> &keys_sorted, bool permute, uint64_t seed,
+                      int32_t adjacency_order, bd_graph **out)
+{
     const int64_t n = (int64_t)1 << scale;
-    const int64_t E = edge_factor << scale;
     cudaStream_t s = 0;
-    DevBuf<uint64_t> keys, keys_sorted;
-    if (keys.alloc(E) != cudaSuccess || keys_sorted.alloc(E) != cudaSuccess) { return BD_ERR_OOM; }
-    rmat_keys_kernel<<<grid_for(E), kThreads, 0, s>>>(scale, E, a, b, c, d, seed, keys.p);
-    BD_CUDA(cudaGetLastError());
-    // flip + sort + dedup (rmat_dataset_dump.cc:48-53)
     BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
         return cub::DeviceRadixSort::SortKeys(tmp, bytes, keys.p, keys_sorted.p, E, 0, 2 * scale, s);
     }, s));
@@ -924,28 +1146,33 @@ bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, 
     }, s));
     int64_t m = 0;
     BD_CUDA(cudaMemcpy(&m, num_unique.p, sizeof(int64_t), cudaMemcpyDeviceToHost));
-    // relabel (rmat_dataset_dump.cc:55): vertex with the k-th smallest key -> k
-    DevBuf<uint64_t> vkeys, vkeys_sorted;
+    const uint64_t *packed = keys.p;  // sorted, deduplicated
+    DevBuf<uint64_t> vkeys, vkeys_sorted, ekeys, ekeys_sorted;
     DevBuf<uint32_t> vidx, vidx_sorted, new_id;
-    if (vkeys.alloc(n) != cudaSuccess || vkeys_sorted.alloc(n) != cudaSuccess ||
-        vidx.alloc(n) != cudaSuccess || vidx_sorted.alloc(n) != cudaSuccess ||
-        new_id.alloc(n) != cudaSuccess) {
-        return BD_ERR_OOM;
+    if (permute) {
+        // relabel (rmat_dataset_dump.cc:55): vertex with the k-th smallest key -> k
+        if (vkeys.alloc(n) != cudaSuccess || vkeys_sorted.alloc(n) != cudaSuccess ||
+            vidx.alloc(n) != cudaSuccess || vidx_sorted.alloc(n) != cudaSuccess ||
+            new_id.alloc(n) != cudaSuccess) {
+            return BD_ERR_OOM;
+        }
+        perm_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(seed, kTagRelabel, n, vkeys.p, vidx.p);
+        BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
+            return cub::DeviceRadixSort::SortPairs(tmp, bytes, vkeys.p, vkeys_sorted.p, vidx.p,
+                                                   vidx_sorted.p, n, 0, 64, s);
+        }, s));
+        scatter_rank_kernel<<<grid_for(n), kThreads, 0, s>>>(vidx_sorted.p, n, new_id.p);
+        // shuffle (rmat_dataset_dump.cc:57): order edges by a keyed permutation
+        if (ekeys.alloc(m) != cudaSuccess || ekeys_sorted.alloc(m) != cudaSuccess) {
+            return BD_ERR_OOM;
+        }
+        edge_shuffle_keys_kernel<<<grid_for(m), kThreads, 0, s>>>(seed, m, ekeys.p);
+        BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
+            return cub::DeviceRadixSort::SortPairs(tmp, bytes, ekeys.p, ekeys_sorted.p, keys.p,
+                                                   keys_sorted.p, m, 0, 64, s);
+        }, s));
+        packed = keys_sorted.p;
     }
-    perm_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(seed, kTagRelabel, n, vkeys.p, vidx.p);
-    BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
-        return cub::DeviceRadixSort::SortPairs(tmp, bytes, vkeys.p, vkeys_sorted.p, vidx.p,
-                                               vidx_sorted.p, n, 0, 64, s);
-    }, s));
-    scatter_rank_kernel<<<grid_for(n), kThreads, 0, s>>>(vidx_sorted.p, n, new_id.p);
-    // shuffle (rmat_dataset_dump.cc:57): order edges by a keyed permutation
-    DevBuf<uint64_t> ekeys, ekeys_sorted;
-    if (ekeys.alloc(m) != cudaSuccess || ekeys_sorted.alloc(m) != cudaSuccess) { return BD_ERR_OOM; }
-    edge_shuffle_keys_kernel<<<grid_for(m), kThreads, 0, s>>>(seed, m, ekeys.p);
-    BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
-        return cub::DeviceRadixSort::SortPairs(tmp, bytes, ekeys.p, ekeys_sorted.p, keys.p,
-                                               keys_sorted.p, m, 0, 64, s);
-    }, s));
     int64_t *d_src = nullptr, *d_dst = nullptr;
     if (cudaMalloc(&d_src, sizeof(int64_t) * (m ? m : 1)) != cudaSuccess ||
         cudaMalloc(&d_dst, sizeof(int64_t) * (m ? m : 1)) != cudaSuccess) {
@@ -953,8 +1180,9 @@ bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, 
         cudaFree(d_dst);
         return BD_ERR_OOM;
     }
-    unpack_relabel_kernel<<<grid_for(m), kThreads, 0, s>>>(keys_sorted.p, m, scale, new_id.p,
-                                                           d_src, d_dst);
+    unpack_relabel_kernel<<<grid_for(m), kThreads, 0, s>>>(packed, m, scale,
+                                                           permute ? new_id.p : nullptr, d_src,
+                                                           d_dst);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) { e = cudaStreamSynchronize(s); }
     if (e != cudaSuccess) {
@@ -970,6 +1198,75 @@ bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, 
     vkeys.reset();
     vkeys_sorted.reset();
     return graph_from_device_edges(n, m, d_src, d_dst, adjacency_order, out);
+}
+
+}  // namespace
+}  // namespace bd
+
+extern "C" {
+
+bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, double c,
+                        double d, uint64_t seed, int32_t adjacency_order, bd_graph **out)
+{
+    BD_TRY(check_rmat_args(scale, edge_factor, a, b, c, d, adjacency_order, out));
+    BD_TRY(ensure_device());
+    const int64_t E = edge_factor << scale;
+    DevBuf<uint64_t> keys, keys_sorted;
+    if (keys.alloc(E) != cudaSuccess || keys_sorted.alloc(E) != cudaSuccess) { return BD_ERR_OOM; }
+    rmat_keys_kernel<<<grid_for(E), kThreads, 0, 0>>>(scale, E, a, b, c, d, seed, keys.p);
+    BD_CUDA(cudaGetLastError());
+    return rmat_finish(scale, E, keys, keys_sorted, true, seed, adjacency_order, out);
+}
+
+bd_status bd_graph_rmat_stream(int32_t scale, int64_t edge_factor, double a, double b, double c,
+                               double d, uint32_t stream_seed, int32_t permute,
+                               uint64_t permute_seed, int32_t adjacency_order, bd_graph **out)
+{
+    BD_TRY(check_rmat_args(scale, edge_factor, a, b, c, d, adjacency_order, out));
+    if (permute != 0 && permute != 1) { return BD_ERR_INVALID; }
+    BD_TRY(ensure_device());
+    const int64_t E = edge_factor << scale;
+    cudaStream_t s = 0;
+    DevBuf<int64_t> src, dst, loops, num_loops;
+    DevBuf<uint8_t> flag;
+    DevBuf<int> err;
+    if (src.alloc(E) != cudaSuccess || dst.alloc(E) != cudaSuccess || flag.alloc(E) != cudaSuccess ||
+        loops.alloc(E) != cudaSuccess || num_loops.alloc(1) != cudaSuccess ||
+        err.alloc(1) != cudaSuccess) {
+        return BD_ERR_OOM;
+    }
+    BD_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    rmat_sitmo_kernel<<<grid_for(E), kThreads, 0, s>>>(scale, E, a, b, c, d, stream_seed, src.p,
+                                                       dst.p, flag.p);
+    BD_CUDA(cudaGetLastError());
+    // the self loops' edge indices, in ascending order, for the serial re-roll
+    iota_kernel<<<grid_for(E), kThreads, 0, s>>>(E, loops.p);
+    BD_CUDA(cudaGetLastError());
+    DevBuf<int64_t> seq;
+    if (seq.alloc(E) != cudaSuccess) { return BD_ERR_OOM; }
+    BD_CUDA(cudaMemcpyAsync(seq.p, loops.p, sizeof(int64_t) * E, cudaMemcpyDeviceToDevice, s));
+    BD_CUDA(cub_run([&](void *tmp, size_t &bytes) {
+        return cub::DeviceSelect::Flagged(tmp, bytes, seq.p, flag.p, loops.p, num_loops.p, E, s);
+    }, s));
+    seq.reset();
+    rmat_sitmo_reroll_kernel<<<1, 1, 0, s>>>(scale, E, a, b, c, d, stream_seed, loops.p,
+                                             num_loops.p, src.p, dst.p, err.p);
+    BD_CUDA(cudaGetLastError());
+    int bad = 0;
+    BD_CUDA(cudaMemcpy(&bad, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (bad) { return BD_ERR_INVALID; }
+    DevBuf<uint64_t> keys, keys_sorted;
+    if (keys.alloc(E) != cudaSuccess) { return BD_ERR_OOM; }
+    flip_keys_kernel<<<grid_for(E), kThreads, 0, s>>>(src.p, dst.p, E, scale, keys.p);
+    BD_CUDA(cudaGetLastError());
+    BD_CUDA(cudaStreamSynchronize(s));
+    src.reset();
+    dst.reset();
+    loops.reset();
+    flag.reset();
+    if (keys_sorted.alloc(E) != cudaSuccess) { return BD_ERR_OOM; }
+    return rmat_finish(scale, E, keys, keys_sorted, permute != 0, permute_seed, adjacency_order,
+                       out);
 }
 
 bd_status bd_graph_grid(int64_t rows, int64_t cols, double delete_frac, uint64_t seed,

@@ -95,6 +95,11 @@ bd_status check_parents_device(const bd_graph *g, int64_t source, const int64_t 
 // has an arc to another label, or -1.
 bd_status check_components_device(const bd_graph *g, const int64_t *d_label, int32_t *ok,
                                   int64_t *bad_vertex);
+// The deterministic parent tree (bd_bfs.cu): for every vertex of depth
+// d > 0, the smallest neighbour of depth d - 1 in the CSR (off, adj), written
+// to parent; other entries are left as they are.  Queued on s.
+cudaError_t launch_min_parent(const int64_t *off, const uint32_t *adj, int64_t n,
+                              const int32_t *depth, int64_t *parent, cudaStream_t s);
 // BD_ORDER_HUB: builds the renumbered traversal CSR of a finished graph.
 bd_status graph_build_hub(bd_graph *g, cudaStream_t s);
 // Fills d_isolated from d_off.

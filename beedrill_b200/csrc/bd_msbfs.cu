@@ -1023,11 +1023,119 @@ __global__ void ms_extract_kernel(const int32_t *depth, const uint32_t *parent, 
         if (depth_out) { depth_out[v] = d; }
         if (parent_out) {
             if (d >= 0) {
-                parent_out[v] = (int64_t)(iperm ? iperm[par] : par);
+                parent_out[v] = (int64_t)(iperm && par < n ? iperm[par] : par);
             } else {
                 const int64_t g = off[v + 1] - off[v];
                 parent_out[v] = g != 0 ? -g : -1;
             }
+        }
+    }
+}
+
+// Every lane of one group in the single-source output format at once: root
+// (root0 + r) gets depth_out[(root0 + r) * n + v] and parent_out[...] for
+// every caller vertex v (caller ids, the reference's encoding: the source is
+// its own parent, unreached vertices -deg or -1).  One pass over the group's
+// state instead of one per lane: thread i of a CTA takes caller vertex
+// v0 + i of a tile of kMatThreads consecutive vertices, reads the vertex's
+// seen word, record count and records once (a record covers every lane one
+// provider delivered at one level, so the provider is renamed once per
+// record), notes for each reached lane which record holds it, and then
+// writes each root's row entry for its vertex: a CTA writes runs of
+// kMatThreads consecutive entries per row (2 KB of depths, 4 KB of
+// parents), streaming past L2.  Lanes whose vertex ran out of records are
+// read from the per-lane rows.  The per-thread tables live in shared
+// memory, column i for thread i (slot-major, so a warp's accesses fall in
+// 32 different banks); no thread reads another's column, so no barrier.
+struct MsOutParams {
+    const int32_t *depth;     // per-lane rows [n][R]
+    const uint32_t *parent;
+    const uint4 *rec;         // [n][kRecSlots]
+    const uint32_t *rec_cnt;  // [n]
+    const ull *seen;          // [n]
+    const int64_t *off;       // the caller's CSR offsets (unreached encoding)
+    const uint32_t *perm;     // caller id -> traversal id, or null
+    const uint32_t *iperm;    // traversal id -> caller id, or null
+    int64_t n;
+    int R;                    // lane stride of the rows
+    int lanes;                // roots in the group
+    int32_t *depth_out;       // row of the group's first root
+    int64_t *parent_out;
+};
+
+constexpr int kMatThreads = 512;
+constexpr uint8_t kMatRows = 0xFE;  // the lane's result is in the per-lane rows
+// per thread: a record slot per lane (64 B), a depth and a provider per
+// record (16 x 8 B)
+constexpr size_t kMatSmem = (size_t)kMatThreads * (64 + kRecSlots * 8);
+
+__global__ void __launch_bounds__(kMatThreads) ms_materialize_kernel(MsOutParams o)
+{
+    extern __shared__ uint32_t mat_smem[];
+    const int tid = threadIdx.x;
+    int32_t *rec_depth = reinterpret_cast<int32_t *>(mat_smem);   // [kRecSlots][threads]
+    uint32_t *rec_prov = mat_smem + kRecSlots * kMatThreads;      // [kRecSlots][threads]
+    uint8_t *slot = reinterpret_cast<uint8_t *>(mat_smem + 2 * kRecSlots * kMatThreads);
+    // slot: [64][threads]
+    const ull all = o.lanes >= 64 ? ~0ull : ((1ull << o.lanes) - 1);
+    const long long tiles = (o.n + kMatThreads - 1) / kMatThreads;
+    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int64_t v = tile * kMatThreads + tid;
+        if (v >= o.n) { continue; }
+        const int64_t t = o.perm ? (int64_t)__ldg(&o.perm[v]) : v;
+        const int64_t deg = __ldg(&o.off[v + 1]) - __ldg(&o.off[v]);
+        const ull s = __ldcs(&o.seen[t]) & all;
+        if (s) {
+            const unsigned cnt = min(__ldcs(&o.rec_cnt[t]), kRecSlots);
+            const uint4 *rv = o.rec + t * kRecSlots;
+            ull left = s;
+            for (unsigned k0 = 0; k0 < cnt && left; k0 += 4) {
+                uint4 x[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    x[j] = k0 + j < cnt ? __ldcs(&rv[k0 + j]) : make_uint4(0, 0, 0, 0);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    ull mask = (((ull)x[j].y << 32) | x[j].x) & left;
+                    if (!mask) { continue; }
+                    left &= ~mask;
+                    const unsigned k = k0 + j;
+                    // (a provider id out of range would only come from a
+                    // broken record; it is passed through, not followed)
+                    rec_depth[k * kMatThreads + tid] = (int32_t)x[j].w;
+                    rec_prov[k * kMatThreads + tid] =
+                        o.iperm && x[j].z < o.n ? __ldg(&o.iperm[x[j].z]) : x[j].z;
+                    do {
+                        const int r = __ffsll((long long)mask) - 1;
+                        mask &= mask - 1;
+                        slot[r * kMatThreads + tid] = (uint8_t)k;
+                    } while (mask);
+                }
+            }
+            while (left) {  // lanes past the vertex's records: the per-lane rows
+                const int r = __ffsll((long long)left) - 1;
+                left &= left - 1;
+                slot[r * kMatThreads + tid] = kMatRows;
+            }
+        }
+        const int64_t unreached = deg != 0 ? -deg : -1;
+        for (int r = 0; r < o.lanes; ++r) {
+            int32_t d = -1;
+            int64_t par = unreached;
+            if ((s >> r) & 1ull) {
+                const unsigned k = slot[r * kMatThreads + tid];
+                if (k < kRecSlots) {
+                    d = rec_depth[k * kMatThreads + tid];
+                    par = rec_prov[k * kMatThreads + tid];
+                } else {
+                    const uint32_t p = __ldcs(&o.parent[t * o.R + r]);
+                    d = __ldcs(&o.depth[t * o.R + r]);
+                    par = o.iperm && p < o.n ? __ldg(&o.iperm[p]) : p;
+                }
+            }
+            __stcs(&o.depth_out[(int64_t)r * o.n + v], d);
+            __stcs(&o.parent_out[(int64_t)r * o.n + v], par);
         }
     }
 }
@@ -1085,6 +1193,12 @@ struct bd_msbfs {
     bool frontier_clean = false;  // F and fb are all zero (kernels leave them so)
     MsCtrl last{};
     std::vector<unsigned long long> counts;
+    // opts.materialize: every root's results, written by each run
+    int32_t *out_depth = nullptr;   // [max_roots][n]
+    int64_t *out_parent = nullptr;  // [max_roots][n]
+    int mat_grid = 0;
+    // otherwise: one root's results, extracted when they are read
+    void *xbuf = nullptr;           // 8 n bytes
 };
 
 namespace bd {
@@ -1142,8 +1256,41 @@ MsParams ms_params(bd_msbfs *b, int group, int count)
     return p;
 }
 
+// Every lane of a finished group into its roots' output rows, and with
+// opts.min_parent each root's smallest-parent tree on the caller's CSR.
+bd_status ms_enqueue_materialize(bd_msbfs *b, int group, int count)
+{
+    const int64_t n = b->g->n;
+    MsOutParams o{};
+    const int64_t slice = n * (int64_t)b->R;
+    o.depth = b->depth + group * slice;
+    o.parent = b->parent + group * slice;
+    o.rec = b->drec + group * n * (int64_t)kRecSlots;
+    o.rec_cnt = b->drec_cnt + group * n;
+    o.seen = b->seen + group * n;
+    o.off = b->g->d_off;
+    o.perm = b->g->d_perm;
+    o.iperm = b->g->d_iperm;
+    o.n = n;
+    o.R = b->R;
+    o.lanes = count;
+    o.depth_out = b->out_depth + (int64_t)group * 64 * n;
+    o.parent_out = b->out_parent + (int64_t)group * 64 * n;
+    ms_materialize_kernel<<<b->mat_grid, kMatThreads, kMatSmem, b->stream>>>(o);
+    BD_CUDA(cudaGetLastError());
+    if (b->opts.min_parent) {
+        for (int r = 0; r < count; ++r) {
+            const int64_t row = ((int64_t)group * 64 + r) * n;
+            BD_CUDA(launch_min_parent(b->g->d_off, b->g->d_adj, n, b->out_depth + row,
+                                      b->out_parent + row, b->stream));
+        }
+    }
+    return BD_OK;
+}
+
 // One group: clear (its seen words, the frontier words), init, the
-// persistent kernel, the per-lane counts.
+// persistent kernel, the per-lane counts (and with opts.materialize the
+// roots' output rows).
 bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
 {
     const int64_t n = b->g->n;
@@ -1161,6 +1308,7 @@ bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
     BD_CUDA(cudaMemsetAsync(dst, 0, sizeof(unsigned long long) * 128, b->stream));
     ms_count_kernel<<<148 * 8, 256, 0, b->stream>>>(p.seen, p.off, n, p.all, count, dst);
     BD_CUDA(cudaGetLastError());
+    if (b->opts.materialize) { BD_TRY(ms_enqueue_materialize(b, group, count)); }
     return BD_OK;
 }
 
@@ -1244,6 +1392,9 @@ void ms_free(bd_msbfs *b)
     cudaFree(b->policy);
     cudaFree(b->heavy);
     cudaFree(b->heavy_cbase);
+    cudaFree(b->out_depth);
+    cudaFree(b->out_parent);
+    cudaFree(b->xbuf);
     if (b->ev0) { cudaEventDestroy(b->ev0); }
     if (b->ev1) { cudaEventDestroy(b->ev1); }
     if (b->stream) { cudaStreamDestroy(b->stream); }
@@ -1271,23 +1422,32 @@ cudaError_t ms_extract_async(bd_msbfs *b, int32_t root_index, int32_t *d_depth, 
     return cudaGetLastError();
 }
 
-bd_status ms_extract(bd_msbfs *b, int32_t root_index, int32_t *depth, int64_t *parent)
+// One root's depths or parents (caller ids, reference encoding) in device
+// memory: its materialized row, or extracted into the handle's buffer.
+bd_status ms_root_device(bd_msbfs *b, int32_t root_index, bool want_depth, const void **out)
 {
     BD_TRY(ms_check_root(b, root_index));
     BD_CUDA(cudaSetDevice(b->device));
     const int64_t n = b->g->n;
-    void *tmp = nullptr;
-    const size_t bytes = depth ? sizeof(int32_t) * n : sizeof(int64_t) * n;
-    BD_CUDA(cudaMalloc(&tmp, bytes));
-    cudaError_t e = ms_extract_async(b, root_index, depth ? static_cast<int32_t *>(tmp) : nullptr,
-                                     parent ? static_cast<int64_t *>(tmp) : nullptr);
-    if (e == cudaSuccess) {
-        e = cudaMemcpyAsync(depth ? (void *)depth : (void *)parent, tmp, bytes,
-                            cudaMemcpyDeviceToHost, b->stream);
+    if (b->opts.materialize) {
+        *out = want_depth ? (const void *)(b->out_depth + (int64_t)root_index * n)
+                          : (const void *)(b->out_parent + (int64_t)root_index * n);
+        return BD_OK;
     }
-    if (e == cudaSuccess) { e = cudaStreamSynchronize(b->stream); }
-    cudaFree(tmp);
-    if (e != cudaSuccess) { return cuda_fail(e, "msbfs extract", __FILE__, __LINE__); }
+    BD_CUDA(ms_extract_async(b, root_index, want_depth ? static_cast<int32_t *>(b->xbuf) : nullptr,
+                             want_depth ? nullptr : static_cast<int64_t *>(b->xbuf)));
+    *out = b->xbuf;
+    return BD_OK;
+}
+
+bd_status ms_extract(bd_msbfs *b, int32_t root_index, int32_t *depth, int64_t *parent)
+{
+    const void *src = nullptr;
+    BD_TRY(ms_root_device(b, root_index, depth != nullptr, &src));
+    const size_t bytes = depth ? sizeof(int32_t) * b->g->n : sizeof(int64_t) * b->g->n;
+    BD_CUDA(cudaMemcpyAsync(depth ? (void *)depth : (void *)parent, src, bytes,
+                            cudaMemcpyDeviceToHost, b->stream));
+    BD_CUDA(cudaStreamSynchronize(b->stream));
     return BD_OK;
 }
 
@@ -1322,6 +1482,10 @@ bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *o
     if (o.heavy_degree <= 0) { o.heavy_degree = 4096; }
     if (o.heavy_chunk <= 0) { o.heavy_chunk = 2048; }
     if (o.spin_limit <= 0) { o.spin_limit = kMsDefaultSpin; }
+    if (o.materialize < 0 || o.materialize > 1 || o.min_parent < 0 || o.min_parent > 1) {
+        return BD_ERR_INVALID;
+    }
+    if (o.min_parent) { o.materialize = 1; }
     if (g->n > (int64_t)UINT32_MAX) { return BD_ERR_LIMIT; }
     BD_TRY(ensure_device());
     auto *b = new bd_msbfs();
@@ -1357,7 +1521,26 @@ bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *o
              cudaMalloc(&b->ql[i], sizeof(uint32_t) * b->cap_large) == cudaSuccess &&
              cudaMalloc(&b->qlb[i], sizeof(ull) * b->cap_large) == cudaSuccess;
     }
+    if (ok && o.materialize) {
+        const size_t rows = (size_t)n * (size_t)max_roots;
+        ok = cudaMalloc(&b->out_depth, sizeof(int32_t) * rows) == cudaSuccess &&
+             cudaMalloc(&b->out_parent, sizeof(int64_t) * rows) == cudaSuccess;
+    } else if (ok) {
+        ok = cudaMalloc(&b->xbuf, sizeof(int64_t) * n) == cudaSuccess;
+    }
     if (!ok) { return fail(BD_ERR_OOM); }
+    if (o.materialize) {
+        int per_sm = 0, sms = 0;
+        if (cudaFuncSetAttribute(ms_materialize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kMatSmem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ms_materialize_kernel,
+                                                          kMatThreads, kMatSmem) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess ||
+            per_sm < 1) {
+            return fail(BD_ERR_CUDA);
+        }
+        b->mat_grid = per_sm * sms;
+    }
     int per_sm = 0, sms = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)ms_pick(b->block),
                                                       b->block, 0) != cudaSuccess ||
@@ -1459,17 +1642,25 @@ bd_status bd_msbfs_get_parents(bd_msbfs *b, int32_t root_index, int64_t *parent)
 bd_status bd_msbfs_check(bd_msbfs *b, int32_t root_index, int32_t *ok)
 {
     if (!b || !ok) { return BD_ERR_INVALID; }
-    BD_TRY(ms_check_root(b, root_index));
-    BD_CUDA(cudaSetDevice(b->device));
-    int64_t *parent = nullptr;
-    BD_CUDA(cudaMalloc(&parent, sizeof(int64_t) * b->g->n));
-    cudaError_t e = ms_extract_async(b, root_index, nullptr, parent);
-    if (e == cudaSuccess) { e = cudaStreamSynchronize(b->stream); }
-    const bd_status st = e == cudaSuccess
-                             ? check_parents_device(b->g, b->sources[root_index], parent, ok, nullptr)
-                             : cuda_fail(e, "msbfs extract", __FILE__, __LINE__);
-    cudaFree(parent);
-    return st;
+    const void *parent = nullptr;
+    BD_TRY(ms_root_device(b, root_index, false, &parent));
+    BD_CUDA(cudaStreamSynchronize(b->stream));
+    return check_parents_device(b->g, b->sources[root_index], static_cast<const int64_t *>(parent),
+                                ok, nullptr);
+}
+
+// Borrowed device pointers to one root's materialized results.
+bd_status bd_msbfs_device_results(bd_msbfs *b, int32_t root_index, const int32_t **depth,
+                                  const int64_t **parent)
+{
+    if (!b) { return BD_ERR_INVALID; }
+    if (!b->opts.materialize) { return BD_ERR_STATE; }
+    const void *d = nullptr, *p = nullptr;
+    BD_TRY(ms_root_device(b, root_index, true, &d));
+    BD_TRY(ms_root_device(b, root_index, false, &p));
+    if (depth) { *depth = static_cast<const int32_t *>(d); }
+    if (parent) { *parent = static_cast<const int64_t *>(p); }
+    return BD_OK;
 }
 
 bd_status bd_msbfs_count_traversed_edges(bd_msbfs *b, int32_t root_index, int64_t *edges,

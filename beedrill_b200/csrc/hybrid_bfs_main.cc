@@ -267,6 +267,9 @@ bool run_batched(const bfs_args &args, beedrill::graph &g, int alg, const std::v
     if (find_tuning(args, g.num_vertices(), &tn)) { tn.apply(&opts); }
     if (alg == BD_ALG_TOP_DOWN) { opts.force_dir = 0; }
     if (alg == BD_ALG_BOTTOM_UP) { opts.force_dir = 1; }
+    // every root's parent_ complete when the run ends, as in the reference
+    opts.materialize = 1;
+    opts.min_parent = args.min_parent ? 1 : 0;
     beedrill::batched_bfs bfs(g, (int32_t)roots.size(), &opts);
     beedrill::policy pol;
     if (alg == BD_ALG_LEARNED && find_policy(args, &pol)) { bfs.set_policy(pol); }
@@ -277,8 +280,7 @@ bool run_batched(const bfs_args &args, beedrill::graph &g, int alg, const std::v
     double ms_all = 0, inv_sum = 0;
     for (size_t s = 0; s < roots.size(); ++s) {
         if (args.check_results) {
-            int32_t ok = 0;
-            beedrill::throw_if(bd_msbfs_check(bfs.handle(), (int32_t)s, &ok), "check");
+            const bool ok = bfs.check((int32_t)s);
             printf("Checking results...\n%s\n", ok ? "PASS" : "FAIL");
             success = success && ok;
         }

@@ -5,9 +5,12 @@ BFS from each of 64 roots (lcg(0) picker of hybrid_bfs_main.cc:136-144) on a
 seeded RMAT scale-24 graph (A=.57 B=.19 C=.19 D=.05, edge factor 16,
 deduplicated, symmetrised; int64 offsets, uint32 ids), generated on the
 device.  Per root, time covers run_* only, as in the reference
-(hybrid_bfs_main.cc:267-282): clear() is outside, the source setup inside.
-TEPS = count_num_traversed_edges() / time; the metric is the harmonic mean of
-the per-root GTEPS (combined.cc:124-128).
+(hybrid_bfs_main.cc:267-282): clear() is outside, the source setup inside,
+and so is the writing of every root's results (int32 depths and int64
+parents, caller ids, the reference's encoding: run_beamer leaves parent_
+complete).  TEPS = count_num_traversed_edges() / time; the metric is the
+harmonic mean of the per-root GTEPS (combined.cc:124-128).  A batched group's
+time is spread evenly over its roots.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -18,7 +21,8 @@ ranks.
 
 --impl reference times the reference's own CPU build (oracle/_ref/hybrid_bfs,
 the unmodified hybrid_bfs sources compiled as a Cilk serial elision: 1 core)
-on the same graph, written as an el64 file, over a bounded sample of roots.
+on the same graph, written as an el64 file by a child process, over a
+bounded sample of roots (8 per step).
 """
 from __future__ import annotations
 
@@ -153,7 +157,27 @@ def reference_cpu_run(el64_path: str, trials: int, timeout: float):
     return rows, out[-400:]
 
 
+REF_ROOTS_PER_STEP = 8
+
+
+def write_graph_el64(path: str, scale: int) -> int:
+    """Writes the benchmark graph as an el64 file from a child process, so
+    the process that times the reference maps none of this repository's
+    native code.  Returns the child's exit code."""
+    code = ("import sys; sys.path.insert(0, %r); import beedrill_b200 as bd; "
+            "g = bd.Graph.rmat(%d, %d, seed=%d); g.write_el64(%r); "
+            "print(g.num_vertices(), g.num_edges())" % (ROOT, scale, EDGE_FACTOR, GRAPH_SEED, path))
+    out = subprocess.run([sys.executable, "-c", code], stdout=subprocess.PIPE,
+                         stderr=subprocess.STDOUT, text=True, timeout=1800)
+    return out.returncode, out.stdout.strip().splitlines()[-1:] or [""]
+
+
 def impl_reference(args):
+    """The reference's own CPU build (oracle/_ref/hybrid_bfs: the unmodified
+    hybrid_bfs sources compiled as a Cilk serial elision, one pinned core)
+    on the benchmark graph.  One step = a bounded sample of the workload:
+    REF_ROOTS_PER_STEP roots of the lcg(0) sequence, in the order the GPU
+    arm takes them (warm-up steps first)."""
     world, rank, local = dist_setup()
     if rank != 0:
         return 0
@@ -161,40 +185,48 @@ def impl_reference(args):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/hybrid_bfs was not built (reference sources absent at build time)"}))
         return 0
-    import beedrill_b200 as bd
-    g = bd.Graph.rmat(SCALE, EDGE_FACTOR, seed=GRAPH_SEED)
-    n, m = g.num_vertices(), g.num_edges()
     with tempfile.TemporaryDirectory(dir=os.environ.get("BD_TMP", None)) as tmp:
         path = os.path.join(tmp, f"rmat{SCALE}.el64")
-        g.write_el64(path)
-        g.close()
-        trials = args.warmup + args.steps
+        rc, last = write_graph_el64(path, SCALE)
+        if rc != 0:
+            print(json.dumps({"impl": "reference",
+                              "unavailable": f"graph generation failed: {last[0][-200:]}"}))
+            return 0
+        n, m = (int(x) for x in last[0].split())
+        trials = (args.warmup + args.steps) * REF_ROOTS_PER_STEP
         t0 = time.time()
         rows, tail = reference_cpu_run(path, trials, timeout=3000)
         wall = time.time() - t0
     if not rows or len(rows) < trials:
         print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {tail}"}))
         return 0
-    timed = rows[args.warmup:]
+    timed = rows[args.warmup * REF_ROOTS_PER_STEP:]
     gteps = [e / (ms * 1e-3) / 1e9 for e, ms in timed]
     value = hmean(gteps)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": float(np.mean([ms for _, ms in timed])), "higher_is_better": True,
+        "ms_per_step": float(np.sum([ms for _, ms in timed]) / args.steps),
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "i64", "data": "synthetic",
-        "config": {"workload": f"rmat-scale{SCALE}-ef{EDGE_FACTOR} lcg(0) roots, one root per step",
+        "config": {"workload": f"rmat-scale{SCALE}-ef{EDGE_FACTOR} seed {GRAPH_SEED}, "
+                               f"{REF_ROOTS_PER_STEP} lcg(0) roots per step (a bounded sample of "
+                               f"the 64-root step)",
                    "scale": SCALE, "edge_factor": EDGE_FACTOR, "graph_seed": GRAPH_SEED,
-                   "num_vertices": n, "num_edges": m},
+                   "num_vertices": n, "num_edges": m, "roots_per_step": REF_ROOTS_PER_STEP,
+                   "results": "parent_ complete per root (the reference's run_beamer)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": f"{args.steps} timed roots after {args.warmup} warm-up roots of "
-                                   f"lcg(0), reference serial-elision build on 1 pinned core; "
-                                   f"process wall {wall:.0f} s incl. el64 load + graph build"},
+                         "sample": f"{len(timed)} timed roots after "
+                                   f"{args.warmup * REF_ROOTS_PER_STEP} warm-up roots of lcg(0), "
+                                   f"reference serial-elision build on 1 pinned core; process "
+                                   f"wall {wall:.0f} s incl. el64 load + graph build"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
 
+
+DEFAULT_MODES = "plain,learned,batched,batched_rule,plain_traversal,batched_traversal"
 
 WORKLOADS = {
     # the headline: RMAT scale 24, 64 roots
@@ -203,13 +235,15 @@ WORKLOADS = {
     "rmat22": {"kind": "rmat", "scale": 22, "roots": 64},
     # 256 roots in four 64-lane groups of one captured launch
     "rmat20-256": {"kind": "rmat", "scale": 20, "roots": 256},
-    # the largest single-GPU case
-    "rmat26": {"kind": "rmat", "scale": 26, "roots": 64},
+    # the largest single-GPU case (materialized rows of 64 roots take 51.5 GB,
+    # so only the batched way keeps every root's results)
+    "rmat26": {"kind": "rmat", "scale": 26, "roots": 64, "modes": "batched,plain_traversal"},
     # graphs inside the learned policies' training range (scales 16-18),
     # seeds the trainer never used: 64-root batches, learned vs rule
     "policy16-18": {"kind": "policy_set", "scales": (16, 17, 18), "seeds": (7001, 7002, 7003)},
     # high-diameter contrast: 4096 x 4096 grid, 1% of its edges deleted
-    "grid4096": {"kind": "grid", "rows": 4096, "cols": 4096, "delete": 0.01, "roots": 64},
+    "grid4096": {"kind": "grid", "rows": 4096, "cols": 4096, "delete": 0.01, "roots": 64,
+                 "modes": "plain,batched,batched_rule"},
     # 512 independent RMAT graphs (scales 10-18, edge factors 4-32), one root each
     "packed512": {"kind": "packed", "graphs": 512},
     # connected components (components.cc) on the same RMAT scale-24 graph
@@ -486,11 +520,12 @@ def main():
     ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS),
                     help="rmat24 is the headline; the others are the remaining evaluation cases")
     ap.add_argument("--scale", type=int, default=None, help="override the RMAT scale")
-    ap.add_argument("--modes", default="plain,learned,batched,batched_rule",
-                    help="subset of plain,learned,batched,batched_rule to run (profiling runs "
-                         "use one, to hold only that handle on the device)")
+    ap.add_argument("--modes", default=None,
+                    help="subset of plain,learned,batched,batched_rule,plain_traversal,"
+                         "batched_traversal to run (default: the workload's set; profiling "
+                         "runs use one, to hold only that handle on the device)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-roots", type=int, default=3)
+    ap.add_argument("--cpu-roots", type=int, default=8)
     ap.add_argument("--order", default="hub", choices=["insertion", "sorted", "degree", "hub"],
                     help="adjacency order / numbering the kernels run on (same results for all)")
     args = ap.parse_args()
@@ -542,9 +577,8 @@ def main():
     roots = g.pick_roots(rank, num_roots)
 
     # CPU baseline: the reference's own build on a bounded sample of the same
-    # workload, in the background while the GPU is measured (rank 0, N = 1).
-    cpu_thread = None
-    cpu_result = {}
+    # workload (rank 0, N = 1), run after the GPU's timed region, not beside it.
+    el64 = None
     tmpdir = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_BIN) \
             and m <= 300_000_000:
@@ -552,74 +586,118 @@ def main():
         el64 = os.path.join(tmpdir.name, "graph.el64")
         g.write_el64(el64)
 
-        def cpu_job():
-            t0 = time.time()
-            rows, tail = reference_cpu_run(el64, args.cpu_roots, timeout=1200)
-            cpu_result["rows"], cpu_result["tail"] = rows, tail
-            cpu_result["wall"] = time.time() - t0
-
-        cpu_thread = threading.Thread(target=cpu_job, daemon=True)
-        cpu_thread.start()
-
-    # the ways of running the roots: one launch per root under the Beamer
-    # rule and under the learned policy; all roots batched (64 per group)
-    # under the learned push/pull policy and under the plain rule
-    want = set(args.modes.split(","))
+    # The ways of running the roots.  Materialized (what a caller gets: every
+    # root's int32 depths and int64 parents in caller ids and the reference's
+    # encoding, in device memory, when the step ends):
+    #   plain         one launch per root, Beamer alpha=15 / beta=18
+    #   learned       one launch per root, the learned top-down/bottom-up policy
+    #   batched       64 roots per group, one captured launch, learned push/pull
+    #   batched_rule  the same under the alpha rule alone
+    # Traversal only (results left in the kernels' own form, as before):
+    #   plain_traversal, batched_traversal
+    want = [x for x in (args.modes or w.get("modes", DEFAULT_MODES)).split(",") if x]
     from beedrill_b200 import policy as P
-    plain = bd.HybridBFS(g, alg="beamer_hybrid") if "plain" in want else None
-    learned = None
+    import torch
+    dev = f"cuda:{local}"
+    handles = {}
+    if any(x in want for x in ("plain", "plain_traversal")):
+        handles["plain"] = bd.HybridBFS(g, alg="beamer_hybrid")
     if "learned" in want and os.path.exists(P.DEFAULT_PATH):
-        learned = bd.HybridBFS(g, alg="learned")
-        P.Policy.load().install(learned)
-    batched = batched_rule = None
-    if "batched" in want:
-        batched = bd.BatchedBFS(g, num_roots)
-        if os.path.exists(P.BATCHED_PATH):
-            P.Policy.load(P.BATCHED_PATH).install(batched)
-    if "batched_rule" in want and os.path.exists(P.BATCHED_PATH):
-        batched_rule = bd.BatchedBFS(g, num_roots)
+        handles["learned"] = bd.HybridBFS(g, alg="learned")
+        P.Policy.load().install(handles["learned"])
+    for name, mat, pol in (("batched", True, True), ("batched_rule", True, False),
+                           ("batched_traversal", False, True)):
+        if name in want:
+            handles[name] = bd.BatchedBFS(g, num_roots, materialize=mat)
+            if pol and os.path.exists(P.BATCHED_PATH):
+                P.Policy.load(P.BATCHED_PATH).install(handles[name])
+    out_depth = out_parent = None
+    if any(x in want for x in ("plain", "learned")):
+        out_depth = torch.empty((num_roots, n), dtype=torch.int32, device=dev)
+        out_parent = torch.empty((num_roots, n), dtype=torch.int64, device=dev)
     groups = (num_roots + 63) // 64
 
     # A 512 MB write (> the 126 MB L2) before each way's runs, so that no
     # way starts with another's graph or state in cache.
-    import torch
-    flush_buf = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    flush_buf = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
 
     def flush_l2():
         flush_buf.fill_(1)
         torch.cuda.synchronize(local)
 
+    def run_way(name):
+        if name in ("plain", "learned"):
+            h = handles[name]
+            ms, edges, reached, _ = h.run_many_into(roots, out_depth.data_ptr(),
+                                                    out_parent.data_ptr())
+            return ms, edges, reached
+        if name == "plain_traversal":
+            ms, edges, reached, _ = handles["plain"].run_many(roots, with_reached=True)
+            return ms, edges, reached
+        h = handles[name]
+        st = h.run(roots)
+        m_c, n_c = h.counts()
+        return np.full(num_roots, st.ms / num_roots), m_c, n_c
+
+    order_run = [x for x in ("plain", "learned", "plain_traversal", "batched", "batched_rule",
+                             "batched_traversal")
+                 if x in want and (x in handles or x == "plain_traversal" and "plain" in handles)]
+
     def one_step():
         out = {}
-        for name, h in (("plain", plain), ("learned", learned)):
-            if h is None:
-                continue
+        for name in order_run:
             flush_l2()
-            ms, edges, reached, e2e = h.run_many(roots, with_reached=True)
-            out[name] = (ms, edges, reached, e2e)
-        for name, h in (("batched", batched), ("batched_rule", batched_rule)):
-            if h is None:
-                continue
-            flush_l2()
-            t0 = time.perf_counter()
-            st = h.run(roots)
-            m_c, n_c = h.counts()
-            wall = (time.perf_counter() - t0) * 1e3
-            out[name] = (np.full(num_roots, st.ms / num_roots), m_c, n_c, wall)
+            out[name] = run_way(name)
         return out
+
+    # e2e: the public call a user makes, host buffers in and out: roots
+    # uploaded by the call, the run, m_c / n_c read back, and every root's
+    # parent array (int64, n entries) copied to pinned host memory.
+    e2e_ways = [x for x in ("batched", "plain") if x in order_run]
+    rows_bytes = 8 * n * num_roots
+    host_rows = torch.empty((num_roots if rows_bytes <= (16 << 30) else 1, n), dtype=torch.int64,
+                            pin_memory=True) if e2e_ways else None
+
+    def e2e_step(name):
+        flush_l2()
+        t0 = time.perf_counter()
+        if name == "batched":
+            h = handles[name]
+            h.run(roots)
+            m_c, _ = h.counts()
+            for i in range(num_roots):
+                row = host_rows[i % host_rows.shape[0]]
+                h.parents_to(i, row.data_ptr())
+        else:
+            _, m_c, _, _ = handles["plain"].run_many_into(roots, out_depth.data_ptr(),
+                                                          out_parent.data_ptr())
+            if host_rows.shape[0] == num_roots:
+                host_rows.copy_(out_parent, non_blocking=False)
+            else:
+                for i in range(num_roots):
+                    host_rows[0].copy_(out_parent[i], non_blocking=False)
+        torch.cuda.synchronize(local)
+        return m_c, (time.perf_counter() - t0) * 1e3
 
     for _ in range(args.warmup):
         one_step()
+        for name in e2e_ways:
+            e2e_step(name)
 
     def barrier():
         if world > 1:
             dist.barrier()
 
     barrier()
-    runs = []
+    torch.cuda.synchronize(local)
+    runs, e2e_runs = [], {name: [] for name in e2e_ways}
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
             runs.append(one_step())
+        for _ in range(args.steps):
+            for name in e2e_ways:
+                e2e_runs[name].append(e2e_step(name))
+    torch.cuda.synchronize(local)
     barrier()
 
     def summarize(name):
@@ -627,40 +705,46 @@ def main():
         edges = np.concatenate([r[name][1] for r in runs])
         reached = np.concatenate([r[name][2] for r in runs])
         gteps = edges / (ms * 1e-3) / 1e9
-        e2e = hmean(np.concatenate([r[name][1] / (r[name][3] / num_roots * 1e-3) / 1e9 for r in runs]))
         step_ms = float(np.mean([r[name][0].sum() for r in runs]))
         if name.startswith("batched"):
             # one shared CSR pass per 64-root group, plus every root's depth
             # and parent outputs, spread evenly over the group's roots
             per_root = np.zeros(len(reached))
-            for s in range(0, len(reached), num_roots):
+            for s0 in range(0, len(reached), num_roots):
                 for g0 in range(0, num_roots, 64):
-                    lo, hi = s + g0, s + min(g0 + 64, num_roots)
+                    lo, hi = s0 + g0, s0 + min(g0 + 64, num_roots)
                     b = 8.0 * (n + 1) + 8.0 * m + 12.0 * reached[lo:hi].sum()
                     per_root[lo:hi] = b / (hi - lo)
             b_alg = per_root
         else:
             b_alg = 8.0 * (n + 1) + 8.0 * edges + 12.0 * reached
-        return {"gteps": hmean(gteps), "e2e": e2e, "step_ms": step_ms, "ms": ms, "edges": edges,
-                "reached": reached, "b_alg": b_alg}
+        out = {"gteps": hmean(gteps), "step_ms": step_ms, "ms": ms, "edges": edges,
+               "reached": reached, "b_alg": b_alg}
+        if name in e2e_runs:
+            per = [m_c / (wall / num_roots * 1e-3) / 1e9 for m_c, wall in e2e_runs[name]]
+            out["e2e"] = hmean(np.concatenate(per))
+            out["e2e_step_ms"] = float(np.mean([w for _, w in e2e_runs[name]]))
+        return out
 
     modes = {name: summarize(name) for name in runs[0]}
     first = next(iter(modes.values()))
     if not all(np.array_equal(modes[k]["edges"], first["edges"]) for k in modes):
         raise RuntimeError("modes disagree on m_c")
-    # the headline: the learned + batched way, else the best that ran
-    best = max(modes, key=lambda k: (k in ("batched", "learned"), modes[k]["gteps"]))
+    # the headline: the learned + batched way with results materialized,
+    # else the best materialized way that ran, else the best of the rest
+    best = max(modes, key=lambda k: (k == "batched", "traversal" not in k, modes[k]["gteps"]))
     head = modes[best]
-    value_rank, e2e_rank, step_ms = head["gteps"], head["e2e"], head["step_ms"]
+    value_rank, step_ms = head["gteps"], head["step_ms"]
+    e2e_rank = head.get("e2e", 0.0)
     if world > 1:
-        step_ms, value, e2e_value = reduce_over_ranks(step_ms, value_rank, e2e_rank,
-                                                      device=f"cuda:{local}")
+        step_ms, value, e2e_value = reduce_over_ranks(step_ms, value_rank, e2e_rank, device=dev)
     else:
         value, e2e_value = value_rank, e2e_rank
 
-    # roofline of the dominant kernel of the headline mode: B_alg per root
-    # = 8(n+1) + 4*(2 m_c) + 12 n_c for one-root launches; a batched group
-    # shares one CSR pass among its 64 roots
+    # roofline of the headline way over its timed launches: SURVEY's B_alg
+    # (one CSR pass per group + every root's int32 depth and int64 parent of
+    # each reached vertex) over the device time of the groups, which covers
+    # the traversal kernel, the per-lane counts and the result rows
     achieved = float(head["b_alg"].sum() / (head["ms"].sum() * 1e-3) / 1e9)
     peak, peak_kind = peaks()
     traffic = None
@@ -668,7 +752,22 @@ def main():
     if os.path.exists(tpath):
         with open(tpath) as f:
             traffic = json.load(f).get(f"{args.workload}-{best}", {}).get("bytes_per_launch")
+    kernels = {}
+    if "batched" in modes and "batched_traversal" in modes:
+        t_all = modes["batched"]["step_ms"] / groups
+        t_trav = modes["batched_traversal"]["step_ms"] / groups
+        rows = 12.0 * n * min(num_roots, 64)
+        kernels = {
+            "traversal_ms_per_group": t_trav,
+            "traversal_GBps_csr_pass": (8.0 * (n + 1) + 8.0 * m) / (t_trav * 1e-3) / 1e9,
+            "result_rows_ms_per_group": t_all - t_trav,
+            "result_rows_GBps_written": rows / max(t_all - t_trav, 1e-9) / 1e6 if t_all > t_trav
+            else None,
+            "note": "traversal = the batched_traversal way's group time; result rows = the "
+                    "difference to the materialized way (12 B x n x 64 written per group)",
+        }
     ms = head["ms"]
+    bi, bo = 8 * num_roots, 16 * num_roots + 8 * n * num_roots
     line = {
         "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
@@ -676,6 +775,9 @@ def main():
         "config": {
             "workload": f"{desc}, {num_roots} roots per step",
             "mode": best,
+            "results": "materialized: every root's int32 depths and int64 parents (caller ids, "
+                       "reference encoding) in device memory when the step ends"
+                       if "traversal" not in best else "traversal only",
             "scale": scale, "edge_factor": EDGE_FACTOR if scale else None, "graph_seed": graph_seed,
             "num_vertices": n, "num_edges": m, "roots": num_roots, "root_seed": rank,
             "l2": "inputs larger than L2 (CSR %.2f GB), and L2 flushed (512 MB write) before "
@@ -684,7 +786,10 @@ def main():
             "graph_build_s": round(gen_s, 2),
             "adjacency_order": args.order,
         },
-        "modes": {k: {"gteps": v["gteps"], "e2e_gteps": v["e2e"], "ms_per_step": v["step_ms"]}
+        "modes": {k: {kk: vv for kk, vv in (("gteps", v["gteps"]), ("ms_per_step", v["step_ms"]),
+                                             ("e2e_gteps", v.get("e2e")),
+                                             ("e2e_ms_per_step", v.get("e2e_step_ms")))
+                      if vv is not None}
                   for k, v in modes.items()},
         "plain_beamer_gteps": modes["plain"]["gteps"] if "plain" in modes else None,
         "learned_gteps": modes["learned"]["gteps"] if "learned" in modes else None,
@@ -694,39 +799,47 @@ def main():
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind,
                      "note": ("B_alg per 64-root group = 8(n+1) + 8m + 12 sum n_c" if best.startswith("batched")
-                              else "B_alg = 8(n+1) + 8 m_c + 12 n_c per root") + " over the run time"},
-        "e2e": {"value": e2e_value, "unit": UNIT,
-                "h2d_bytes_per_step": 8 * num_roots,
-                "d2h_bytes_per_step": 16 * num_roots,
-                "note": "public API call per step: root upload, clear + runs, m_c/n_c download"},
-        "gpu_launches": args.steps * (3 * num_roots * ((plain is not None) + (learned is not None))
-                                      + 3 * groups * ((batched is not None)
-                                                      + (batched_rule is not None))),
+                              else "B_alg = 8(n+1) + 8 m_c + 12 n_c per root") +
+                             " over the device time of the " + best + " way (traffic: ncu DRAM "
+                             "bytes of the launches of one group or root, profiles/traffic.json)",
+                     "kernels": kernels or None},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bi,
+                "d2h_bytes_per_step": bo,
+                "note": f"public API per step ({best if best in e2e_runs else 'none'}): the run "
+                        "(roots uploaded by the call), m_c / n_c read back, and every root's int64 "
+                        "parent array copied to pinned host memory"},
+        # kernels per root (init, traversal, result rows, counters) or per
+        # group (init, traversal, per-lane counts, result rows); the e2e
+        # passes launch the same kernels again
+        "gpu_launches": args.steps * (
+            sum({"plain": 4 * num_roots, "learned": 4 * num_roots, "plain_traversal": 3 * num_roots,
+                 "batched": 4 * groups, "batched_rule": 4 * groups,
+                 "batched_traversal": 3 * groups}[x] for x in order_run)
+            + sum({"batched": 4 * groups, "plain": 4 * num_roots}[x] for x in e2e_ways)),
         "clocks": clocks.summary(),
     }
-    if cpu_thread is not None:
-        cpu_thread.join()
-        rows = cpu_result.get("rows")
+    if el64 is not None:
+        t0 = time.time()
+        rows, tail = reference_cpu_run(el64, args.cpu_roots, timeout=1200)
+        wall = time.time() - t0
         if rows:
             cg = [e / (t * 1e-3) / 1e9 for e, t in rows]
             line["cpu_baseline"] = {
                 "value": hmean(cg), "unit": UNIT, "cores": 1, "kind": "reference",
                 "sample": f"{len(rows)} lcg(0) roots of the same graph, reference serial-elision "
-                          f"build (oracle/_ref/hybrid_bfs) pinned to 1 core; wall "
-                          f"{cpu_result['wall']:.0f} s incl. el64 load + graph build"}
+                          f"build (oracle/_ref/hybrid_bfs) pinned to 1 core, after the GPU's "
+                          f"timed region; wall {wall:.0f} s incl. el64 load + graph build"}
         else:
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
-                                    "sample": f"failed: {cpu_result.get('tail')}"}
+                                    "sample": f"failed: {tail}"}
         tmpdir.cleanup()
     if rank == 0:
         print(json.dumps(line))
-    for h in (plain, learned, batched, batched_rule):
-        if h is not None:
-            h.close()
+    for h in handles.values():
+        h.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
-
 
 if __name__ == "__main__":
     sys.exit(main())

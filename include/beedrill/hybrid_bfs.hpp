@@ -554,6 +554,19 @@ public:
         throw_if(bd_msbfs_get_parents(h_, i, p.data()), "parents");
         return p;
     }
+    // Root i's parent_ in device memory (opts.materialize handles only).
+    const int64_t *device_parents(int32_t i)
+    {
+        const int64_t *p = nullptr;
+        throw_if(bd_msbfs_device_results(h_, i, nullptr, &p), "device_parents");
+        return p;
+    }
+    bool check(int32_t i)
+    {
+        int32_t ok = 0;
+        throw_if(bd_msbfs_check(h_, i, &ok), "check");
+        return ok != 0;
+    }
     std::vector<bd_step> steps()
     {
         int64_t count = 0;

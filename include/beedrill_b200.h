@@ -16,6 +16,8 @@
  *   create_graph_from_edge_list on in-memory edges          -> bd_graph_from_edges
  *   graph::check (graph_base.h:110-134)                     -> bd_graph_check
  *   generator/rmat_dataset_dump.cc (seeded, on the device)  -> bd_graph_rmat
+ *   rmat_edge_generator + rmat_fill (rmat_generator.h:70-193)
+ *     + rmat_dataset_dump.cc:48-53, the reference's stream  -> bd_graph_rmat_stream
  *   pick_random_vertex + lcg (hybrid_bfs_main.cc:136-144)   -> bd_graph_pick_roots
  *   hybrid_bfs::hybrid_bfs(graph&) (hybrid_bfs.cc:10-18)    -> bd_bfs_create
  *   hybrid_bfs::clear (hybrid_bfs.cc:433-443)               -> bd_bfs_clear
@@ -142,6 +144,20 @@ bd_status bd_graph_from_csr(int64_t num_vertices, int64_t num_arcs, const int64_
  * permuted and edge order shuffled by `seed`. */
 bd_status bd_graph_rmat(int32_t scale, int64_t edge_factor, double a, double b, double c,
                         double d, uint64_t seed, int32_t adjacency_order, bd_graph **out);
+/* RMAT edges drawn exactly as the reference's generator draws them
+ * (generator/rmat_generator.h:70-193 with rmat_edge_generator(.., seed =
+ * stream_seed)): the sitmo::prng_engine stream (generator/prng_engine.hpp)
+ * through libstdc++'s uniform_real_distribution<double>, edge i from stream
+ * position i x 2 x (5 (scale-1) + 1), self loops re-rolled serially from the
+ * stream's tail in edge order, as rmat_fill does; then flipped, sorted and
+ * deduplicated (rmat_dataset_dump.cc:48-53).  edge_factor << scale edges.
+ * permute = 0: the graph keeps the generator's vertex ids and the sorted
+ * edge order -- the reference's edge list before its thread-count-dependent
+ * relabel and shuffle (rmat_dataset_dump.cc:55-57); permute = 1: the seeded
+ * relabel and shuffle of bd_graph_rmat (keyed by permute_seed) follow. */
+bd_status bd_graph_rmat_stream(int32_t scale, int64_t edge_factor, double a, double b, double c,
+                               double d, uint32_t stream_seed, int32_t permute,
+                               uint64_t permute_seed, int32_t adjacency_order, bd_graph **out);
 /* rows x cols grid, vertex r*cols+c, 4-neighbour edges (horizontal edges
  * first, row by row, then vertical), each deleted independently with
  * probability delete_frac by a seeded Philox draw.  The high-diameter
@@ -199,6 +215,14 @@ bd_status bd_bfs_run_multi(bd_bfs *b, const int64_t *sources, int64_t count,
  * copy of the roots to the device to the copy of the results back. */
 bd_status bd_bfs_run_many(bd_bfs *b, const int64_t *sources, int64_t k, double *ms_out,
                           int64_t *edges_out, int64_t *reached_out, double *e2e_ms);
+/* bd_bfs_run_many, and root i's results end in d_depth[i * n ...] (int32,
+ * -1 unreached) and d_parent[i * n ...] (int64, caller ids, the reference's
+ * encoding), device arrays of k x n entries, written inside each root's
+ * timed region: the trial loop with every trial's parent_ kept
+ * (hybrid_bfs_main.cc:252-302). */
+bd_status bd_bfs_run_many_into(bd_bfs *b, const int64_t *sources, int64_t k, int32_t *d_depth,
+                               int64_t *d_parent, double *ms_out, int64_t *edges_out,
+                               int64_t *reached_out, double *e2e_ms);
 bd_status bd_bfs_get_depths(bd_bfs *b, int32_t *depth);
 bd_status bd_bfs_get_parents(bd_bfs *b, int64_t *parent);
 bd_status bd_bfs_device_ptrs(bd_bfs *b, const int32_t **depth, const int64_t **parent);
@@ -268,6 +292,16 @@ typedef struct bd_msbfs_opts {
     int32_t heavy_degree;  /* pull: lists longer than this are cut into chunks
                               shared by all warps; 0 = default (4096)           */
     int32_t heavy_chunk;   /* arcs per such chunk; 0 = default (2048)           */
+    int32_t materialize;   /* 1: every run ends with each root's int32 depths
+                              and int64 parents (caller ids, the reference's
+                              encoding) in device memory owned by the handle,
+                              as run_beamer leaves parent_ complete
+                              (hybrid_bfs.cc:152-191); the run's time covers
+                              it.  Costs 12 bytes x n x max_roots of device
+                              memory.  0: results are extracted when read   */
+    int32_t min_parent;    /* 1 (implies materialize): each root's parent(v) is
+                              the smallest neighbour one level up, as
+                              bd_bfs_opts.min_parent -- bit-exact trees        */
 } bd_msbfs_opts;
 void bd_msbfs_default_opts(bd_msbfs_opts *opts);
 /* max_roots: capacity of one call (results of all roots stay readable). */
@@ -283,6 +317,12 @@ bd_status bd_msbfs_count_traversed_edges(bd_msbfs *b, int32_t root_index, int64_
                                          int64_t *reached);
 /* hybrid_bfs::check (hybrid_bfs.cc:281-379) of one root's parents. */
 bd_status bd_msbfs_check(bd_msbfs *b, int32_t root_index, int32_t *ok);
+/* Borrowed device pointers (n entries each, valid until the next run or
+ * destroy) to one root's materialized depths and parents; BD_ERR_STATE
+ * unless the handle was made with opts.materialize.  Counterpart of
+ * bd_bfs_device_ptrs: the reference's parent_ (hybrid_bfs.h:43) per root. */
+bd_status bd_msbfs_device_results(bd_msbfs *b, int32_t root_index, const int32_t **depth,
+                                  const int64_t **parent);
 /* Step records of the last group of the last call (found = new lanes). */
 bd_status bd_msbfs_get_steps(bd_msbfs *b, bd_step *steps, int64_t capacity, int64_t *count);
 /* Installs (params != NULL) or removes the learned push/pull policy of the

@@ -623,6 +623,142 @@ void or_rmat_edges(int scale, int64_t num_edges, double a, double b, double c,
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* The reference generator's own stream (rmat_generator.h, prng_engine.hpp)   */
+/* ------------------------------------------------------------------------ */
+
+/* sitmo::prng_engine (generator/prng_engine.hpp, MIT licence, vendored by the
+ * reference): Threefish-256 as specified for Skein 1.3, cut to 20 rounds,
+ * tweak zero, key (seed, 0, 0, 0), encrypting the counter (block, 0, 0, 0).
+ * Words are mixed in pairs (x, y) -> (x + y, rotl(y, R) ^ (x + y)); even
+ * rounds pair words 0-1 and 2-3, odd rounds 0-3 and 2-1 (the Threefish-256
+ * permutation); subkey s = (k[s], k[s+1], k[s+2], k[s+3] + s) mod-5 indexed,
+ * k[4] = C240 ^ k0 ^ k1 ^ k2 ^ k3, is added before every fourth round and
+ * after the last (s = 5). */
+void or_threefish20(uint64_t key0, uint64_t block, uint64_t out[4])
+{
+    static const int rot[8][2] = {{14, 16}, {52, 57}, {23, 40}, {5, 37},
+                                  {25, 33}, {46, 12}, {58, 22}, {32, 32}};
+    uint64_t k[5] = {key0, 0, 0, 0, 0};
+    k[4] = 0x1BD11BDAA9FC1A22ull ^ k[0] ^ k[1] ^ k[2] ^ k[3];
+    uint64_t x[4] = {block, 0, 0, 0};
+    for (int r = 0; r <= 20; ++r) {
+        if (r % 4 == 0) {
+            int sub = r / 4;
+            for (int w = 0; w < 4; ++w) { x[w] += k[(sub + w) % 5]; }
+            x[3] += (uint64_t)sub;
+        }
+        if (r == 20) { break; }
+        int a = 0, b = (r % 2 == 0) ? 1 : 3, c = 2, d = (r % 2 == 0) ? 3 : 1;
+        int ra = rot[r % 8][0], rc = rot[r % 8][1];
+        x[a] += x[b];
+        x[b] = ((x[b] << ra) | (x[b] >> (64 - ra))) ^ x[a];
+        x[c] += x[d];
+        x[d] = ((x[d] << rc) | (x[d] >> (64 - rc))) ^ x[c];
+    }
+    for (int w = 0; w < 4; ++w) { out[w] = x[w]; }
+}
+
+/* 32-bit output t of the engine seeded with `seed`: half (low for even t,
+ * high for odd t) of word (t % 8) / 2 of block t / 8. */
+uint32_t or_sitmo_output(uint32_t seed, uint64_t t)
+{
+    uint64_t o[4];
+    or_threefish20(seed, t >> 3, o);
+    uint64_t w = o[(t & 7) >> 1];
+    return (t & 1) ? (uint32_t)(w >> 32) : (uint32_t)w;
+}
+
+/* A sequential reader of the stream that keeps the current block. */
+typedef struct {
+    uint32_t seed;
+    uint64_t t, block;
+    uint64_t o[4];
+    int have;
+} or_sitmo;
+
+static uint32_t sitmo_next(or_sitmo *g)
+{
+    uint64_t blk = g->t >> 3;
+    if (!g->have || blk != g->block) {
+        or_threefish20(g->seed, blk, g->o);
+        g->block = blk;
+        g->have = 1;
+    }
+    uint64_t w = g->o[(g->t & 7) >> 1];
+    uint32_t u = (g->t & 1) ? (uint32_t)(w >> 32) : (uint32_t)w;
+    g->t += 1;
+    return u;
+}
+
+/* libstdc++'s generate_canonical<double, 53> over a 32-bit engine (two
+ * outputs: (u0 + u1 * 2^32) / 2^64, one rounding at the sum; a result of 1
+ * becomes nextafter(1, 0)), which uniform_real_distribution<double>(0, 1)
+ * returns unchanged. */
+static double sitmo_uniform(or_sitmo *g)
+{
+    double sum = 0.0, scale = 1.0;
+    for (int k = 0; k < 2; ++k) {
+        sum += (double)sitmo_next(g) * scale;
+        scale *= 4294967296.0;
+    }
+    double r = sum / scale;
+    return r >= 1.0 ? 1.0 - 1.0 / 9007199254740992.0 : r;
+}
+
+/* next_edge (rmat_generator.h:91-140) on the reference stream. */
+static void sitmo_next_edge(int scale, double a, double b, double c, double d, or_sitmo *g,
+                            int64_t *src, int64_t *dst)
+{
+    double A = a, B = b, C = c, D = d;
+    int64_t si = 0, sj = 0;
+    int64_t bit = (int64_t)1 << (scale - 1);
+    for (;;) {
+        double r = sitmo_uniform(g);
+        if (r > A) {
+            if (r <= A + B) { sj |= bit; }
+            else if (r <= A + B + C) { si |= bit; }
+            else { sj |= bit; si |= bit; }
+        }
+        if (bit == 1) { break; }
+        A *= (9.5 + sitmo_uniform(g)) / 10;
+        B *= (9.5 + sitmo_uniform(g)) / 10;
+        C *= (9.5 + sitmo_uniform(g)) / 10;
+        D *= (9.5 + sitmo_uniform(g)) / 10;
+        {
+            double norm = 1.0 / (A + B + C + D);
+            A *= norm;
+            B *= norm;
+            C *= norm;
+        }
+        D = 1.0 - (A + B + C);
+        bit >>= 1;
+    }
+    *src = si;
+    *dst = sj;
+}
+
+/* rmat_fill (rmat_generator.h:145-193) run serially: edge after edge from
+ * the start of the stream, then every self loop, in edge order, re-rolled
+ * with further edges from where the stream stands.  Returns 0, or -1 when
+ * a degenerate A-D keeps producing self loops. */
+int or_rmat_stream_edges(int scale, int64_t num_edges, double a, double b, double c,
+                         double d, uint32_t seed, int64_t *src, int64_t *dst)
+{
+    or_sitmo g = {seed, 0, 0, {0, 0, 0, 0}, 0};
+    for (int64_t i = 0; i < num_edges; ++i) {
+        sitmo_next_edge(scale, a, b, c, d, &g, &src[i], &dst[i]);
+    }
+    int64_t draws = 0;
+    for (int64_t i = 0; i < num_edges; ++i) {
+        while (src[i] == dst[i]) {
+            if (++draws > (int64_t)OR_MAX_ATTEMPTS * (num_edges + 1)) { return -1; }
+            sitmo_next_edge(scale, a, b, c, d, &g, &src[i], &dst[i]);
+        }
+    }
+    return 0;
+}
+
 typedef struct { uint64_t key; uint64_t idx; } or_keyed;
 
 static int cmp_keyed(const void *pa, const void *pb)

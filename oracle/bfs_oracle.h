@@ -101,6 +101,19 @@ void or_rmat_edges(int scale, int64_t num_edges, double a, double b, double c,
 int64_t or_rmat_finish(int scale, int64_t num_edges, uint64_t seed,
                        int64_t *src, int64_t *dst);
 
+/* ---- the reference generator's own stream, restated ---------------------- */
+/* Threefish-256 cut to 20 rounds, key (key0, 0, 0, 0), zero tweak, on the
+ * counter (block, 0, 0, 0): the block function of sitmo::prng_engine
+ * (generator/prng_engine.hpp). */
+void or_threefish20(uint64_t key0, uint64_t block, uint64_t out[4]);
+/* Output t (0-based) of sitmo::prng_engine(seed). */
+uint32_t or_sitmo_output(uint32_t seed, uint64_t t);
+/* rmat_edge_generator(2^scale, a, b, c, d, seed) + rmat_fill
+ * (rmat_generator.h:70-193) run serially: edges in generation order after
+ * the self-loop re-roll.  Returns 0, -1 if re-rolls never end. */
+int or_rmat_stream_edges(int scale, int64_t num_edges, double a, double b, double c,
+                         double d, uint32_t seed, int64_t *src, int64_t *dst);
+
 /* The project's grid generator (vertex r*cols+c, 4-neighbour edges, each
  * deleted with probability delete_frac by a seeded Philox draw). */
 int64_t or_grid_edges(int64_t rows, int64_t cols, double delete_frac, uint64_t seed,

@@ -70,6 +70,13 @@ def lib() -> ctypes.CDLL:
         L.or_rmat_finish.restype = c_int64
         L.or_grid_edges.argtypes = [c_int64, c_int64, c_double, c_uint64, i64p, i64p]
         L.or_grid_edges.restype = c_int64
+        L.or_threefish20.argtypes = [c_uint64, c_uint64, POINTER(c_uint64)]
+        L.or_threefish20.restype = None
+        L.or_sitmo_output.argtypes = [ctypes.c_uint32, c_uint64]
+        L.or_sitmo_output.restype = ctypes.c_uint32
+        L.or_rmat_stream_edges.argtypes = [c_int, c_int64, c_double, c_double, c_double,
+                                           c_double, ctypes.c_uint32, i64p, i64p]
+        L.or_rmat_stream_edges.restype = c_int
         _lib = L
     return _lib
 
@@ -252,6 +259,37 @@ def rmat_graph(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, d=0.05
     if m < 0:
         raise MemoryError("oracle generator allocation failed")
     return 1 << scale, src[:m].copy(), dst[:m].copy()
+
+
+def rmat_stream_edges(scale: int, num_edges: int, a=0.57, b=0.19, c=0.19, d=0.05,
+                      seed: int = 0):
+    """Edges of the reference generator (rmat_edge_generator(2^scale, a, b,
+    c, d, seed) + rmat_fill, rmat_generator.h:70-193, run serially) in
+    generation order, self loops re-rolled."""
+    src = np.empty(num_edges, np.int64)
+    dst = np.empty(num_edges, np.int64)
+    if lib().or_rmat_stream_edges(scale, num_edges, a, b, c, d, seed, _p(src, c_int64),
+                                  _p(dst, c_int64)):
+        raise ValueError("self loops never end for these RMAT parameters")
+    return src, dst
+
+
+def dedup_sorted(src: np.ndarray, dst: np.ndarray):
+    """flip_edges, sort_edges, dedup_edges (edge_list_utils.h:14-56): the
+    edge list with src < dst, sorted by (src, dst), without repeats."""
+    lo = np.minimum(src, dst)
+    hi = np.maximum(src, dst)
+    pairs = np.unique(np.stack([lo, hi], axis=1), axis=0)
+    return pairs[:, 0].copy(), pairs[:, 1].copy()
+
+
+def rmat_stream_graph(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, d=0.05,
+                      seed: int = 0):
+    """(n, src, dst): the reference generator's deduplicated, sorted edge
+    list (rmat_dataset_dump.cc:43-53), before its relabel and shuffle."""
+    src, dst = rmat_stream_edges(scale, edge_factor << scale, a, b, c, d, seed)
+    s, t = dedup_sorted(src, dst)
+    return 1 << scale, s, t
 
 
 def grid_graph(rows: int, cols: int, delete_frac: float = 0.01, seed: int = 0):

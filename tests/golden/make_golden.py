@@ -32,6 +32,13 @@ What it writes, and where each number comes from:
   the verdict of the reference's own components::check on each
   (oracle/_ref/ref_components_check).  `python tests/golden/make_golden.py
   --components` rewrites only this file.
+* ref_gen.npz -- oracle/_ref/ref_gen_edges (the reference's own RMAT
+  generator, rmat_generator.h, run serially, plus the flip / sort / dedup of
+  rmat_dataset_dump.cc:48-53) on six cases (scales 8-14, several A-D,
+  seeds 0-12345, one where most edges are self loops): edge counts and the
+  sha256 of the generated list (after the self-loop re-roll) and of the
+  deduplicated sorted list; the scale-10 case keeps both lists.
+  `python tests/golden/make_golden.py --generator` rewrites only this file.
 * ref_check.npz -- hybrid_bfs::check run by the reference itself
   (oracle/_ref/ref_check) on parent arrays of graph500-scale10.el64: the
   reference's beamer_hybrid tree of each of its 8 roots, and for each root
@@ -314,14 +321,65 @@ def components_fixture(tmp):
     np.savez_compressed(os.path.join(HERE, "ref_components.npz"), **arrays)
 
 
+# (scale, edge factor, a, b, c, d, seed) of the generator fixture; the first
+# case keeps its full edge lists, the others their sha256.  The last one
+# makes most edges self loops, so the serial re-roll runs long.
+GEN_CASES = [
+    (10, 16, 0.57, 0.19, 0.19, 0.05, 0),
+    (12, 16, 0.57, 0.19, 0.19, 0.05, 0),
+    (11, 4, 0.45, 0.25, 0.25, 0.05, 7),
+    (14, 16, 0.57, 0.19, 0.19, 0.05, 12345),
+    (9, 32, 0.7, 0.1, 0.1, 0.1, 3),
+    (8, 8, 0.9, 0.03, 0.03, 0.04, 11),
+]
+
+
+def ref_gen_edges(case, tmp):
+    """The reference generator's edges for one case (oracle/_ref/ref_gen_edges):
+    generation order after the self-loop re-roll, and the deduplicated,
+    sorted list of rmat_dataset_dump.cc:48-53."""
+    path = os.path.join(tmp, "gen.bin")
+    subprocess.run([os.path.join(O.REF_DIR, "ref_gen_edges")] + [str(x) for x in case] + [path],
+                   check=True)
+    with open(path, "rb") as f:
+        raw = f.read()
+    assert raw[:8] == b"BDGEN001"
+    nv, e = np.frombuffer(raw[8:24], np.int64)
+    gen = np.frombuffer(raw[24:24 + 16 * e], np.int64).reshape(e, 2)
+    m = int(np.frombuffer(raw[24 + 16 * e:32 + 16 * e], np.int64)[0])
+    ded = np.frombuffer(raw[32 + 16 * e:], np.int64).reshape(m, 2)
+    return int(nv), gen, ded
+
+
+def generator_fixture(tmp):
+    """ref_gen.npz: per case, the parameters, the generated and deduplicated
+    edge counts and the sha256 of both lists (int64 src, dst pairs, in
+    order); the first case also keeps both lists whole."""
+    arrays = {"cases": np.array([(c[0], c[1], c[6]) for c in GEN_CASES], np.int64),
+              "params": np.array([c[2:6] for c in GEN_CASES], np.float64)}
+    for i, case in enumerate(GEN_CASES):
+        nv, gen, ded = ref_gen_edges(case, tmp)
+        arrays[f"{i}.counts"] = np.array([nv, len(gen), len(ded),
+                                          int((gen[:, 0] == gen[:, 1]).sum())], np.int64)
+        arrays[f"{i}.gen_sha"] = np.frombuffer(hashlib.sha256(gen.tobytes()).digest(), np.uint8)
+        arrays[f"{i}.ded_sha"] = np.frombuffer(hashlib.sha256(ded.tobytes()).digest(), np.uint8)
+        if i == 0:
+            arrays["0.gen"] = gen
+            arrays["0.ded"] = ded
+    np.savez_compressed(os.path.join(HERE, "ref_gen.npz"), **arrays)
+
+
 def main():
     O.build()
-    if "--components" in sys.argv[1:] or "--check" in sys.argv[1:]:
+    flags = ("--components", "--check", "--generator")
+    if any(f in sys.argv[1:] for f in flags):
         with tempfile.TemporaryDirectory() as tmp:
             if "--components" in sys.argv[1:]:
                 components_fixture(tmp)
             if "--check" in sys.argv[1:]:
                 check_fixture(tmp)
+            if "--generator" in sys.argv[1:]:
+                generator_fixture(tmp)
         return
     if not os.path.exists(os.path.join(O.REF_DIR, "ref_dump")):
         sys.exit("reference builds missing: the reference sources are needed")
@@ -383,6 +441,7 @@ def main():
         }
         components_fixture(tmp)
         check_fixture(tmp)
+        generator_fixture(tmp)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
         f.write("\n")

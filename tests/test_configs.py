@@ -6,12 +6,14 @@
     packed into one CSR and traversed from one root each in one launch.
   * The largest single-GPU case: RMAT scale 26 with 64 roots batched.
 
-Depths are compared bit-exactly with the oracle's BFS and parents go through
-the oracle's check() wherever the oracle finishes in seconds; at scale 26 the
-64 batched roots are compared with the single-source kernel (a different
-kernel with a different traversal order) and one root with the oracle.
+Depths are compared bit-exactly with the oracle's BFS and every root's
+parents go through the oracle's check() (the oracle runs in a thread pool on
+the host cores; its C calls release the GIL).  At scale 26 the 64 batched
+roots are compared with the single-source kernel (a different kernel with a
+different traversal order), and four of them with the oracle as well.
 """
 import os
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import pytest
@@ -21,6 +23,25 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 bd = pytest.importorskip("beedrill_b200")
+
+
+def _pool():
+    return ThreadPoolExecutor(max(1, min(16, os.cpu_count() or 1)))
+
+
+def _oracle_verdict(off, adj, root, depth, parent, m_c, n_c):
+    """Failure strings for one root's device results against the oracle."""
+    want = O.bfs_depth(off, adj, root)
+    bad = []
+    if not np.array_equal(depth, want):
+        bad.append("depths differ")
+    if not O.check(off, adj, root, parent):
+        bad.append("check() failed")
+    if m_c is not None and O.count_traversed(off, parent) != m_c:
+        bad.append("m_c differs")
+    if n_c is not None and int((want >= 0).sum()) != n_c:
+        bad.append("n_c differs")
+    return bad
 
 
 def _batched(g, roots):
@@ -37,16 +58,18 @@ def test_scale22_64_roots_one_launch_each():
     roots = g.pick_roots(0, 64)
     bfs = bd.HybridBFS(g)
     _, edges, _ = bfs.run_many(roots)
-    for i, root in enumerate(roots):
-        root = int(root)
-        bfs.clear()
-        bfs.run(root)
-        depth = bfs.depths()
-        assert np.array_equal(depth, O.bfs_depth(off, adj, root)), i
-        par = bfs.parents()
-        if i % 4 == 0:
-            assert O.check(off, adj, root, par), i
-        assert edges[i] == O.count_traversed(off, par), i
+    failures = []
+    with _pool() as pool:
+        jobs = []
+        for i, root in enumerate(roots):
+            root = int(root)
+            bfs.clear()
+            bfs.run(root)
+            jobs.append((i, pool.submit(_oracle_verdict, off, adj, root, bfs.depths(),
+                                        bfs.parents(), int(edges[i]), None)))
+        for i, job in jobs:
+            failures += [f"root {i}: {msg}" for msg in job.result()]
+    assert not failures, failures[:10]
 
 
 def test_batched_256_roots_scale20():
@@ -57,15 +80,14 @@ def test_batched_256_roots_scale20():
     st = ms.run(roots)
     assert st.ms > 0
     m_c, n_c = ms.counts()
-    for i, root in enumerate(roots):
-        root = int(root)
-        depth = O.bfs_depth(off, adj, root)
-        assert np.array_equal(ms.depths(i), depth), i
-        assert n_c[i] == int((depth >= 0).sum()), i
-        if i % 8 == 0:
-            par = ms.parents(i)
-            assert O.check(off, adj, root, par), i
-            assert m_c[i] == O.count_traversed(off, par), i
+    failures = []
+    with _pool() as pool:
+        jobs = [(i, pool.submit(_oracle_verdict, off, adj, int(root), ms.depths(i), ms.parents(i),
+                                int(m_c[i]), int(n_c[i])))
+                for i, root in enumerate(roots)]
+        for i, job in jobs:
+            failures += [f"root {i}: {msg}" for msg in job.result()]
+    assert not failures, failures[:10]
 
 
 def test_packed_512_graphs_one_root_each():
@@ -107,8 +129,12 @@ def test_scale26_batched_64_roots():
     ms.close()
     bfs.close()
     off, adj = g.csr()
-    root = int(roots[0])
-    ms = _batched(g, roots[:1])
-    ms.run(roots[:1])
-    assert np.array_equal(ms.depths(0), O.bfs_depth(off, adj, root))
-    assert O.check(off, adj, root, ms.parents(0))
+    ms = _batched(g, roots)
+    ms.run(roots)
+    m_c, n_c = ms.counts()
+    picks = (0, 21, 42, 63)
+    with _pool() as pool:
+        jobs = [(i, pool.submit(_oracle_verdict, off, adj, int(roots[i]), ms.depths(i),
+                                ms.parents(i), int(m_c[i]), int(n_c[i]))) for i in picks]
+        failures = [f"root {i}: {msg}" for i, job in jobs for msg in job.result()]
+    assert not failures, failures

@@ -87,3 +87,61 @@ def test_256_roots_scale18():
     _, edges, _ = single.run_many(roots)
     m_c, _ = ms.counts()
     assert np.array_equal(m_c, edges)
+
+
+@pytest.mark.parametrize("order", [bd.ORDER_INSERTION, bd.ORDER_HUB])
+def test_materialized_rows_equal_the_oracle(order):
+    """materialize=True: the run itself leaves every root's depths and
+    parents (caller ids, the reference's encoding) in device memory, written
+    by one pass over each group's state.  Every lane of three groups (a
+    partial last group, a duplicate root and a root of degree zero) must
+    equal the oracle, and the rows read through the device pointers must
+    equal the rows the copy-out path returns."""
+    g = bd.Graph.rmat(15, 8, seed=48, order=order)
+    off, adj = g.csr()
+    deg = np.diff(off)
+    roots = list(g.pick_roots(4, 150))
+    roots[7] = roots[6]
+    roots[140] = int(np.flatnonzero(deg == 0)[0])
+    ms = bd.BatchedBFS(g, 150, materialize=True)
+    for _ in range(2):  # the second run replays the captured graph
+        ms.run(roots)
+    _check_all(ms, off, adj, roots)
+    n = g.num_vertices()
+    for i in (0, 63, 64, 149):
+        dp, pp = ms.device_results(i)
+        assert np.array_equal(_device_to_host(dp, n, np.int32), ms.depths(i))
+        assert np.array_equal(_device_to_host(pp, n, np.int64), ms.parents(i))
+
+
+def _device_to_host(addr, n, dtype):
+    """n elements at a borrowed device address, copied to a host array
+    (through torch, which reads the CUDA array interface)."""
+    torch = pytest.importorskip("torch")
+
+    class View:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": np.dtype(dtype).str,
+                                    "data": (addr, False), "version": 3}
+
+    return torch.as_tensor(View(), device="cuda:0").cpu().numpy()
+
+
+@pytest.mark.parametrize("order", [bd.ORDER_DEGREE, bd.ORDER_HUB])
+def test_batched_min_parent_bit_exact(order):
+    """min_parent=True: every root's parent tree is the smallest neighbour
+    one level up, bit-exact against the oracle's min-parent tree, on 64
+    roots at scale 16 (both numberings)."""
+    g = bd.Graph.rmat(16, seed=49, order=order)
+    off, adj = g.csr()
+    roots = g.pick_roots(0, 64)
+    ms = bd.BatchedBFS(g, 64, min_parent=True)
+    ms.run(roots)
+    m_c, _ = ms.counts()
+    for i, root in enumerate(roots):
+        root = int(root)
+        depth = O.bfs_depth(off, adj, root)
+        assert np.array_equal(ms.depths(i), depth)
+        want = O.min_parent(off, adj, root, depth)
+        got = ms.parents(i)
+        assert np.array_equal(got, want), f"lane {i}: min-parent tree differs"
+        assert m_c[i] == O.count_traversed(off, got)

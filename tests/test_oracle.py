@@ -5,6 +5,7 @@ sources (oracle/_ref, see tests/golden/make_golden.py).  These tests run on
 CPU only and are the reason the oracle may be trusted as the parity checker
 for the device path.
 """
+import ctypes
 import hashlib
 import json
 import os
@@ -202,3 +203,60 @@ def test_el64_header_rules(tmp_path):
     assert O.el64_header(write(b" --format el64 --num_edges 0 --num_vertices 2 --is_deduped\n"))[0] == -3
     assert O.el64_header(write(b" --format el64 --num_edges 1 --num_vertices 2 --is_deduped"))[0] == -2
     assert O.el64_header(write(b" --format el64 --bogus --num_edges 1 --num_vertices 2 --is_deduped\n"))[0] == -2
+
+
+def _gen_cases(golden_dir):
+    d = np.load(os.path.join(golden_dir, "ref_gen.npz"))
+    for i, ((scale, ef, seed), (a, b, c, dd)) in enumerate(zip(d["cases"], d["params"])):
+        yield i, int(scale), int(ef), float(a), float(b), float(c), float(dd), int(seed), d
+
+
+def test_reference_stream_restatement_matches_the_reference_generator(golden_dir):
+    """The oracle's restatement of the reference generator (sitmo stream,
+    libstdc++ uniform doubles, next_edge, rmat_fill's serial self-loop
+    re-roll; then flip / sort / dedup) gives, on every fixture case, the
+    reference's own generated list and deduplicated list (ref_gen_edges,
+    tests/golden/ref_gen.npz) byte for byte."""
+    import hashlib
+    for i, scale, ef, a, b, c, d, seed, fx in _gen_cases(golden_dir):
+        src, dst = O.rmat_stream_edges(scale, ef << scale, a, b, c, d, seed)
+        gen = np.stack([src, dst], axis=1)
+        counts = fx[f"{i}.counts"]
+        assert len(gen) == counts[1] and (src != dst).all(), i
+        assert hashlib.sha256(gen.tobytes()).digest() == bytes(fx[f"{i}.gen_sha"]), i
+        s, t = O.dedup_sorted(src, dst)
+        ded = np.stack([s, t], axis=1)
+        assert len(ded) == counts[2], i
+        assert hashlib.sha256(ded.tobytes()).digest() == bytes(fx[f"{i}.ded_sha"]), i
+        if i == 0:
+            assert np.array_equal(gen, fx["0.gen"]) and np.array_equal(ded, fx["0.ded"])
+
+
+def test_reference_stream_and_the_reference_el64_file(golden_dir):
+    """graph500-scale10.el64, written by the reference's rmat_dataset_dump,
+    is the oracle's deduplicated scale-10 list after a vertex relabel and an
+    edge shuffle: same edge count, same multiset of degrees, same multiset
+    of per-edge degree pairs."""
+    n, src, dst = O.rmat_stream_graph(10, 16, seed=0)
+    n2, s2, d2 = O.el64_load(os.path.join(golden_dir, "graph500-scale10.el64"))
+    assert n == n2 and len(src) == len(s2)
+    deg = np.bincount(np.concatenate([src, dst]), minlength=n)
+    deg2 = np.bincount(np.concatenate([s2, d2]), minlength=n)
+    assert np.array_equal(np.sort(deg), np.sort(deg2))
+    pairs = np.sort(np.sort(np.stack([deg[src], deg[dst]], 1), axis=1), axis=0)
+    pairs2 = np.sort(np.sort(np.stack([deg2[s2], deg2[d2]], 1), axis=1), axis=0)
+    assert np.array_equal(np.sort(pairs.view([("a", np.int64), ("b", np.int64)]), axis=0),
+                          np.sort(pairs2.view([("a", np.int64), ("b", np.int64)]), axis=0))
+
+
+def test_threefish20_stream_positions():
+    """Output t of the engine is half of block t / 8: the sequential reader
+    and direct access by position agree, across block boundaries."""
+    ts = [0, 1, 2, 7, 8, 9, 15, 16, 1 << 20, (1 << 33) + 5]
+    for seed in (0, 1, 0xFFFFFFFF):
+        for t in ts:
+            out = (ctypes.c_uint64 * 4)()
+            O.lib().or_threefish20(seed, t >> 3, out)
+            w = out[(t & 7) >> 1]
+            want = (w >> 32) if t & 1 else (w & 0xFFFFFFFF)
+            assert O.lib().or_sitmo_output(seed, t) == want
