@@ -640,10 +640,14 @@ __device__ void beamer_after_step(LevelState &c, const BfsParams &p, int dir, lo
     }
 }
 
-// Whether the learned policy is consulted for the step after state c.
+// Whether the learned policy is consulted for the step after state c: it is
+// installed, the BFS goes on, and the frontier's degree sum over the
+// unexplored one lies in the band the policy was trained to decide in
+// (outside it the rule decides and the network is not run).
 __device__ __forceinline__ bool policy_applies(const LevelState &c, const BfsParams &p)
 {
-    return p.alg == BD_ALG_LEARNED && p.policy != nullptr && c.f_count != 0;
+    return p.alg == BD_ALG_LEARNED && p.policy != nullptr && c.f_count != 0 &&
+           policy_in_band(p.policy, c.f_degsum, 2 * p.m - c.visited_degsum);
 }
 
 // The rule's direction for the next step (committed into the Beamer state

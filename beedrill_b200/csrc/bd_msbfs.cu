@@ -3,28 +3,31 @@
 //
 // The reference runs its trials one root at a time (hybrid_bfs_main.cc:252-302);
 // every root re-reads the whole graph.  Here R <= 64 roots share each pass
-// over the adjacency: vertex v carries seen[v] (lanes that reached it
-// before the current level) and F[v] (lanes whose frontier holds it), and a
-// level updates all lanes with 64-bit ORs.  Results per lane are exactly
+// over the adjacency: vertex v carries reach[v] (lanes delivered to it so
+// far, this step's deliveries included) and F[v] (lanes whose frontier holds
+// it), and a level updates all lanes with 64-bit ORs.  Results per lane are exactly
 // those of a single-source BFS from that lane's root: depths equal, parents
 // one level up (each (vertex, lane) gets the first neighbour that delivered
 // the lane's bit).
 //
 // Steps, chosen per level on the device (Beamer-style rule over the batch):
-//   push  frontier vertices OR their lanes into their neighbours' next
+//   push  frontier vertices OR their lanes into their neighbours' reach
 //         word (atomicOr; the returned old word identifies the one writer
-//         that delivered each new lane, which becomes that lane's parent);
+//         that delivered each new lane, which becomes that lane's parent),
+//         then into the next frontier word;
 //   pull  each vertex not yet reached by every lane ORs its neighbours'
-//         frontier words until it has all the lanes it still needs.
+//         frontier words until it has all the lanes it still needs that
+//         some frontier holds (the lanes delivered by the step before).
 //
 // Layout in HBM (n vertices, R lanes):
-//   seen    uint64[n]      lanes that reached v at an earlier level
+//   reach   uint64[n]      lanes delivered to v so far: one load tells a
+//                          push which lanes v still lacks; after the run,
+//                          the lanes that reached v
 //   F[3]    uint64[n]      frontier words, three buffers: step s reads
 //                          F[s%3], writes F[(s+1)%3], clears F[(s+2)%3]
 //   Q[3]                   the vertex lists of those frontiers (degree bins)
 //   done    uint32[n/32]   vertices every lane has reached, and isolated ones:
-//                          pull steps skip them by the word, push steps
-//                          drop arcs into them before touching seen
+//                          pull steps skip them by the word
 //   drec    16 B [n][16]   delivery records of pull steps: {lane mask lo,
 //                          hi, provider, level}, one store for all the
 //                          lanes one neighbour delivered (drec_cnt[n] counts
@@ -33,8 +36,7 @@
 //   parent  uint32[n][R]   sectors): push deliveries, and pull deliveries
 //                          past a vertex's 16 records; widened to the
 //                          reference's int64 encoding when copied out
-//   fb[3]   uint32[n/32]   bit v set iff F[.][v] != 0
-// The kernel leaves F and fb zero when it ends (it clears the last
+// The kernel leaves F zero when it ends (it clears the last
 // frontier's words), so a call needs no memsets of them.
 #include <algorithm>
 #include <cstring>
@@ -68,6 +70,7 @@ struct MsAcc {
     ull done_degsum; // degree sum of vertices that just got every lane
     ull t_end;       // max over CTAs of their arrival time
     ull work;        // pull steps: next bitmap word to hand out
+    ull lanes_or;    // lanes delivered in the step (the next frontier's lanes)
 };
 
 // State between steps: written first by the init kernel, then kept by every
@@ -81,6 +84,7 @@ struct MsState {
     long long lanes_total;
     long long t_last, push_steps, pull_steps;
     long long prev_ns, policy_overrides;
+    ull active;                  // lanes the frontier about to be expanded holds
 };
 
 struct MsCtrl {
@@ -96,9 +100,8 @@ struct MsParams {
     const uint32_t *adj;
     uint32_t *done;   // bit v: every lane reached v, or v is isolated (no lane can)
     int64_t n, m;
-    ull *seen;
+    ull *reach;       // lanes delivered to v so far (the handle's seen array)
     ull *F[3];
-    uint32_t *fb[3];  // bit v set iff F[.][v] != 0 (pull steps skip done words by it)
     uint32_t *qs[3];
     uint32_t *ql[3];
     ull *qlb[3];
@@ -128,7 +131,7 @@ struct MsParams {
 };
 
 struct MsLocal {
-    ull vertices, degsum, lanes, done_degsum;
+    ull vertices, degsum, lanes, done_degsum, lanes_or;
 };
 
 // Frontier word of v (zero outside the frontier).  Read directly: most arcs
@@ -222,6 +225,7 @@ __device__ __forceinline__ void record_shared(const MsParams &p, uint32_t v, ull
 struct MsView {
     int dir, level, step;
     long long f_small, f_large, f_chunks, p_small, p_large;
+    ull active;
 };
 
 __device__ __forceinline__ MsView ms_view(const MsState &c)
@@ -235,6 +239,7 @@ __device__ __forceinline__ MsView ms_view(const MsState &c)
     v.f_chunks = c.f_chunks;
     v.p_small = c.p_small;
     v.p_large = c.p_large;
+    v.active = c.active;
     return v;
 }
 
@@ -244,16 +249,8 @@ __device__ void ms_clear_old(const MsParams &p, const MsView &sv)
     const int old = (sv.step + 2) % 3;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long nt = (long long)gridDim.x * blockDim.x;
-    for (long long i = t; i < sv.p_small; i += nt) {
-        const uint32_t v = p.qs[old][i];
-        p.F[old][v] = 0ull;
-        p.fb[old][v >> 5] = 0u;
-    }
-    for (long long i = t; i < sv.p_large; i += nt) {
-        const uint32_t v = p.ql[old][i];
-        p.F[old][v] = 0ull;
-        p.fb[old][v >> 5] = 0u;
-    }
+    for (long long i = t; i < sv.p_small; i += nt) { p.F[old][p.qs[old][i]] = 0ull; }
+    for (long long i = t; i < sv.p_large; i += nt) { p.F[old][p.ql[old][i]] = 0ull; }
 }
 
 // Warp-collective append of up to K new frontier vertices per lane: one
@@ -321,10 +318,13 @@ __device__ __forceinline__ void ms_append_k(const MsParams &p, MsAcc *acc, int q
 
 // push: lanes of frontier vertex u flow into neighbours [b, e), four arcs
 // per lane per round with each stage's loads and atomics issued back to
-// back.  The atomicOr on the neighbour's next word tells each deliverer
-// which lanes it delivered first; those lanes' depth and parent go to the
-// per-lane rows (every (vertex, lane) pair is delivered exactly once, so the
-// rows and the pull steps' records never hold the same pair).
+// back.  One plain read of the neighbour's reach word (and of its done bit,
+// in parallel) filters the arcs that deliver nothing; the atomicOr on the
+// reach word tells each deliverer which lanes it delivered first -- those
+// lanes' depth and parent go to the per-lane rows (every (vertex, lane) pair
+// is delivered exactly once, so the rows and the pull steps' records never
+// hold the same pair) -- and an atomicOr on the next frontier word tells
+// which deliverer puts the neighbour on the next frontier's list.
 constexpr int kPushU = 4;
 
 // One round of up to kPushU arcs per lane: arc i of this lane goes from
@@ -335,45 +335,40 @@ __device__ __forceinline__ void push_arcs(const MsParams &p, MsAcc *acc, int cur
                                           const uint32_t (&src)[kPushU],
                                           const ull (&bits)[kPushU], MsLocal &loc)
 {
-    uint32_t dn[kPushU];
-#pragma unroll
-    for (int i = 0; i < kPushU; ++i) { dn[i] = in[i] ? __ldcg(&p.done[v[i] >> 5]) : ~0u; }
-    // lanes v already has (seen, current frontier) or was already given in
-    // this step (a plain read of its next word: hot targets of many pushers
-    // then skip the atomic; a stale read only costs an atomic that changes
-    // nothing)
-    ull vis[kPushU], nxt_seen[kPushU];
+    ull g[kPushU];  // lanes to give, then the lanes this writer delivered first
 #pragma unroll
     for (int i = 0; i < kPushU; ++i) {
-        const bool open = in[i] && !((dn[i] >> (v[i] & 31)) & 1u);
-        vis[i] = open ? (__ldcg(&p.seen[v[i]]) | frontier_word(p, cur, v[i])) : ~0ull;
-        nxt_seen[i] = open ? __ldcg(&p.F[nxt][v[i]]) : ~0ull;
+        const uint32_t dn = in[i] ? __ldcg(&p.done[v[i] >> 5]) : ~0u;
+        // a stale read only costs an atomic that changes nothing
+        const ull have = in[i] ? __ldcg(&p.reach[v[i]]) : ~0ull;
+        g[i] = ((dn >> (v[i] & 31)) & 1u) ? 0ull : bits[i] & ~have;
     }
-    ull old[kPushU], give[kPushU];
+    bool completed[kPushU];
 #pragma unroll
     for (int i = 0; i < kPushU; ++i) {
-        give[i] = bits[i] & ~vis[i];
-        old[i] = (give[i] & ~nxt_seen[i]) ? atomicOr(&p.F[nxt][v[i]], give[i]) : ~0ull;
+        const ull old = g[i] ? atomicOr(&p.reach[v[i]], g[i]) : ~0ull;
+        g[i] &= ~old;
+        completed[i] = g[i] && ((old | g[i]) & p.all) == p.all;
     }
     bool first[kPushU];
+#pragma unroll
+    for (int i = 0; i < kPushU; ++i) {
+        first[i] = g[i] && atomicOr(&p.F[nxt][v[i]], g[i]) == 0ull;
+    }
     int64_t deg[kPushU];
 #pragma unroll
     for (int i = 0; i < kPushU; ++i) {
-        const ull fresh = give[i] & ~old[i];
-        first[i] = give[i] != 0 && old[i] == 0ull;
         deg[i] = 0;
-        if (fresh) {
-            write_rows(p, v[i], fresh, new_level, src[i]);
-            loc.lanes += __popcll(fresh);
+        if (g[i]) {
+            write_rows(p, v[i], g[i], new_level, src[i]);
+            loc.lanes += __popcll(g[i]);
+            loc.lanes_or |= g[i];
         }
-        if (first[i] || (fresh && ((vis[i] | old[i] | fresh) & p.all) == p.all)) {
-            deg[i] = ms_degree(p, v[i]);
-        }
-        if (fresh && ((vis[i] | old[i] | fresh) & p.all) == p.all) {
+        if (first[i] || completed[i]) { deg[i] = ms_degree(p, v[i]); }
+        if (completed[i]) {
             loc.done_degsum += (ull)deg[i];
             atomicOr(&p.done[v[i] >> 5], 1u << (v[i] & 31));
         }
-        if (first[i]) { atomicOr(&p.fb[nxt][v[i] >> 5], 1u << (v[i] & 31)); }
         if (!first[i]) { deg[i] = 0; }
     }
     ms_append_k<kPushU>(p, acc, nxt, first, v, deg, loc);
@@ -430,7 +425,6 @@ __device__ void ms_push_step(const MsParams &p, const MsView &sv, MsWarpScratch 
         const uint32_t u = __ldcg(&p.ql[cur][lo]);
         const long long j = c - (long long)__ldcg(&p.qlb[cur][lo]);
         const ull bits = __ldcg(&p.F[cur][u]);
-        if (j == 0 && lane == 0) { p.seen[u] |= bits; }
         const int64_t ub = __ldg(&p.off[u]), ue = __ldg(&p.off[u + 1]);
         const int64_t b = ub + j * (int64_t)p.chunk;
         push_edges(p, acc, cur, nxt, new_level, u, bits, b, min(ue, b + (int64_t)p.chunk), loc);
@@ -448,7 +442,6 @@ __device__ void ms_push_step(const MsParams &p, const MsView &sv, MsWarpScratch 
             bits = __ldcg(&p.F[cur][u]);
             beg = __ldg(&p.off[u]);
             deg = (int32_t)(__ldg(&p.off[u + 1]) - beg);
-            p.seen[u] |= bits;
         }
         const int32_t incl = warp_incl_scan(deg);
         const int32_t total = __shfl_sync(kFullMask, incl, 31);
@@ -509,8 +502,9 @@ __device__ void ms_pull_heavy(const MsParams &p, const MsView &sv, MsLocal &loc)
             if ((long long)__ldg(&p.heavy_cbase[mid]) <= c) { lo = mid; } else { hi = mid - 1; }
         }
         const uint32_t v = __ldg(&p.heavy[lo]);
-        const ull vis = __ldcg(&p.seen[v]) | __ldcg(&p.F[cur][v]);
-        const ull need = p.all & ~vis;
+        // lanes v lacks that the frontier holds (other chunks of v may have
+        // delivered some already this step)
+        const ull need = p.all & ~__ldcg(&p.reach[v]) & sv.active;
         if (!need) { continue; }
         const int64_t vb = __ldg(&p.off[v]), ve = __ldg(&p.off[v + 1]);
         const int64_t b = vb + (c - (long long)__ldg(&p.heavy_cbase[lo])) * (int64_t)p.heavy_chunk;
@@ -543,12 +537,14 @@ __device__ void ms_pull_heavy(const MsParams &p, const MsView &sv, MsLocal &loc)
                 const bool first = lane == 0 && old == 0ull;
                 if (lane == 0 && fresh) {
                     loc.lanes += __popcll(fresh);
-                    if (((vis | old | fresh) & p.all) == p.all) {
+                    loc.lanes_or |= fresh;
+                    // the chunk whose update completes v's lanes marks it done
+                    const ull before = atomicOr(&p.reach[v], fresh) & p.all;
+                    if (before != p.all && ((before | fresh) & p.all) == p.all) {
                         loc.done_degsum += (ull)(ve - vb);
                         atomicOr(&p.done[v >> 5], 1u << (v & 31));
                     }
                 }
-                if (first) { atomicOr(&p.fb[nxt][v >> 5], 1u << (v & 31)); }
                 ms_append(p, acc, nxt, first, v, ve - vb, loc);
                 have |= round | old;
             }
@@ -584,8 +580,7 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
     // Smaller graphs: warp gw owns words gw, gw + nw, gw + 2 nw, ... (a
     // chunk per warp would leave most warps idle).  Either way a warp loads
     // 32 skip masks at once (one per lane) and walks only the words with
-    // work.  Done vertices outside the frontier have nothing to do (frontier
-    // ones still fold their frontier lanes into seen below).
+    // work: done vertices have nothing to do.
     const long long gw = (long long)blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5);
     const long long nw = (long long)gridDim.x * (BLOCK / 32);
     const long long chunks = (words + 31) / 32;
@@ -595,8 +590,7 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
     for (long long base = gw; base < limit;
          base = dynamic ? (long long)ms_next_chunk(&acc->work, nw, chunks) : base + 32 * nw) {
         const long long wl = base + lane * stride;
-        const uint32_t sk =
-            wl < words ? (__ldcg(&p.done[wl]) & ~__ldcg(&p.fb[cur][wl])) : kFullMask;
+        const uint32_t sk = wl < words ? __ldcg(&p.done[wl]) : kFullMask;
         unsigned todo = __ballot_sync(kFullMask, sk != kFullMask);
         while (todo) {
             const int src = __ffs(todo) - 1;
@@ -605,17 +599,14 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
             const uint32_t skip = __shfl_sync(kFullMask, sk, src);
             const uint32_t v = (uint32_t)(w * 32 + lane);
             const bool live = !((skip >> lane) & 1u);
-            ull need = 0, got = 0;
+            ull need = 0, got = 0, s = 0;
             int64_t beg = 0, end = 0, next = 0;
             unsigned cnt = 0, cnt0 = 0;  // this vertex's delivery records
             if (live) {
-                const ull f = __ldcg(&p.F[cur][v]);
-                ull s = __ldcg(&p.seen[v]);
-                if (f) {
-                    s |= f;
-                    p.seen[v] = s;
-                }
-                need = p.all & ~s;
+                // lanes v lacks that some frontier vertex holds: only lanes
+                // delivered by the previous step can arrive in this one
+                s = __ldcg(&p.reach[v]);
+                need = p.all & ~s & sv.active;
                 if (need) {
                     beg = __ldg(&p.off[v]);
                     end = __ldg(&p.off[v + 1]);
@@ -697,14 +688,16 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
             }
             if (cnt != cnt0) { p.drec_cnt[v] = cnt; }
             const bool gained = got != 0;
-            const unsigned gm = __ballot_sync(kFullMask, gained);
-            if (lane == 0 && gm) { atomicOr(&p.fb[nxt][w], gm); }
-            const bool completed = gained && ((p.all & ~need) | got) == p.all;
+            const bool completed = gained && ((s | got) & p.all) == p.all;
             const unsigned cm = __ballot_sync(kFullMask, completed);
             if (lane == 0 && cm) { atomicOr(&p.done[w], cm); }
             if (gained) {
+                // v is this lane's alone in a pull step (heavy vertices are
+                // left to ms_pull_heavy), so plain stores
                 p.F[nxt][v] = got;
+                p.reach[v] = s | got;
                 loc.lanes += __popcll(got);
+                loc.lanes_or |= got;
                 if (completed) { loc.done_degsum += (ull)(end - beg); }
             }
             ms_append(p, acc, nxt, gained, v, end - beg, loc);
@@ -715,7 +708,7 @@ __device__ void ms_pull_step(const MsParams &p, const MsView &sv, MsLocal &loc)
 template <int BLOCK>
 struct MsShared {
     MsWarpScratch warp[BLOCK / 32];
-    ull red[4][BLOCK / 32];
+    ull red[5][BLOCK / 32];
     MsState st;     // this CTA's copy of the state
     PolicyBlob pol; // the learned policy's weights, staged once
     int rule_dir;
@@ -741,6 +734,7 @@ __device__ void ms_advance(MsState &c, const MsAcc &a, long long t_end)
     c.prev_ns = t_end - c.t_last;
     c.t_last = t_end;
     c.lanes_total += (long long)a.lanes;
+    c.active = a.lanes_or;
     c.arcs_left -= (long long)a.done_degsum;
     c.p_small = c.f_small;
     c.p_large = c.f_large;
@@ -762,7 +756,10 @@ __device__ void ms_decide(MsState &c, const MsParams &p, const PolicyBlob *w, Sh
     const int tid = threadIdx.x;
     if (tid == 0) { sh.rule_dir = ms_rule(c, p); }
     __syncthreads();
-    const bool learned = p.policy && p.force_dir < 0 && sh.rule_dir != kMsDone;
+    // the network runs only where the frontier's degree sum over the
+    // unexplored one lies in the band the policy was trained to decide in
+    const bool learned = p.policy && p.force_dir < 0 && sh.rule_dir != kMsDone &&
+                         policy_in_band(w, c.f_degsum, c.arcs_left);
     if (!learned) {
         if (tid == 0) { c.dir = sh.rule_dir; }
         return;
@@ -792,19 +789,21 @@ __device__ void ms_end_step(const MsParams &p, const MsView &sv, MsShared<BLOCK>
     MsCtrl *c = p.ctrl;
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     const ull a0 = warp_sum(loc.vertices), a1 = warp_sum(loc.degsum), a2 = warp_sum(loc.lanes),
-              a3 = warp_sum(loc.done_degsum);
+              a3 = warp_sum(loc.done_degsum), a4 = warp_or(loc.lanes_or);
     if (lane == 0) {
         sh.red[0][warp] = a0;
         sh.red[1][warp] = a1;
         sh.red[2][warp] = a2;
         sh.red[3][warp] = a3;
+        sh.red[4][warp] = a4;
     }
-    loc = MsLocal{0, 0, 0, 0};
+    loc = MsLocal{0, 0, 0, 0, 0};
     __syncthreads();
     if (threadIdx.x == 0) {
-        ull t[4] = {0, 0, 0, 0};
+        ull t[4] = {0, 0, 0, 0}, lanes_or = 0;
         for (int i = 0; i < BLOCK / 32; ++i) {
             for (int j = 0; j < 4; ++j) { t[j] += sh.red[j][i]; }
+            lanes_or |= sh.red[4][i];
         }
         const int s = sv.step;
         MsAcc *acc = &c->acc[s % 3];
@@ -812,10 +811,11 @@ __device__ void ms_end_step(const MsParams &p, const MsView &sv, MsShared<BLOCK>
         if (t[1]) { atomicAdd(&acc->degsum, t[1]); }
         if (t[2]) { atomicAdd(&acc->lanes, t[2]); }
         if (t[3]) { atomicAdd(&acc->done_degsum, t[3]); }
+        if (lanes_or) { atomicOr(&acc->lanes_or, lanes_or); }
         if (blockIdx.x == 0) {
             MsAcc *z = &c->acc[(s + 1) % 3];
             z->vertices = z->degsum = z->lanes = z->small_cnt = z->large_packed = 0;
-            z->done_degsum = z->t_end = z->work = 0;
+            z->done_degsum = z->t_end = z->work = z->lanes_or = 0;
         }
         atomicMax(&acc->t_end, (ull)globaltimer());
         red_release_add64(&c->bar, 1ull);
@@ -839,6 +839,7 @@ __device__ void ms_end_step(const MsParams &p, const MsView &sv, MsShared<BLOCK>
             a.small_cnt = __ldcg(&acc->small_cnt);
             a.large_packed = __ldcg(&acc->large_packed);
             a.done_degsum = __ldcg(&acc->done_degsum);
+            a.lanes_or = __ldcg(&acc->lanes_or);
             const long long t_end = (long long)__ldcg(&acc->t_end);
             if (s == 0) { st.t_last = (long long)__ldcg(&c->t_start); }
             if (blockIdx.x == 0 && s < p.rec_cap) {
@@ -879,7 +880,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) msbfs_kernel(MsParams p)
         }
     }
     __syncthreads();
-    MsLocal loc{0, 0, 0, 0};
+    MsLocal loc{0, 0, 0, 0, 0};
     while (sh.st.dir != kMsDone) {
         const MsView sv = ms_view(sh.st);
         ms_clear_old(p, sv);
@@ -912,11 +913,10 @@ __global__ void ms_init_kernel(MsParams p, const int64_t *sources, int count)
         const ull bit = 1ull << r;
         const ull before = p.F[0][s];
         p.F[0][s] = before | bit;
-        p.fb[0][s >> 5] |= 1u << (s & 31);
-        p.seen[s] |= bit;
+        p.reach[s] |= bit;
         put_record(p, s, p.drec_cnt[s]++, bit, 0, s);
         const int64_t deg = p.off[s + 1] - p.off[s];
-        if (p.seen[s] == p.all) {
+        if (p.reach[s] == p.all) {
             done += deg;
             p.done[s >> 5] |= 1u << (s & 31);
         }
@@ -940,6 +940,7 @@ __global__ void ms_init_kernel(MsParams p, const int64_t *sources, int count)
     st.f_large = (long long)(lp >> kLargeShift);
     st.f_chunks = (long long)(lp & kChunkMask);
     st.arcs_left = 2 * p.m - done;
+    st.active = p.all;
     st.lanes_total = count;
     st.dir = ms_rule(st, p);
 }
@@ -1036,17 +1037,24 @@ __global__ void ms_extract_kernel(const int32_t *depth, const uint32_t *parent, 
 // (root0 + r) gets depth_out[(root0 + r) * n + v] and parent_out[...] for
 // every caller vertex v (caller ids, the reference's encoding: the source is
 // its own parent, unreached vertices -deg or -1).  One pass over the group's
-// state instead of one per lane: thread i of a CTA takes caller vertex
-// v0 + i of a tile of kMatThreads consecutive vertices, reads the vertex's
-// seen word, record count and records once (a record covers every lane one
-// provider delivered at one level, so the provider is renamed once per
-// record), notes for each reached lane which record holds it, and then
-// writes each root's row entry for its vertex: a CTA writes runs of
-// kMatThreads consecutive entries per row (2 KB of depths, 4 KB of
-// parents), streaming past L2.  Lanes whose vertex ran out of records are
-// read from the per-lane rows.  The per-thread tables live in shared
-// memory, column i for thread i (slot-major, so a warp's accesses fall in
-// 32 different banks); no thread reads another's column, so no barrier.
+// state instead of one per lane.  A CTA takes a tile of kMatV consecutive
+// caller vertices in two phases:
+//   fill   two threads per vertex (lanes 0-31 and 32-63) read the vertex's
+//          seen word, record count and records once (a record covers every
+//          lane one provider delivered at one level, so the provider is
+//          renamed once per record) and put each reached lane's depth and
+//          parent into a [64][kMatV] shared tile (lanes past the vertex's
+//          records come from the per-lane rows);
+//   write  each half-warp writes one row at a time (rows 2w and 2w + 1 of
+//          warp w, then 8 further): lane l takes vertices 4(l%16)..+3, so a
+//          half-warp stores a row's 64 vertices as 256 B of depths and 512 B
+//          of parents in 16-byte stores, streaming past L2 (4-byte and 8-byte
+//          stores when n is not a multiple of 4).
+// The tile is small (33 KB of shared memory) so that six CTAs share an SM
+// and one's fill phase overlaps another's writes.
+// Each (vertex, lane) costs a few shared-memory operations and 3/4 of a
+// global store instruction; the write traffic (12 bytes per pair) is the
+// bound.
 struct MsOutParams {
     const int32_t *depth;     // per-lane rows [n][R]
     const uint32_t *parent;
@@ -1063,80 +1071,137 @@ struct MsOutParams {
     int64_t *parent_out;
 };
 
-constexpr int kMatThreads = 512;
-constexpr uint8_t kMatRows = 0xFE;  // the lane's result is in the per-lane rows
-// per thread: a record slot per lane (64 B), a depth and a provider per
-// record (16 x 8 B)
-constexpr size_t kMatSmem = (size_t)kMatThreads * (64 + kRecSlots * 8);
+constexpr int kMatV = 64;                  // vertices per tile
+constexpr int kMatThreads = 2 * kMatV;     // two threads per vertex in the fill phase
+struct MatShared {
+    int32_t depth[64][kMatV];
+    uint32_t parent[64][kMatV];
+    ull seen[kMatV];
+    int64_t unreached[kMatV];
+};
+constexpr size_t kMatSmem = sizeof(MatShared);
 
 __global__ void __launch_bounds__(kMatThreads) ms_materialize_kernel(MsOutParams o)
 {
-    extern __shared__ uint32_t mat_smem[];
+    extern __shared__ __align__(16) unsigned char mat_raw[];
+    MatShared &sh = *reinterpret_cast<MatShared *>(mat_raw);
     const int tid = threadIdx.x;
-    int32_t *rec_depth = reinterpret_cast<int32_t *>(mat_smem);   // [kRecSlots][threads]
-    uint32_t *rec_prov = mat_smem + kRecSlots * kMatThreads;      // [kRecSlots][threads]
-    uint8_t *slot = reinterpret_cast<uint8_t *>(mat_smem + 2 * kRecSlots * kMatThreads);
-    // slot: [64][threads]
+    const int lane = lane_id(), warp = tid >> 5;
     const ull all = o.lanes >= 64 ? ~0ull : ((1ull << o.lanes) - 1);
-    const long long tiles = (o.n + kMatThreads - 1) / kMatThreads;
+    const bool vec = (o.n & 3) == 0;
+    const long long tiles = (o.n + kMatV - 1) / kMatV;
     for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const int64_t v = tile * kMatThreads + tid;
-        if (v >= o.n) { continue; }
-        const int64_t t = o.perm ? (int64_t)__ldg(&o.perm[v]) : v;
-        const int64_t deg = __ldg(&o.off[v + 1]) - __ldg(&o.off[v]);
-        const ull s = __ldcs(&o.seen[t]) & all;
-        if (s) {
-            const unsigned cnt = min(__ldcs(&o.rec_cnt[t]), kRecSlots);
-            const uint4 *rv = o.rec + t * kRecSlots;
-            ull left = s;
-            for (unsigned k0 = 0; k0 < cnt && left; k0 += 4) {
-                uint4 x[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    x[j] = k0 + j < cnt ? __ldcs(&rv[k0 + j]) : make_uint4(0, 0, 0, 0);
+        const int64_t v0 = tile * kMatV;
+        // ---- fill: thread tid handles vertex v0 + (tid % kMatV), lanes of
+        // half tid / kMatV
+        {
+            const int i = tid % kMatV;
+            const ull half = tid < kMatV ? 0x00000000FFFFFFFFull : 0xFFFFFFFF00000000ull;
+            const int64_t v = v0 + i;
+            ull s = 0;
+            int64_t t = 0;
+            if (v < o.n) {
+                t = o.perm ? (int64_t)__ldg(&o.perm[v]) : v;
+                s = __ldcs(&o.seen[t]) & all;
+                if (tid < kMatV) {
+                    const int64_t deg = __ldg(&o.off[v + 1]) - __ldg(&o.off[v]);
+                    sh.seen[i] = s;
+                    sh.unreached[i] = deg != 0 ? -deg : -1;
                 }
+            } else if (tid < kMatV) {
+                sh.seen[i] = 0;
+                sh.unreached[i] = -1;
+            }
+            ull left = s & half;
+            if (left) {
+                const uint4 *rv = o.rec + t * kRecSlots;
+                // the first two slots are read together with the count (they
+                // lie in the vertex's record block whatever the count says)
+                const uint4 x0 = __ldg(&rv[0]), x1 = __ldg(&rv[1]);
+                const unsigned cnt = min(__ldg(&o.rec_cnt[t]), kRecSlots);
+                for (unsigned k0 = 0; k0 < cnt && left; k0 += 4) {
+                    uint4 x[4];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    ull mask = (((ull)x[j].y << 32) | x[j].x) & left;
-                    if (!mask) { continue; }
-                    left &= ~mask;
-                    const unsigned k = k0 + j;
-                    // (a provider id out of range would only come from a
-                    // broken record; it is passed through, not followed)
-                    rec_depth[k * kMatThreads + tid] = (int32_t)x[j].w;
-                    rec_prov[k * kMatThreads + tid] =
-                        o.iperm && x[j].z < o.n ? __ldg(&o.iperm[x[j].z]) : x[j].z;
-                    do {
-                        const int r = __ffsll((long long)mask) - 1;
-                        mask &= mask - 1;
-                        slot[r * kMatThreads + tid] = (uint8_t)k;
-                    } while (mask);
+                    for (int j = 0; j < 4; ++j) {
+                        x[j] = (k0 == 0 && j < 2) ? (j ? x1 : x0)
+                                                  : (k0 + j < cnt ? __ldg(&rv[k0 + j])
+                                                                  : make_uint4(0, 0, 0, 0));
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        ull mask = k0 + j < cnt ? (((ull)x[j].y << 32) | x[j].x) & left : 0ull;
+                        if (!mask) { continue; }
+                        left &= ~mask;
+                        // (a provider id out of range would only come from a
+                        // broken record; it is passed through, not followed)
+                        const uint32_t prov =
+                            o.iperm && x[j].z < o.n ? __ldg(&o.iperm[x[j].z]) : x[j].z;
+                        const int32_t d = (int32_t)x[j].w;
+                        do {
+                            const int r = __ffsll((long long)mask) - 1;
+                            mask &= mask - 1;
+                            sh.depth[r][i] = d;
+                            sh.parent[r][i] = prov;
+                        } while (mask);
+                    }
                 }
-            }
-            while (left) {  // lanes past the vertex's records: the per-lane rows
-                const int r = __ffsll((long long)left) - 1;
-                left &= left - 1;
-                slot[r * kMatThreads + tid] = kMatRows;
-            }
-        }
-        const int64_t unreached = deg != 0 ? -deg : -1;
-        for (int r = 0; r < o.lanes; ++r) {
-            int32_t d = -1;
-            int64_t par = unreached;
-            if ((s >> r) & 1ull) {
-                const unsigned k = slot[r * kMatThreads + tid];
-                if (k < kRecSlots) {
-                    d = rec_depth[k * kMatThreads + tid];
-                    par = rec_prov[k * kMatThreads + tid];
-                } else {
+                while (left) {  // lanes past the vertex's records: the per-lane rows
+                    const int r = __ffsll((long long)left) - 1;
+                    left &= left - 1;
                     const uint32_t p = __ldcs(&o.parent[t * o.R + r]);
-                    d = __ldcs(&o.depth[t * o.R + r]);
-                    par = o.iperm && p < o.n ? __ldg(&o.iperm[p]) : p;
+                    sh.depth[r][i] = __ldcs(&o.depth[t * o.R + r]);
+                    sh.parent[r][i] = o.iperm && p < o.n ? __ldg(&o.iperm[p]) : p;
                 }
             }
-            __stcs(&o.depth_out[(int64_t)r * o.n + v], d);
-            __stcs(&o.parent_out[(int64_t)r * o.n + v], par);
         }
+        __syncthreads();
+        // ---- write: half-warp h of warp w, rows 2w + h, 2w + h + 8, ...;
+        // lane l, vertices 4(l % 16)..4(l % 16) + 3
+        {
+            const int i0 = 4 * (lane & 15);
+            ull sv[4];
+            int64_t un[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                sv[j] = sh.seen[i0 + j];
+                un[j] = sh.unreached[i0 + j];
+            }
+            const int64_t v = v0 + i0;
+            for (int r = 2 * warp + (lane >> 4); r < o.lanes; r += 2 * (kMatThreads / 32)) {
+                const int4 dq = *reinterpret_cast<const int4 *>(&sh.depth[r][i0]);
+                const uint4 pq = *reinterpret_cast<const uint4 *>(&sh.parent[r][i0]);
+                const int32_t dd[4] = {dq.x, dq.y, dq.z, dq.w};
+                const uint32_t pp[4] = {pq.x, pq.y, pq.z, pq.w};
+                int32_t d[4];
+                int64_t par[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const bool got = (sv[j] >> r) & 1ull;
+                    d[j] = got ? dd[j] : -1;
+                    par[j] = got ? (int64_t)pp[j] : un[j];
+                }
+                const int64_t at = (int64_t)r * o.n + v;
+                if (vec) {
+                    if (v < o.n) {
+                        __stcs(reinterpret_cast<int4 *>(o.depth_out + at),
+                               make_int4(d[0], d[1], d[2], d[3]));
+                        __stcs(reinterpret_cast<longlong2 *>(o.parent_out + at),
+                               make_longlong2(par[0], par[1]));
+                        __stcs(reinterpret_cast<longlong2 *>(o.parent_out + at + 2),
+                               make_longlong2(par[2], par[3]));
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        if (v + j < o.n) {
+                            __stcs(o.depth_out + at + j, d[j]);
+                            __stcs(o.parent_out + at + j, par[j]);
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -1164,7 +1229,6 @@ struct bd_msbfs {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ull *seen = nullptr;         // [groups][n]: a group's final words mark its valid lanes
     ull *F[3] = {nullptr, nullptr, nullptr};
-    uint32_t *fb[3] = {nullptr, nullptr, nullptr};
     uint32_t *qs[3] = {nullptr, nullptr, nullptr};
     uint32_t *ql[3] = {nullptr, nullptr, nullptr};
     ull *qlb[3] = {nullptr, nullptr, nullptr};
@@ -1190,7 +1254,7 @@ struct bd_msbfs {
     cudaGraphExec_t graph = nullptr;
     int graph_count = -1;
     bool graph_ok = true;
-    bool frontier_clean = false;  // F and fb are all zero (kernels leave them so)
+    bool frontier_clean = false;  // F is all zero (kernels leave it so)
     MsCtrl last{};
     std::vector<unsigned long long> counts;
     // opts.materialize: every root's results, written by each run
@@ -1222,10 +1286,9 @@ MsParams ms_params(bd_msbfs *b, int group, int count)
     p.done = b->done;
     p.n = b->g->n;
     p.m = b->g->m;
-    p.seen = b->seen + group * b->g->n;
+    p.reach = b->seen + group * b->g->n;
     for (int i = 0; i < 3; ++i) {
         p.F[i] = b->F[i];
-        p.fb[i] = b->fb[i];
         p.qs[i] = b->qs[i];
         p.ql[i] = b->ql[i];
         p.qlb[i] = b->qlb[i];
@@ -1306,7 +1369,7 @@ bd_status ms_enqueue_group(bd_msbfs *b, int group, int count)
                                         dim3(b->block), args, 0, b->stream));
     unsigned long long *dst = b->d_counts + 128 * group;
     BD_CUDA(cudaMemsetAsync(dst, 0, sizeof(unsigned long long) * 128, b->stream));
-    ms_count_kernel<<<148 * 8, 256, 0, b->stream>>>(p.seen, p.off, n, p.all, count, dst);
+    ms_count_kernel<<<148 * 8, 256, 0, b->stream>>>(p.reach, p.off, n, p.all, count, dst);
     BD_CUDA(cudaGetLastError());
     if (b->opts.materialize) { BD_TRY(ms_enqueue_materialize(b, group, count)); }
     return BD_OK;
@@ -1325,13 +1388,12 @@ bd_status ms_enqueue_all(bd_msbfs *b, int count)
 // count); falls back to plain stream launches if capture is refused.
 bd_status ms_launch(bd_msbfs *b, int count)
 {
-    // The kernels leave F and fb zero; after a first use or an error, zero
+    // The kernels leave F zero; after a first use or an error, zero
     // them here (outside any captured graph).
     if (!b->frontier_clean) {
         const int64_t n = b->g->n;
         for (int i = 0; i < 3; ++i) {
             BD_CUDA(cudaMemsetAsync(b->F[i], 0, sizeof(ull) * n, b->stream));
-            BD_CUDA(cudaMemsetAsync(b->fb[i], 0, sizeof(uint32_t) * ((n + 31) / 32), b->stream));
         }
     }
     b->frontier_clean = false;  // until this call is known to have finished cleanly
@@ -1376,7 +1438,6 @@ void ms_free(bd_msbfs *b)
     cudaFree(b->done);
     for (int i = 0; i < 3; ++i) {
         cudaFree(b->F[i]);
-        cudaFree(b->fb[i]);
         cudaFree(b->qs[i]);
         cudaFree(b->ql[i]);
         cudaFree(b->qlb[i]);
@@ -1516,7 +1577,6 @@ bd_status bd_msbfs_create(bd_graph *g, int32_t max_roots, const bd_msbfs_opts *o
               cudaMalloc(&b->d_counts, sizeof(unsigned long long) * 128 * b->groups) == cudaSuccess;
     for (int i = 0; i < 3 && ok; ++i) {
         ok = cudaMalloc(&b->F[i], sizeof(ull) * n) == cudaSuccess &&
-             cudaMalloc(&b->fb[i], sizeof(uint32_t) * ((n + 31) / 32)) == cudaSuccess &&
              cudaMalloc(&b->qs[i], sizeof(uint32_t) * n) == cudaSuccess &&
              cudaMalloc(&b->ql[i], sizeof(uint32_t) * b->cap_large) == cudaSuccess &&
              cudaMalloc(&b->qlb[i], sizeof(ull) * b->cap_large) == cudaSuccess;

@@ -31,24 +31,50 @@ struct PolicyBlob {
     float pad[3];
 };
 
-// Raw feature i, in the order the trainer uses: log2(1 + frontier vertices),
-// log2(1 + frontier degree sum), log2(1 + unexplored degree sum), level,
-// log2(1 + n), log2(1 + m), previous direction, log2(1 + previous step us).
-// The lanes of a warp each pick their argument, then take one logarithm
-// together (no divergent branches around the call).
+// Raw feature i, in the order the trainer uses.  Every feature but the
+// previous direction is a difference of two logarithms, so that graphs of
+// any size share one range (a network trained on scales 16-24 is not
+// outside its range at scale 26):
+//   0  log2(1 + m_f) - log2(1 + m_u)     frontier degree sum over unexplored
+//   1  log2(1 + frontier) - log2(1 + n)  frontier share of the vertices
+//   2  log2(1 + m_u) - log2(1 + 2m)      unexplored share of the arcs
+//   3  log2(1 + level)
+//   4  log2(1 + m) - log2(1 + n)         average degree
+//   5  previous direction (0 top-down / push, 1 bottom-up / pull)
+//   6  log2(1 + previous step us) - log2(1 + m / 2^20)   time per M edges
+//   7  log2(1 + m_f) - log2(1 + frontier) frontier average degree
+// The lanes of a warp each pick their two arguments, then take two
+// logarithms together (no divergent branches around the calls).
 __device__ __forceinline__ float policy_feature(int i, long long frontier, long long frontier_edges,
                                                 long long unexplored, int level, long long n,
                                                 long long m, int prev_dir, long long prev_ns)
 {
-    const long long counts[6] = {frontier, frontier_edges, unexplored, n, m, prev_ns};
-    const int which = i < 3 ? i : (i == 4 ? 3 : (i == 5 ? 4 : 5));
-    long long v = 0;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) { v = which == k ? counts[k] : v; }
-    float arg = (float)(v > 0 ? v : 0);
-    if (i == 7) { arg *= 1e-3f; }  // ns -> us
-    const float lg = log2f(1.0f + arg);
-    return i == 3 ? (float)level : (i == 6 ? (float)prev_dir : lg);
+    float a = 0.f, b = 0.f;
+    switch (i) {
+        case 0: a = (float)frontier_edges; b = (float)unexplored; break;
+        case 1: a = (float)frontier; b = (float)n; break;
+        case 2: a = (float)unexplored; b = (float)(2 * m); break;
+        case 3: a = (float)level; break;
+        case 4: a = (float)m; b = (float)n; break;
+        case 6: a = (float)prev_ns * 1e-3f; b = (float)m * (1.0f / 1048576.0f); break;
+        case 7: a = (float)frontier_edges; b = (float)frontier; break;
+        default: break;
+    }
+    a = fmaxf(a, 0.f);
+    b = fmaxf(b, 0.f);
+    const float d = log2f(1.0f + a) - log2f(1.0f + b);
+    return i == 5 ? (float)prev_dir : d;
+}
+
+// Feature 0 alone (thread 0, before the network is woken): the policy is
+// only consulted where feature 0 lies in its trusted range, the band in
+// which the trainer saw the best direction differ from the rule's.
+__device__ __forceinline__ bool policy_in_band(const PolicyBlob *w, long long frontier_edges,
+                                               long long unexplored)
+{
+    const float f0 = log2f(1.0f + (float)(frontier_edges > 0 ? frontier_edges : 0)) -
+                     log2f(1.0f + (float)(unexplored > 0 ? unexplored : 0));
+    return f0 >= w->lo[0] && f0 <= w->hi[0];
 }
 
 // Forward pass by the 32 lanes of one warp (lane j owns hidden unit j;

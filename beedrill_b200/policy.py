@@ -45,24 +45,28 @@ BATCHED_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "policy"
 def raw_features(frontier, frontier_edges, unexplored, level, n, m, prev_dir, prev_ns):
     """The features the traversal kernels compute on the device
     (policy_feature in bd_policy.cuh), in the same order, units and float32
-    arithmetic."""
+    arithmetic: differences of log2(1 + x) terms, so that one range covers
+    graphs of every size --
+      0 m_f vs m_u, 1 frontier vs n, 2 m_u vs 2m, 3 level (alone),
+      4 m vs n, 5 previous direction, 6 previous step us vs m / 2^20,
+      7 m_f vs frontier."""
     one = np.float32(1.0)
 
-    def lg(x, scale=None):
-        v = np.float32(max(int(x), 0))
-        if scale is not None:
-            v = np.float32(v * np.float32(scale))
-        return np.log2(one + v, dtype=np.float32)
+    def lg(x):
+        return np.log2(one + np.maximum(np.float32(x), np.float32(0)), dtype=np.float32)
+
+    def f32(x):
+        return np.float32(max(int(x), 0))
 
     f = np.empty(NUM_FEATURES, np.float32)
-    f[0] = lg(frontier)
-    f[1] = lg(frontier_edges)
-    f[2] = lg(unexplored)
-    f[3] = level
-    f[4] = lg(n)
-    f[5] = lg(m)
-    f[6] = prev_dir
-    f[7] = lg(prev_ns, 1e-3)
+    f[0] = lg(f32(frontier_edges)) - lg(f32(unexplored))
+    f[1] = lg(f32(frontier)) - lg(f32(n))
+    f[2] = lg(f32(unexplored)) - lg(f32(2 * m))
+    f[3] = lg(f32(level))
+    f[4] = lg(f32(m)) - lg(f32(n))
+    f[5] = prev_dir
+    f[6] = lg(f32(prev_ns) * np.float32(1e-3)) - lg(f32(m) * np.float32(1.0 / 1048576.0))
+    f[7] = lg(f32(frontier_edges)) - lg(f32(frontier))
     return f
 
 
@@ -220,6 +224,7 @@ class Policy:
     lo: np.ndarray | None = None  # trusted raw-feature range (None: unbounded)
     hi: np.ndarray | None = None
     extremes: tuple | None = None  # training (min, max, std) per feature
+    band: tuple | None = None  # feature-0 range the network decides in
 
     def trusts(self, raw: np.ndarray) -> bool:
         if self.lo is None:
@@ -335,7 +340,7 @@ def he_init(seed: int = 0) -> np.ndarray:
                            np.zeros(2)]).astype(np.float32)
 
 
-def fit(X, y, w, epochs=3000, lr=3e-3, weight_decay=1e-4, seed=0, widen=3.0):
+def fit(X, y, w, epochs=3000, lr=3e-3, weight_decay=1e-4, seed=0, widen=3.0, band=None):
     """Standardises the features and trains on the device; returns a Policy
     (margin 0) whose trusted range is the training extremes widened by
     `widen` standard deviations, and the loss history."""
@@ -347,21 +352,43 @@ def fit(X, y, w, epochs=3000, lr=3e-3, weight_decay=1e-4, seed=0, widen=3.0):
     hist = bd.policy_train(params, Xs, y, w, epochs, lr, weight_decay)
     pol = Policy(params, mean, inv_std, 0.0, {}, None, None)
     pol.extremes = (X.min(0).astype(np.float32), X.max(0).astype(np.float32), std)
+    pol.band = band
     set_widen(pol, widen)
     return pol, hist
 
 
-# raw features that measure the graph's size (log2 n, log2 m): the network is
-# never trusted on a graph larger than every graph it was trained on
-SIZE_FEATURES = (4, 5)
-
-
 def set_widen(pol: Policy, widen: float) -> None:
+    """Trusted range: the training extremes widened by `widen` standard
+    deviations, feature 0 cut to the policy's band (the kernels test
+    feature 0 first and run the network only inside it)."""
     xmin, xmax, std = pol.extremes
     pol.lo = (xmin - widen * std).astype(np.float32)
     pol.hi = (xmax + widen * std).astype(np.float32)
-    for i in SIZE_FEATURES:
-        pol.hi[i] = xmax[i]
+    if pol.band is not None:
+        pol.lo[0] = max(pol.lo[0], np.float32(pol.band[0]))
+        pol.hi[0] = min(pol.hi[0], np.float32(pol.band[1]))
+
+
+# the band extends this far (log2 units) past the feature-0 values at which
+# the best direction differed from the rule's
+BAND_PAD = 1.0
+
+
+def disagreement_band(tables, rule_fn):
+    """The range of feature 0 (log2 of frontier edges over unexplored edges)
+    over the levels of `tables` at which the faster direction is not the
+    rule's, padded by BAND_PAD; None when the rule is right at every level.
+    Outside it the rule decides without the network."""
+    f0 = []
+    for t in tables:
+        dirs = rule_fn(t)
+        for lv in range(t.levels):
+            best = "B" if t.t_bu[lv] < t.t_td[lv] else "T"
+            if best != dirs[lv]:
+                f0.append(t.features(lv, 0, 0.0)[0])
+    if not f0:
+        return None
+    return float(min(f0) - BAND_PAD), float(max(f0) + BAND_PAD)
 
 
 WIDEN_CANDIDATES = (0.0, 0.5, 1.0, 2.0, 3.0)
@@ -371,12 +398,11 @@ OFF = float("inf")  # margin of a policy that leaves every step to the rule
 
 def inference_overhead(spec, policy, batched: bool, roots=16, repeats=3):
     """Measured cost of the policy inside the traversal kernel, in ns per
-    level: (features only, features + network).  Three handles run the same
-    roots: no policy, a policy trusted nowhere (the kernel computes the
-    features and stops), and one trusted everywhere whose margin never lets
-    it override (the network runs, the rule still decides)."""
-    g = bd.Graph.rmat(spec["scale"], spec["edge_factor"], spec["a"], spec["b"], spec["c"],
-                      spec["d"], spec["seed"], order=bd.ORDER_HUB)
+    level: (outside its band, inside it).  Three handles run the same
+    roots: no policy, a policy trusted nowhere (the kernel tests feature 0
+    against the band and stops), and one trusted everywhere whose margin
+    never lets it override (the network runs, the rule still decides)."""
+    g = spec_graph(spec)
     rs = g.pick_roots(spec["seed"] + 1, 64 if batched else roots)
     big = np.full(NUM_FEATURES, 1e30, np.float32)
     make = (lambda: bd.BatchedBFS(g, len(rs))) if batched else \
@@ -448,8 +474,12 @@ def train_policy(tables, rule_fn, args, log, batched=False):
     top = max(t.meta["scale"] for t in train)
     lower = [t for t in train if t.meta["scale"] < top]
     upper = [t for t in train if t.meta["scale"] == top]
+    band = disagreement_band(train, rule_fn)
+    log(f"feature-0 band where the rule's choice is not the faster one: {band}")
+    if band is None:  # the rule is right everywhere: an empty band keeps the network out
+        band = (1.0, -1.0)
     X, y, w = dataset(lower)
-    probe, _ = fit(X, y, w, epochs=args.epochs, lr=args.lr)
+    probe, _ = fit(X, y, w, epochs=args.epochs, lr=args.lr, band=band)
     widen_cost = []
     for widen in WIDEN_CANDIDATES:
         set_widen(probe, widen)
@@ -458,7 +488,7 @@ def train_policy(tables, rule_fn, args, log, batched=False):
     widen = min(widen_cost)[1]
     log(f"trusted range for extrapolation to scale {top}: training extremes +{widen} sd")
     X, y, w = dataset(train)
-    policy, hist = fit(X, y, w, epochs=args.epochs, lr=args.lr, widen=widen)
+    policy, hist = fit(X, y, w, epochs=args.epochs, lr=args.lr, widen=widen, band=band)
     overhead = inference_overhead(upper[0].meta, policy, batched)
     log(f"inference cost per level: features {overhead[0]:.0f} ns, network {overhead[1]:.0f} ns")
     policy.margin = OFF
@@ -495,30 +525,50 @@ def train_policy(tables, rule_fn, args, log, batched=False):
     return policy, rb, rl
 
 
-def training_graph_specs(count=200, seed=2024):
-    """The training distribution: scales 16-22, A ~ U[0.45, 0.65],
-    D = 0.05, B = C = (1 - A - D) / 2, edge factor 16."""
+def training_graph_specs(count=200, seed=2024, large=True, grids=True):
+    """The training distribution: RMAT scales 16-22, A ~ U[0.45, 0.65],
+    D = 0.05, B = C = (1 - A - D) / 2, edge factor 16; with `large`, five
+    more at scales 23-24 (A = 0.57); with `grids`, six rows x cols grids
+    (512^2 to 2048^2, 1 % of the edges deleted), whose thousands of small
+    levels are the high-diameter case.  Graph seeds decide the split
+    (seed % 5: 0 report, 1 validation, else training)."""
     rng = np.random.default_rng(seed)
     specs = []
     for k in range(count):
         a = float(rng.uniform(0.45, 0.65))
         d = 0.05
         b = c = (1.0 - a - d) / 2
-        specs.append({"scale": int(16 + k % 7), "edge_factor": 16, "a": a, "b": b, "c": c, "d": d,
-                      "seed": 10_000 + k})
+        specs.append({"kind": "rmat", "scale": int(16 + k % 7), "edge_factor": 16, "a": a, "b": b,
+                      "c": c, "d": d, "seed": 10_000 + k})
+    if large:
+        for scale, s in ((23, 20_002), (23, 20_003), (23, 20_001), (24, 20_012), (24, 20_014)):
+            specs.append({"kind": "rmat", "scale": scale, "edge_factor": 16, "a": 0.57,
+                          "b": 0.19, "c": 0.19, "d": 0.05, "seed": s})
+    if grids:
+        for side, s in ((512, 30_002), (1024, 30_003), (1024, 30_001), (2048, 30_004),
+                        (2048, 30_007), (2048, 30_005)):
+            specs.append({"kind": "grid", "rows": side, "cols": side, "delete": 0.01,
+                          "scale": int(np.log2(side * side)), "seed": s})
     return specs
+
+
+def spec_graph(s, order=None):
+    """The graph of a training spec, in the layout the policy runs on."""
+    order = bd.ORDER_HUB if order is None else order
+    if s.get("kind", "rmat") == "grid":
+        return bd.Graph.grid(s["rows"], s["cols"], s["delete"], s["seed"], order=order)
+    return bd.Graph.rmat(s["scale"], s["edge_factor"], s["a"], s["b"], s["c"], s["d"], s["seed"],
+                         order=order)
 
 
 def collect(specs, roots_per_graph=8, repeats=2, log=None, order=None):
     """Level tables of the training graphs, built with the layout the
     policy will run on (the hub numbering by default, as the benchmark's
     graphs are; the layout changes step costs)."""
-    order = bd.ORDER_HUB if order is None else order
     tables = []
     for i, s in enumerate(specs):
-        g = bd.Graph.rmat(s["scale"], s["edge_factor"], s["a"], s["b"], s["c"], s["d"], s["seed"],
-                          order=order)
-        roots = g.pick_roots(s["seed"], roots_per_graph)
+        g = spec_graph(s, order)
+        roots = g.pick_roots(s["seed"], roots_per_graph if s.get("kind") != "grid" else 2)
         for t in measure_tables(g, roots, repeats=repeats, with_beamer=False):
             t.meta.update(s)
             tables.append(t)
@@ -535,8 +585,7 @@ def train_batched(args, log):
     tables = []
     t0 = time.time()
     for i, s in enumerate(specs):
-        g = bd.Graph.rmat(s["scale"], s["edge_factor"], s["a"], s["b"], s["c"], s["d"], s["seed"],
-                          order=bd.ORDER_HUB)
+        g = spec_graph(s)
         tab = measure_tables_batched(g, g.pick_roots(s["seed"], 64), repeats=2)
         tab.meta.update(s)
         tables.append(tab)
@@ -547,15 +596,56 @@ def train_batched(args, log):
     policy, rb, rl = train_policy(tables, alpha_dirs, args, log, batched=True)
     policy.info.update({"kind": "batched", "graphs": args.graphs,
                         "distribution": "RMAT scales 16-22, A~U[0.45,0.65], D=0.05, "
-                                        "B=C=(1-A-D)/2, ef 16, 64 roots per graph, hub numbering"})
+                                        "B=C=(1-A-D)/2, ef 16; 5 RMAT graphs at scales 23-24; "
+                                        "6 grids 512^2-2048^2 (1% of edges deleted); 64 roots per "
+                                        "graph, hub numbering"})
     policy.save(args.out)
     log(f"saved {args.out}: rule regret {rb['regret_frac']:.3%}, learned {rl['regret_frac']:.3%}")
+    return 0
+
+
+def headroom(args, log):
+    """How much any direction policy could gain on one graph: per level, the
+    measured cost of both directions (forced runs; a level discovers the
+    same vertices either way), the rule's choices, and the sum of the
+    per-level minima against the rule's cost on the same table."""
+    g = bd.Graph.rmat(args.scale, 16, seed=args.seed, order=bd.ORDER_HUB)
+    out = {"graph": {"scale": args.scale, "seed": args.seed, "n": g.num_vertices(),
+                     "m": g.num_edges()}}
+    if args.batched:
+        tab = measure_tables_batched(g, g.pick_roots(args.root_seed, 64), repeats=args.repeats)
+        rule = alpha_dirs(tab)
+        tables, names = [tab], ("push", "pull")
+    else:
+        tables = measure_tables(g, g.pick_roots(args.root_seed, args.roots), repeats=args.repeats,
+                                with_beamer=False)
+        rule, names = None, ("top-down", "bottom-up")
+    rows = []
+    for t in tables:
+        dirs = rule if rule is not None else beamer_dirs(t)
+        rows.append({"frontier": [int(x) for x in t.frontier],
+                     names[0] + "_us": [round(x * 1e-3, 1) for x in t.t_td],
+                     names[1] + "_us": [round(x * 1e-3, 1) for x in t.t_bu],
+                     "rule": dirs, "rule_us": round(t.cost_ns(dirs) * 1e-3, 1),
+                     "best_us": round(t.optimal_ns() * 1e-3, 1)})
+    r = regret(tables, (lambda t: rule) if rule is not None else beamer_dirs)
+    out.update({"kind": "batched (64 roots)" if args.batched else f"single-source ({args.roots} roots)",
+                "tables": rows if args.batched else rows[:4], "rule_regret": r})
+    print(json.dumps(out))
+    g.close()
     return 0
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
+    h = sub.add_parser("headroom", help="per-level costs of both directions against the rule")
+    h.add_argument("--scale", type=int, default=24)
+    h.add_argument("--seed", type=int, default=24)
+    h.add_argument("--root-seed", type=int, default=0)
+    h.add_argument("--roots", type=int, default=16)
+    h.add_argument("--repeats", type=int, default=3)
+    h.add_argument("--batched", action="store_true")
     t = sub.add_parser("train")
     t.add_argument("--graphs", type=int, default=200)
     t.add_argument("--roots", type=int, default=8)
@@ -567,6 +657,8 @@ def main(argv=None):
                    help="train the push/pull policy of the 64-root batched traversal")
     args = ap.parse_args(argv)
     log = lambda s: print(f"[policy {time.strftime('%H:%M:%S')}] {s}", flush=True)  # noqa: E731
+    if args.cmd == "headroom":
+        return headroom(args, log)
     if args.batched:
         args.out = args.out or BATCHED_PATH
         return train_batched(args, log)
@@ -579,7 +671,9 @@ def main(argv=None):
     policy.info.update({"kind": "single-source", "graphs": args.graphs,
                         "roots_per_graph": args.roots,
                         "distribution": "RMAT scales 16-22, A~U[0.45,0.65], D=0.05, "
-                                        "B=C=(1-A-D)/2, ef 16, hub numbering"})
+                                        "B=C=(1-A-D)/2, ef 16; 5 RMAT graphs at scales 23-24; "
+                                        "6 grids 512^2-2048^2 (1% of edges deleted, 2 roots "
+                                        "each); hub numbering"})
     policy.save(args.out)
     log(f"saved {args.out}: beamer regret {rb['regret_frac']:.3%}, learned {rl['regret_frac']:.3%}")
     if args.tables_out:

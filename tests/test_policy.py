@@ -150,14 +150,63 @@ def test_trained_policies_at_scale24_held_out():
     pol = P.Policy.load()
     rb = P.regret(tables, P.beamer_dirs)
     rl = P.regret(tables, lambda t: P.policy_dirs(pol, t))
-    print(f"scale 24 regret: Beamer {rb['regret_frac']:.2%}, learned {rl['regret_frac']:.2%}")
+    print(f"scale 24 regret: Beamer {rb['regret_frac']:.2%}, learned {rl['regret_frac']:.2%}, "
+          f"consulted at {_consulted(pol, tables, P.beamer_dirs)} of "
+          f"{sum(t.levels for t in tables)} levels")
     assert rl["cost_ms"] <= rb["cost_ms"] * 1.005, (rl, rb)
     tab = P.measure_tables_batched(g, g.pick_roots(8, 64), repeats=2)
     bpol = P.Policy.load(P.BATCHED_PATH)
     rule = P.regret([tab], P.alpha_dirs)
     rl = P.regret([tab], lambda t: P.policy_dirs(bpol, t, rule=P.alpha_dirs(t)))
-    print(f"scale 24 batched regret: rule {rule['regret_frac']:.2%}, learned {rl['regret_frac']:.2%}")
+    print(f"scale 24 batched regret: rule {rule['regret_frac']:.2%}, learned {rl['regret_frac']:.2%}, "
+          f"consulted at {_consulted(bpol, [tab], P.alpha_dirs)} of {tab.levels} levels")
     assert rl["cost_ms"] <= rule["cost_ms"] * 1.005, (rl, rule)
+
+
+def _consulted(pol, tables, rule_fn):
+    """Levels at which the policy's trusted range (the band on feature 0
+    included) lets the network decide, over the rule's path."""
+    from beedrill_b200 import policy as P
+    count = 0
+    for t in tables:
+        prev_dir, prev_ns = 0, 0.0
+        for lv, d in enumerate(P.policy_dirs(pol, t, rule=rule_fn(t))):
+            if pol.trusts(t.features(lv, prev_dir, prev_ns)):
+                count += 1
+            prev_dir = 1 if d == "B" else 0
+            prev_ns = t.t_bu[lv] if d == "B" else t.t_td[lv]
+    return count
+
+
+@pytest.mark.gpu
+def test_trained_policies_on_a_held_out_grid():
+    """The high-diameter contrast: a 1024 x 1024 grid with 1 % of its edges
+    deleted (a seed no training grid used).  Grids are in the training set,
+    and the features are scale-free, so the network's range covers their
+    thousands of small levels; its decisions must cost no more than the
+    rule's (single-source against Beamer, batched against its rule)."""
+    bd = pytest.importorskip("beedrill_b200")
+    from beedrill_b200 import policy as P
+    if not (os.path.exists(P.DEFAULT_PATH) and os.path.exists(P.BATCHED_PATH)):
+        pytest.skip("no trained policies committed")
+    g = bd.Graph.grid(1024, 1024, 0.01, 4242, order=bd.ORDER_HUB)
+    tables = P.measure_tables(g, g.pick_roots(3, 2), repeats=2, with_beamer=False)
+    pol = P.Policy.load()
+    net = P.decisions_policy(pol) or pol
+    rb = P.regret(tables, P.beamer_dirs)
+    rn = P.regret(tables, lambda t: P.policy_dirs(net, t))
+    print(f"grid regret: Beamer {rb['regret_frac']:.2%}, network {rn['regret_frac']:.2%}, "
+          f"consulted at {_consulted(net, tables, P.beamer_dirs)} of "
+          f"{sum(t.levels for t in tables)} levels")
+    assert rn["cost_ms"] <= rb["cost_ms"] * 1.005, (rn, rb)
+    tab = P.measure_tables_batched(g, g.pick_roots(4, 64), repeats=2)
+    bpol = P.Policy.load(P.BATCHED_PATH)
+    rule = P.regret([tab], P.alpha_dirs)
+    rl = P.regret([tab], lambda t: P.policy_dirs(bpol, t, rule=P.alpha_dirs(t)))
+    print(f"grid batched regret: rule {rule['regret_frac']:.2%}, learned {rl['regret_frac']:.2%}, "
+          f"consulted at {_consulted(bpol, [tab], P.alpha_dirs)} of {tab.levels} levels")
+    assert rl["cost_ms"] <= rule["cost_ms"] * 1.005, (rl, rule)
+    g.close()
 
 
 @pytest.mark.gpu
@@ -206,7 +255,7 @@ def test_in_kernel_decisions_follow_the_network():
     from beedrill_b200 import policy as P
     rng = np.random.default_rng(11)
     pol = P.Policy(PO.init_params(21).astype(np.float32), np.array(
-        [10, 20, 25, 3, 18, 22, 0.5, 5], np.float32), np.full(8, 0.25, np.float32), 0.05)
+        [-5, -8, -1, 1.5, 4, 0.5, 3, 5], np.float32), np.full(8, 0.25, np.float32), 0.05)
     checked = 0
     for scale in (14, 16, 17):
         g = bd.Graph.rmat(scale, 16, seed=int(rng.integers(1 << 30)), order=bd.ORDER_DEGREE)

@@ -52,19 +52,41 @@ def test_batched_rule_mirror():
     assert dirs[3] == "T"
 
 
-def test_trusted_range_never_past_the_largest_training_graph():
+def test_trusted_range_is_the_band_on_feature_0_and_scale_free():
+    """The features are differences of logarithms, so a graph larger than
+    any training graph is not outside the trusted range by its size; the
+    range of feature 0 is cut to the band where the rule's choice was not
+    the faster one, and outside it the network is never consulted."""
     rng = np.random.default_rng(0)
     X = rng.normal(0, 1, (200, 8)).astype(np.float32)
-    X[:, 4] = rng.uniform(16, 22, 200)    # log2 n of the training graphs
-    X[:, 5] = X[:, 4] + 4                 # log2 m
     pol = P.Policy(np.zeros(1410, np.float32), np.zeros(8, np.float32), np.ones(8, np.float32))
     pol.extremes = (X.min(0), X.max(0), X.std(0))
+    pol.band = (-0.5, 0.25)
     P.set_widen(pol, 3.0)
-    assert pol.hi[4] == X[:, 4].max() and pol.hi[5] == X[:, 5].max()
-    assert pol.hi[0] > X[:, 0].max() and pol.lo[4] < X[:, 4].min()
-    raw = X[0].copy()
-    raw[4] = X[:, 4].max() + 0.5          # a larger graph than any in training
+    assert pol.lo[0] == np.float32(-0.5) and pol.hi[0] == np.float32(0.25)
+    assert pol.hi[4] > X[:, 4].max() and pol.lo[4] < X[:, 4].min()
+    raw = np.zeros(8, np.float32)
+    assert pol.trusts(raw)
+    raw[0] = 0.5
     assert not pol.trusts(raw)
+    # the same frontier shares at scale 16 and at scale 26 give the same
+    # size-free features (0, 1, 2, 7) and the same average-degree feature
+    a = P.raw_features(1 << 10, 1 << 14, 1 << 20, 3, 1 << 16, 1 << 20, 0, 0)
+    b = P.raw_features(1 << 20, 1 << 24, 1 << 30, 3, 1 << 26, 1 << 30, 0, 0)
+    assert np.allclose(a[[0, 1, 2, 4, 7]], b[[0, 1, 2, 4, 7]], atol=2e-3)
+
+
+def test_disagreement_band():
+    """The band is the feature-0 range of the levels where the faster
+    direction is not the rule's, padded; None when the rule is always
+    right."""
+    t = _table(1 << 16, 1 << 20, np.array([1, 100, 5000, 200]), np.array([16, 2000, 80000, 3000]),
+               np.array([2 << 20, 2 << 20, 2 << 20, 2 << 19]), np.array([1.0, 5.0, 90.0, 2.0]),
+               np.array([50.0, 50.0, 10.0, 1.0]))
+    assert P.disagreement_band([t], lambda tab: "TTBB") is None
+    lo, hi = P.disagreement_band([t], lambda tab: "TTTB")
+    f0 = t.features(2, 0, 0.0)[0]
+    assert lo == pytest.approx(f0 - P.BAND_PAD) and hi == pytest.approx(f0 + P.BAND_PAD)
 
 
 def _fake_train(params, Xs, y, w, epochs, lr, wd):
