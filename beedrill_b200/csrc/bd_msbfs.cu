@@ -415,19 +415,44 @@ __device__ void ms_push_step(const MsParams &p, const MsView &sv, MsWarpScratch 
     const int cur = sv.step % 3, nxt = (sv.step + 1) % 3;
     MsAcc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
-    // large frontier vertices: chunk c of vertex ql[i]
-    for (long long c = gw; c < sv.f_chunks; c += nw) {
-        long long lo = 0, hi = sv.f_large - 1;
-        while (lo < hi) {
-            long long mid = (lo + hi + 1) >> 1;
-            if ((long long)__ldcg(&p.qlb[cur][mid]) <= c) { lo = mid; } else { hi = mid - 1; }
+    // large frontier vertices: chunk c of vertex ql[i].  Each warp takes a
+    // contiguous range of chunk ids -- one binary search for its first
+    // vertex, then a forward walk -- so no chunk pays a search of its own
+    // (the frontier of hubs at the second level splits into hundreds of
+    // thousands of chunks), and a vertex's frontier word and list bounds
+    // are loaded once per warp.
+    if (sv.f_chunks > 0) {
+        const long long per = (sv.f_chunks + nw - 1) / nw;
+        long long c = gw * per;
+        const long long c_end = min(c + per, sv.f_chunks);
+        if (c < c_end) {
+            long long lo = 0, hi = sv.f_large - 1;  // last i with qlb[i] <= c
+            while (lo < hi) {
+                const long long mid = (lo + hi + 1) >> 1;
+                if ((long long)__ldcg(&p.qlb[cur][mid]) <= c) { lo = mid; } else { hi = mid - 1; }
+            }
+            long long vbase = (long long)__ldcg(&p.qlb[cur][lo]);
+            long long vnext = lo + 1 < sv.f_large ? (long long)__ldcg(&p.qlb[cur][lo + 1])
+                                                  : sv.f_chunks;
+            uint32_t u = __ldcg(&p.ql[cur][lo]);
+            ull bits = __ldcg(&p.F[cur][u]);
+            int64_t ub = __ldg(&p.off[u]), ue = __ldg(&p.off[u + 1]);
+            for (; c < c_end; ++c) {
+                while (c >= vnext) {  // the next vertex's chunks
+                    lo += 1;
+                    vbase = vnext;
+                    vnext = lo + 1 < sv.f_large ? (long long)__ldcg(&p.qlb[cur][lo + 1])
+                                                : sv.f_chunks;
+                    u = __ldcg(&p.ql[cur][lo]);
+                    bits = __ldcg(&p.F[cur][u]);
+                    ub = __ldg(&p.off[u]);
+                    ue = __ldg(&p.off[u + 1]);
+                }
+                const int64_t b = ub + (c - vbase) * (int64_t)p.chunk;
+                push_edges(p, acc, cur, nxt, new_level, u, bits, b,
+                           min(ue, b + (int64_t)p.chunk), loc);
+            }
         }
-        const uint32_t u = __ldcg(&p.ql[cur][lo]);
-        const long long j = c - (long long)__ldcg(&p.qlb[cur][lo]);
-        const ull bits = __ldcg(&p.F[cur][u]);
-        const int64_t ub = __ldg(&p.off[u]), ue = __ldg(&p.off[u + 1]);
-        const int64_t b = ub + j * (int64_t)p.chunk;
-        push_edges(p, acc, cur, nxt, new_level, u, bits, b, min(ue, b + (int64_t)p.chunk), loc);
     }
     // small frontier vertices, 32 per warp: their lists are laid end to end
     // and dealt to the lanes kPushU x 32 arcs at a time
@@ -495,6 +520,9 @@ __device__ void ms_pull_heavy(const MsParams &p, const MsView &sv, MsLocal &loc)
     MsAcc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
     const long long total = p.n_heavy ? (long long)__ldg(&p.heavy_cbase[p.n_heavy]) : 0;
+    // chunks dealt round robin: the chunks of one heavy vertex run on
+    // different warps at once, and any of them may find the vertex's last
+    // missing lanes
     for (long long c = gw; c < total; c += nw) {
         long long lo = 0, hi = p.n_heavy - 1;  // last i with heavy_cbase[i] <= c
         while (lo < hi) {

@@ -374,6 +374,25 @@ def set_widen(pol: Policy, widen: float) -> None:
 BAND_PAD = 1.0
 
 
+def network_band(policy: Policy, tables, rule_fn):
+    """The feature-0 range (padded by BAND_PAD) of the levels at which the
+    policy, trusted and confident, picks another direction than the rule,
+    along its own path over `tables`; None when it never does."""
+    f0 = []
+    for t in tables:
+        rule = rule_fn(t)
+        dirs = policy_dirs(policy, t, rule=rule)
+        prev_dir, prev_ns = 0, 0.0
+        for lv, d in enumerate(dirs):
+            if d != rule[lv]:
+                f0.append(t.features(lv, prev_dir, prev_ns)[0])
+            prev_dir = 1 if d == "B" else 0
+            prev_ns = t.t_bu[lv] if d == "B" else t.t_td[lv]
+    if not f0:
+        return None
+    return float(min(f0) - BAND_PAD), float(max(f0) + BAND_PAD)
+
+
 def disagreement_band(tables, rule_fn):
     """The range of feature 0 (log2 of frontier edges over unexplored edges)
     over the levels of `tables` at which the faster direction is not the
@@ -396,12 +415,20 @@ MARGIN_CANDIDATES = (0.0, 0.25, 0.5, 1.0, 2.0)
 OFF = float("inf")  # margin of a policy that leaves every step to the rule
 
 
-def inference_overhead(spec, policy, batched: bool, roots=16, repeats=3):
+# the graph the inference cost is measured on: thousands of small levels, so
+# a per-level cost of a few hundred ns stands out of the run-to-run noise
+OVERHEAD_SPEC = {"kind": "grid", "rows": 1024, "cols": 1024, "delete": 0.01, "scale": 20,
+                 "seed": 31_337}
+
+
+def inference_overhead(spec, policy, batched: bool, roots=4, repeats=5):
     """Measured cost of the policy inside the traversal kernel, in ns per
     level: (outside its band, inside it).  Three handles run the same
     roots: no policy, a policy trusted nowhere (the kernel tests feature 0
     against the band and stops), and one trusted everywhere whose margin
-    never lets it override (the network runs, the rule still decides)."""
+    never lets it override (the network runs, the rule still decides).
+    `spec` None: OVERHEAD_SPEC."""
+    spec = OVERHEAD_SPEC if spec is None else spec
     g = spec_graph(spec)
     rs = g.pick_roots(spec["seed"] + 1, 64 if batched else roots)
     big = np.full(NUM_FEATURES, 1e30, np.float32)
@@ -489,7 +516,14 @@ def train_policy(tables, rule_fn, args, log, batched=False):
     log(f"trusted range for extrapolation to scale {top}: training extremes +{widen} sd")
     X, y, w = dataset(train)
     policy, hist = fit(X, y, w, epochs=args.epochs, lr=args.lr, widen=widen, band=band)
-    overhead = inference_overhead(upper[0].meta, policy, batched)
+    # the network is needed only where it disagrees with the rule: cut the
+    # band to the feature-0 range of those levels (training tables, along
+    # the network's own path), so elsewhere the kernels skip it
+    tight = network_band(policy, train, rule_fn)
+    log(f"feature-0 band where the network overrides the rule: {tight}")
+    policy.band = tight if tight is not None else (1.0, -1.0)
+    set_widen(policy, widen)
+    overhead = inference_overhead(None, policy, batched)
     log(f"inference cost per level: features {overhead[0]:.0f} ns, network {overhead[1]:.0f} ns")
     policy.margin = OFF
     rule_cost = priced_cost_ns(policy, val, rule_fn, overhead)
