@@ -67,6 +67,12 @@ int grid_for_warps(int64_t warps)
     return (int)b;
 }
 
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x)
+{
+    for (int d = 16; d > 0; d >>= 1) { x += __shfl_xor_sync(0xffffffffu, x, d); }
+    return x;
+}
+
 // Root of x's tree, pointing each vertex on the way at its grandparent.
 __device__ __forceinline__ uint32_t cc_find(uint32_t *parent, uint32_t x)
 {
@@ -255,12 +261,26 @@ __global__ void __launch_bounds__(kThreads) cc_heavy_kernel(
     }
 }
 
-// Labels, sizes and roots.  Sizes: the lanes of a warp that share a label
-// add it once (the largest component's label is shared by most lanes).
-__global__ void cc_compress_kernel(uint32_t *parent, int64_t n, int64_t *label, int64_t *size,
-                                   unsigned long long *roots)
+// Labels, sizes and roots.  `hint` is a vertex of the largest tree (or
+// ~0u): the lanes whose label is that tree's root count it in a block-wide
+// total added once per block, as do the roots; the lanes of a warp that
+// share any other label add it once (__match_any_sync).  (One atomic per
+// warp on the largest component's size and on the root count put a few
+// hundred thousand atomics on two addresses, which serialise at their L2
+// slices.)
+__global__ void cc_compress_kernel(uint32_t *parent, int64_t n, uint32_t hint, int64_t *label,
+                                   int64_t *size, unsigned long long *roots)
 {
+    __shared__ uint32_t giant;
+    __shared__ unsigned long long blk_giant, blk_roots;
     const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        giant = hint < n ? cc_find(parent, hint) : 0xFFFFFFFFu;
+        blk_giant = blk_roots = 0;
+    }
+    __syncthreads();
+    const uint32_t g = giant;
+    unsigned long long my_giant = 0, my_roots = 0;
     for (int64_t base = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane; base < n;
          base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t v = base + lane;
@@ -268,16 +288,29 @@ __global__ void cc_compress_kernel(uint32_t *parent, int64_t n, int64_t *label, 
         uint32_t r = 0xFFFFFFFFu;
         if (valid) {
             r = cc_find(parent, (uint32_t)v);
-            __stcg(&parent[v], r);
             __stcs(&label[v], (int64_t)r);
         }
-        const unsigned same = __match_any_sync(0xffffffffu, r);
-        if (valid && lane == __ffs(same) - 1) {
+        const bool other = valid && r != g;
+        const unsigned same = __match_any_sync(0xffffffffu, other ? r : 0xFFFFFFFFu);
+        if (other && lane == __ffs(same) - 1) {
             atomicAdd(reinterpret_cast<unsigned long long *>(&size[r]),
                       (unsigned long long)__popc(same));
         }
-        const unsigned mask = __ballot_sync(0xffffffffu, valid && r == (uint32_t)v);
-        if (lane == 0 && mask) { atomicAdd(roots, (unsigned long long)__popc(mask)); }
+        my_giant += (valid && r == g) ? 1ull : 0ull;
+        my_roots += (valid && r == (uint32_t)v) ? 1ull : 0ull;
+    }
+    my_giant = warp_sum_u64(my_giant);
+    my_roots = warp_sum_u64(my_roots);
+    if (lane == 0) {
+        if (my_giant) { atomicAdd(&blk_giant, my_giant); }
+        if (my_roots) { atomicAdd(&blk_roots, my_roots); }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (blk_giant) {
+            atomicAdd(reinterpret_cast<unsigned long long *>(&size[g]), blk_giant);
+        }
+        if (blk_roots) { atomicAdd(roots, blk_roots); }
     }
 }
 
@@ -410,7 +443,7 @@ bd_status bd_components_run(bd_components *c, bd_components_stats *stats)
                                                   c->cbase);
     bd::cc_heavy_kernel<<<148 * 8, bd::kThreads, 0, s>>>(g->d_off, g->d_adj, c->parent, c->heavy,
                                                         c->counters, c->cbase, first, 1);
-    bd::cc_compress_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(c->parent, n, c->label,
+    bd::cc_compress_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(c->parent, n, skip, c->label,
                                                                     c->size, c->counters + 1);
     BD_CUDA(cudaGetLastError());
     BD_CUDA(cudaEventRecord(c->ev1, s));

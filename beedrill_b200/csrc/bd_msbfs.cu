@@ -189,6 +189,69 @@ __device__ __forceinline__ void ms_append(const MsParams &p, MsAcc *acc, int qn,
     }
 }
 
+// Warp-collective append of up to K new frontier vertices per lane: one
+// atomic for all the small-degree ones of the warp, one for the large ones.
+template <int K>
+__device__ __forceinline__ void ms_append_k(const MsParams &p, MsAcc *acc, int qn,
+                                            const bool (&has)[K], const uint32_t (&v)[K],
+                                            const int64_t (&deg)[K], MsLocal &loc)
+{
+    const int lane = lane_id();
+    unsigned sm[K];
+    bool large[K];
+    unsigned total = 0, any_large = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (has[k]) {
+            loc.vertices += 1;
+            loc.degsum += (ull)deg[k];
+        }
+        large[k] = has[k] && deg[k] >= (int64_t)p.large_deg;
+        sm[k] = __ballot_sync(kFullMask, has[k] && !large[k]);
+        total += __popc(sm[k]);
+        any_large |= __ballot_sync(kFullMask, large[k]);
+    }
+    if (total) {
+        ull base = 0;
+        if (lane == 0) { base = atomicAdd(&acc->small_cnt, (ull)total); }
+        base = __shfl_sync(kFullMask, base, 0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (has[k] && !large[k]) { p.qs[qn][base + __popc(sm[k] & lanemask_lt())] = v[k]; }
+            base += __popc(sm[k]);
+        }
+    }
+    if (any_large) {
+        unsigned count = 0;
+        ull chunks = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (large[k]) {
+                count += 1;
+                chunks += (ull)((deg[k] + p.chunk - 1) / p.chunk);
+            }
+        }
+        const unsigned ci = warp_incl_scan(count);
+        const ull hi = warp_incl_scan(chunks);
+        const unsigned ct = __shfl_sync(kFullMask, ci, 31);
+        const ull ht = __shfl_sync(kFullMask, hi, 31);
+        ull old = 0;
+        if (lane == 0) { old = atomicAdd(&acc->large_packed, ((ull)ct << kLargeShift) | ht); }
+        old = __shfl_sync(kFullMask, old, 0);
+        ull pos = (old >> kLargeShift) + (ci - count);
+        ull cbase = (old & kChunkMask) + (hi - chunks);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (large[k]) {
+                p.ql[qn][pos] = v[k];
+                p.qlb[qn][pos] = cbase;
+                pos += 1;
+                cbase += (ull)((deg[k] + p.chunk - 1) / p.chunk);
+            }
+        }
+    }
+}
+
 // Lanes whose vertex has run out of delivery records: one depth and one
 // parent entry per lane in the vertex-major rows.
 __device__ __forceinline__ void write_rows(const MsParams &p, uint32_t v, ull lanes, int level,
@@ -251,69 +314,6 @@ __device__ void ms_clear_old(const MsParams &p, const MsView &sv)
     const long long nt = (long long)gridDim.x * blockDim.x;
     for (long long i = t; i < sv.p_small; i += nt) { p.F[old][p.qs[old][i]] = 0ull; }
     for (long long i = t; i < sv.p_large; i += nt) { p.F[old][p.ql[old][i]] = 0ull; }
-}
-
-// Warp-collective append of up to K new frontier vertices per lane: one
-// atomic for all the small-degree ones of the warp, one for the large ones.
-template <int K>
-__device__ __forceinline__ void ms_append_k(const MsParams &p, MsAcc *acc, int qn,
-                                            const bool (&has)[K], const uint32_t (&v)[K],
-                                            const int64_t (&deg)[K], MsLocal &loc)
-{
-    const int lane = lane_id();
-    unsigned sm[K];
-    bool large[K];
-    unsigned total = 0, any_large = 0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        if (has[k]) {
-            loc.vertices += 1;
-            loc.degsum += (ull)deg[k];
-        }
-        large[k] = has[k] && deg[k] >= (int64_t)p.large_deg;
-        sm[k] = __ballot_sync(kFullMask, has[k] && !large[k]);
-        total += __popc(sm[k]);
-        any_large |= __ballot_sync(kFullMask, large[k]);
-    }
-    if (total) {
-        ull base = 0;
-        if (lane == 0) { base = atomicAdd(&acc->small_cnt, (ull)total); }
-        base = __shfl_sync(kFullMask, base, 0);
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            if (has[k] && !large[k]) { p.qs[qn][base + __popc(sm[k] & lanemask_lt())] = v[k]; }
-            base += __popc(sm[k]);
-        }
-    }
-    if (any_large) {
-        unsigned count = 0;
-        ull chunks = 0;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            if (large[k]) {
-                count += 1;
-                chunks += (ull)((deg[k] + p.chunk - 1) / p.chunk);
-            }
-        }
-        const unsigned ci = warp_incl_scan(count);
-        const ull hi = warp_incl_scan(chunks);
-        const unsigned ct = __shfl_sync(kFullMask, ci, 31);
-        const ull ht = __shfl_sync(kFullMask, hi, 31);
-        ull old = 0;
-        if (lane == 0) { old = atomicAdd(&acc->large_packed, ((ull)ct << kLargeShift) | ht); }
-        old = __shfl_sync(kFullMask, old, 0);
-        ull pos = (old >> kLargeShift) + (ci - count);
-        ull cbase = (old & kChunkMask) + (hi - chunks);
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            if (large[k]) {
-                p.ql[qn][pos] = v[k];
-                p.qlb[qn][pos] = cbase;
-                pos += 1;
-                cbase += (ull)((deg[k] + p.chunk - 1) / p.chunk);
-            }
-        }
-    }
 }
 
 // push: lanes of frontier vertex u flow into neighbours [b, e), four arcs
@@ -415,44 +415,19 @@ __device__ void ms_push_step(const MsParams &p, const MsView &sv, MsWarpScratch 
     const int cur = sv.step % 3, nxt = (sv.step + 1) % 3;
     MsAcc *acc = &p.ctrl->acc[sv.step % 3];
     const int new_level = sv.level + 1;
-    // large frontier vertices: chunk c of vertex ql[i].  Each warp takes a
-    // contiguous range of chunk ids -- one binary search for its first
-    // vertex, then a forward walk -- so no chunk pays a search of its own
-    // (the frontier of hubs at the second level splits into hundreds of
-    // thousands of chunks), and a vertex's frontier word and list bounds
-    // are loaded once per warp.
-    if (sv.f_chunks > 0) {
-        const long long per = (sv.f_chunks + nw - 1) / nw;
-        long long c = gw * per;
-        const long long c_end = min(c + per, sv.f_chunks);
-        if (c < c_end) {
-            long long lo = 0, hi = sv.f_large - 1;  // last i with qlb[i] <= c
-            while (lo < hi) {
-                const long long mid = (lo + hi + 1) >> 1;
-                if ((long long)__ldcg(&p.qlb[cur][mid]) <= c) { lo = mid; } else { hi = mid - 1; }
-            }
-            long long vbase = (long long)__ldcg(&p.qlb[cur][lo]);
-            long long vnext = lo + 1 < sv.f_large ? (long long)__ldcg(&p.qlb[cur][lo + 1])
-                                                  : sv.f_chunks;
-            uint32_t u = __ldcg(&p.ql[cur][lo]);
-            ull bits = __ldcg(&p.F[cur][u]);
-            int64_t ub = __ldg(&p.off[u]), ue = __ldg(&p.off[u + 1]);
-            for (; c < c_end; ++c) {
-                while (c >= vnext) {  // the next vertex's chunks
-                    lo += 1;
-                    vbase = vnext;
-                    vnext = lo + 1 < sv.f_large ? (long long)__ldcg(&p.qlb[cur][lo + 1])
-                                                : sv.f_chunks;
-                    u = __ldcg(&p.ql[cur][lo]);
-                    bits = __ldcg(&p.F[cur][u]);
-                    ub = __ldg(&p.off[u]);
-                    ue = __ldg(&p.off[u + 1]);
-                }
-                const int64_t b = ub + (c - vbase) * (int64_t)p.chunk;
-                push_edges(p, acc, cur, nxt, new_level, u, bits, b,
-                           min(ue, b + (int64_t)p.chunk), loc);
-            }
+    // large frontier vertices: chunk c of vertex ql[i]
+    for (long long c = gw; c < sv.f_chunks; c += nw) {
+        long long lo = 0, hi = sv.f_large - 1;
+        while (lo < hi) {
+            long long mid = (lo + hi + 1) >> 1;
+            if ((long long)__ldcg(&p.qlb[cur][mid]) <= c) { lo = mid; } else { hi = mid - 1; }
         }
+        const uint32_t u = __ldcg(&p.ql[cur][lo]);
+        const long long j = c - (long long)__ldcg(&p.qlb[cur][lo]);
+        const ull bits = __ldcg(&p.F[cur][u]);
+        const int64_t ub = __ldg(&p.off[u]), ue = __ldg(&p.off[u + 1]);
+        const int64_t b = ub + j * (int64_t)p.chunk;
+        push_edges(p, acc, cur, nxt, new_level, u, bits, b, min(ue, b + (int64_t)p.chunk), loc);
     }
     // small frontier vertices, 32 per warp: their lists are laid end to end
     // and dealt to the lanes kPushU x 32 arcs at a time
@@ -1065,24 +1040,25 @@ __global__ void ms_extract_kernel(const int32_t *depth, const uint32_t *parent, 
 // (root0 + r) gets depth_out[(root0 + r) * n + v] and parent_out[...] for
 // every caller vertex v (caller ids, the reference's encoding: the source is
 // its own parent, unreached vertices -deg or -1).  One pass over the group's
-// state instead of one per lane.  A CTA takes a tile of kMatV consecutive
-// caller vertices in two phases:
-//   fill   two threads per vertex (lanes 0-31 and 32-63) read the vertex's
-//          seen word, record count and records once (a record covers every
-//          lane one provider delivered at one level, so the provider is
-//          renamed once per record) and put each reached lane's depth and
-//          parent into a [64][kMatV] shared tile (lanes past the vertex's
-//          records come from the per-lane rows);
-//   write  each half-warp writes one row at a time (rows 2w and 2w + 1 of
-//          warp w, then 8 further): lane l takes vertices 4(l%16)..+3, so a
-//          half-warp stores a row's 64 vertices as 256 B of depths and 512 B
-//          of parents in 16-byte stores, streaming past L2 (4-byte and 8-byte
-//          stores when n is not a multiple of 4).
-// The tile is small (33 KB of shared memory) so that six CTAs share an SM
-// and one's fill phase overlaps another's writes.
-// Each (vertex, lane) costs a few shared-memory operations and 3/4 of a
-// global store instruction; the write traffic (12 bytes per pair) is the
-// bound.
+// state instead of one per lane: thread i of a CTA takes caller vertex
+// v0 + i of a tile of kMatThreads consecutive vertices and
+//   fill   reads the vertex's seen word, record count and records once (a
+//          record covers every lane one provider delivered at one level, so
+//          the provider is renamed once per record) and the per-lane rows of
+//          lanes past its records.  Every distinct (depth, parent) pair gets
+//          a slot of a 16-entry table in shared memory (a record's slot is
+//          its own; lanes one push delivered share a pair), and the slot of
+//          every lane is kept as four 64-bit planes (bit r of plane b = bit b
+//          of lane r's slot): a record sets its lanes in four ORs, whatever
+//          their number, so the threads of a warp do not wait for the one
+//          whose records hold the most lanes;
+//   write  walks the roots with the planes shifted one lane a step: the
+//          lane's slot gives its depth and parent with no branch, and the
+//          CTA's threads store each root's row entries for kMatThreads
+//          consecutive vertices, streaming past L2.
+// No thread reads another's table, so there is no barrier and a warp's
+// writes overlap another's loads.  A lane whose pair finds the table full
+// reads its row in the write loop (more than 16 distinct deliverers).
 struct MsOutParams {
     const int32_t *depth;     // per-lane rows [n][R]
     const uint32_t *parent;
@@ -1099,137 +1075,137 @@ struct MsOutParams {
     int64_t *parent_out;
 };
 
-constexpr int kMatV = 64;                  // vertices per tile
-constexpr int kMatThreads = 2 * kMatV;     // two threads per vertex in the fill phase
-struct MatShared {
-    int32_t depth[64][kMatV];
-    uint32_t parent[64][kMatV];
-    ull seen[kMatV];
-    int64_t unreached[kMatV];
-};
-constexpr size_t kMatSmem = sizeof(MatShared);
+constexpr int kMatThreads = 256;
+constexpr unsigned kMatSlots = 16;
+// per thread: a (depth, parent) pair per slot, slot-major [kMatSlots][threads]
+constexpr size_t kMatSmem = (size_t)kMatThreads * kMatSlots * sizeof(uint2);
+
+// Adds `lanes` to the planes of slot k.
+__device__ __forceinline__ void mat_set_slot(ull (&plane)[4], unsigned k, ull lanes)
+{
+#pragma unroll
+    for (int b = 0; b < 4; ++b) { plane[b] |= ((k >> b) & 1u) ? lanes : 0ull; }
+}
 
 __global__ void __launch_bounds__(kMatThreads) ms_materialize_kernel(MsOutParams o)
 {
     extern __shared__ __align__(16) unsigned char mat_raw[];
-    MatShared &sh = *reinterpret_cast<MatShared *>(mat_raw);
     const int tid = threadIdx.x;
-    const int lane = lane_id(), warp = tid >> 5;
+    uint2 *tab = reinterpret_cast<uint2 *>(mat_raw);  // [kMatSlots][threads]: {depth, parent}
     const ull all = o.lanes >= 64 ? ~0ull : ((1ull << o.lanes) - 1);
-    const bool vec = (o.n & 3) == 0;
-    const long long tiles = (o.n + kMatV - 1) / kMatV;
+    const long long tiles = (o.n + kMatThreads - 1) / kMatThreads;
     for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const int64_t v0 = tile * kMatV;
-        // ---- fill: thread tid handles vertex v0 + (tid % kMatV), lanes of
-        // half tid / kMatV
-        {
-            const int i = tid % kMatV;
-            const ull half = tid < kMatV ? 0x00000000FFFFFFFFull : 0xFFFFFFFF00000000ull;
-            const int64_t v = v0 + i;
-            ull s = 0;
-            int64_t t = 0;
-            if (v < o.n) {
-                t = o.perm ? (int64_t)__ldg(&o.perm[v]) : v;
-                s = __ldcs(&o.seen[t]) & all;
-                if (tid < kMatV) {
-                    const int64_t deg = __ldg(&o.off[v + 1]) - __ldg(&o.off[v]);
-                    sh.seen[i] = s;
-                    sh.unreached[i] = deg != 0 ? -deg : -1;
-                }
-            } else if (tid < kMatV) {
-                sh.seen[i] = 0;
-                sh.unreached[i] = -1;
-            }
-            ull left = s & half;
-            if (left) {
-                const uint4 *rv = o.rec + t * kRecSlots;
-                // the first two slots are read together with the count (they
-                // lie in the vertex's record block whatever the count says)
-                const uint4 x0 = __ldg(&rv[0]), x1 = __ldg(&rv[1]);
-                const unsigned cnt = min(__ldg(&o.rec_cnt[t]), kRecSlots);
-                for (unsigned k0 = 0; k0 < cnt && left; k0 += 4) {
-                    uint4 x[4];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        x[j] = (k0 == 0 && j < 2) ? (j ? x1 : x0)
-                                                  : (k0 + j < cnt ? __ldg(&rv[k0 + j])
-                                                                  : make_uint4(0, 0, 0, 0));
-                    }
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        ull mask = k0 + j < cnt ? (((ull)x[j].y << 32) | x[j].x) & left : 0ull;
-                        if (!mask) { continue; }
-                        left &= ~mask;
-                        // (a provider id out of range would only come from a
-                        // broken record; it is passed through, not followed)
-                        const uint32_t prov =
-                            o.iperm && x[j].z < o.n ? __ldg(&o.iperm[x[j].z]) : x[j].z;
-                        const int32_t d = (int32_t)x[j].w;
-                        do {
-                            const int r = __ffsll((long long)mask) - 1;
-                            mask &= mask - 1;
-                            sh.depth[r][i] = d;
-                            sh.parent[r][i] = prov;
-                        } while (mask);
-                    }
-                }
-                while (left) {  // lanes past the vertex's records: the per-lane rows
-                    const int r = __ffsll((long long)left) - 1;
-                    left &= left - 1;
-                    const uint32_t p = __ldcs(&o.parent[t * o.R + r]);
-                    sh.depth[r][i] = __ldcs(&o.depth[t * o.R + r]);
-                    sh.parent[r][i] = o.iperm && p < o.n ? __ldg(&o.iperm[p]) : p;
-                }
-            }
-        }
-        __syncthreads();
-        // ---- write: half-warp h of warp w, rows 2w + h, 2w + h + 8, ...;
-        // lane l, vertices 4(l % 16)..4(l % 16) + 3
-        {
-            const int i0 = 4 * (lane & 15);
-            ull sv[4];
-            int64_t un[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                sv[j] = sh.seen[i0 + j];
-                un[j] = sh.unreached[i0 + j];
-            }
-            const int64_t v = v0 + i0;
-            for (int r = 2 * warp + (lane >> 4); r < o.lanes; r += 2 * (kMatThreads / 32)) {
-                const int4 dq = *reinterpret_cast<const int4 *>(&sh.depth[r][i0]);
-                const uint4 pq = *reinterpret_cast<const uint4 *>(&sh.parent[r][i0]);
-                const int32_t dd[4] = {dq.x, dq.y, dq.z, dq.w};
-                const uint32_t pp[4] = {pq.x, pq.y, pq.z, pq.w};
-                int32_t d[4];
-                int64_t par[4];
+        const int64_t v = tile * kMatThreads + tid;
+        if (v >= o.n) { continue; }
+        const int64_t t = o.perm ? (int64_t)__ldg(&o.perm[v]) : v;
+        const int64_t deg = __ldg(&o.off[v + 1]) - __ldg(&o.off[v]);
+        const ull s = __ldcs(&o.seen[t]) & all;
+        ull plane[4] = {0ull, 0ull, 0ull, 0ull};
+        ull row_lanes = 0;  // lanes read from their rows in the write loop
+        if (s) {
+            const uint4 *rv = o.rec + t * kRecSlots;
+            // the first two slots are read together with the count (they lie
+            // in the vertex's record block whatever the count says)
+            const uint4 x0 = __ldcs(&rv[0]), x1 = __ldcs(&rv[1]);
+            const unsigned cnt = min(__ldcs(&o.rec_cnt[t]), kRecSlots);
+            ull left = s;
+            for (unsigned k0 = 0; k0 < cnt && left; k0 += 4) {
+                uint4 x[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const bool got = (sv[j] >> r) & 1ull;
-                    d[j] = got ? dd[j] : -1;
-                    par[j] = got ? (int64_t)pp[j] : un[j];
+                    x[j] = (k0 == 0 && j < 2) ? (j ? x1 : x0)
+                                              : (k0 + j < cnt ? __ldcs(&rv[k0 + j])
+                                                              : make_uint4(0, 0, 0, 0));
                 }
-                const int64_t at = (int64_t)r * o.n + v;
-                if (vec) {
-                    if (v < o.n) {
-                        __stcs(reinterpret_cast<int4 *>(o.depth_out + at),
-                               make_int4(d[0], d[1], d[2], d[3]));
-                        __stcs(reinterpret_cast<longlong2 *>(o.parent_out + at),
-                               make_longlong2(par[0], par[1]));
-                        __stcs(reinterpret_cast<longlong2 *>(o.parent_out + at + 2),
-                               make_longlong2(par[2], par[3]));
-                    }
-                } else {
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        if (v + j < o.n) {
-                            __stcs(o.depth_out + at + j, d[j]);
-                            __stcs(o.parent_out + at + j, par[j]);
+                for (int j = 0; j < 4; ++j) {
+                    const ull mask = k0 + j < cnt ? (((ull)x[j].y << 32) | x[j].x) & left : 0ull;
+                    if (!mask) { continue; }
+                    left &= ~mask;
+                    const unsigned k = k0 + j;
+                    // (a provider id out of range would only come from a
+                    // broken record; it is passed through, not followed)
+                    tab[k * kMatThreads + tid] = make_uint2(
+                        x[j].w, o.iperm && x[j].z < o.n ? __ldg(&o.iperm[x[j].z]) : x[j].z);
+                    mat_set_slot(plane, k, mask);
+                }
+            }
+            // lanes past the records: their rows, four loads in flight; lanes
+            // with the (depth, parent) pair of the previous one share its slot
+            unsigned used = cnt;
+            int32_t last_d = -2;
+            uint32_t last_p = 0;
+            unsigned last_k = kMatSlots;
+            while (left) {
+                int rr[4];
+                int32_t dd[4];
+                uint32_t pp[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    rr[j] = left ? __ffsll((long long)left) - 1 : -1;
+                    left &= left ? left - 1 : 0ull;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    dd[j] = rr[j] >= 0 ? __ldcs(&o.depth[t * o.R + rr[j]]) : 0;
+                    pp[j] = rr[j] >= 0 ? __ldcs(&o.parent[t * o.R + rr[j]]) : 0u;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (rr[j] < 0) { continue; }
+                    if (dd[j] != last_d || pp[j] != last_p) {
+                        last_d = dd[j];
+                        last_p = pp[j];
+                        last_k = kMatSlots;
+                        if (used < kMatSlots) {
+                            last_k = used++;
+                            tab[last_k * kMatThreads + tid] = make_uint2(
+                                (uint32_t)dd[j],
+                                o.iperm && pp[j] < o.n ? __ldg(&o.iperm[pp[j]]) : pp[j]);
                         }
+                    }
+                    const ull bit = 1ull << rr[j];
+                    if (last_k < kMatSlots) {
+                        mat_set_slot(plane, last_k, bit);
+                    } else {
+                        row_lanes |= bit;
                     }
                 }
             }
         }
-        __syncthreads();
+        const int64_t unreached = deg != 0 ? -deg : -1;
+        int32_t *dp = o.depth_out + v;
+        int64_t *pq = o.parent_out + v;
+        // two halves of 32 lanes, so that the planes shift as 32-bit words
+        for (int h = 0; h < 2 && 32 * h < o.lanes; ++h) {
+            uint32_t g = (uint32_t)(s >> (32 * h)), rw = (uint32_t)(row_lanes >> (32 * h));
+            uint32_t q0 = (uint32_t)(plane[0] >> (32 * h)), q1 = (uint32_t)(plane[1] >> (32 * h));
+            uint32_t q2 = (uint32_t)(plane[2] >> (32 * h)), q3 = (uint32_t)(plane[3] >> (32 * h));
+            const int end = min(32, o.lanes - 32 * h);
+            for (int j = 0; j < end; ++j) {
+                const unsigned k = (q0 & 1u) | ((q1 & 1u) << 1) | ((q2 & 1u) << 2) | ((q3 & 1u) << 3);
+                const uint2 e = tab[k * kMatThreads + tid];
+                int32_t d = (int32_t)e.x;
+                int64_t par = (int64_t)e.y;
+                if (rw & 1u) {  // more pairs than slots: the lane's own row
+                    const int r = 32 * h + j;
+                    const uint32_t pr = __ldcs(&o.parent[t * o.R + r]);
+                    d = __ldcs(&o.depth[t * o.R + r]);
+                    par = (int64_t)(o.iperm && pr < o.n ? __ldg(&o.iperm[pr]) : pr);
+                }
+                const bool got = g & 1u;
+                __stcs(dp, got ? d : -1);
+                __stcs(pq, got ? par : unreached);
+                dp += o.n;
+                pq += o.n;
+                g >>= 1;
+                rw >>= 1;
+                q0 >>= 1;
+                q1 >>= 1;
+                q2 >>= 1;
+                q3 >>= 1;
+            }
+        }
     }
 }
 

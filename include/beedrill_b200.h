@@ -374,13 +374,21 @@ bd_status bd_graph_check_components(const bd_graph *g, const int64_t *component,
  * every step in place of the alpha/beta rule (hybrid_bfs.cc:166-188).
  * Parameter vector, BD_POLICY_PARAMS floats:
  *   w1[32][8], b1[32], w2[32][32], b2[32], w3[2][32], b3[2].
- * Features per step (raw, before standardisation with mean / inv_std):
- *   log2(1+frontier vertices), log2(1+frontier degree sum m_f),
- *   log2(1+unexplored degree sum m_u), level, log2(1+n), log2(1+m),
- *   previous direction (0 top-down, 1 bottom-up),
- *   log2(1+previous step time in microseconds).
+ * Features per step (raw, before standardisation with mean / inv_std), with
+ * L(x) = log2(1 + x), all free of the graph's size:
+ *   L(m_f) - L(m_u)            frontier degree sum vs unexplored degree sum
+ *   L(frontier) - L(n)         frontier vertices vs vertices
+ *   L(m_u) - L(2m)             unexplored degree sum vs arcs
+ *   L(level)
+ *   L(m) - L(n)                average degree
+ *   previous direction (0 top-down, 1 bottom-up)
+ *   L(previous step us) - L(m / 2^20)
+ *   L(m_f) - L(frontier)       frontier average degree
  * Output: logits (top-down, bottom-up).  The Beamer rule decides whenever
- * |logit gap| < margin, and always when no policy is installed. */
+ * |logit gap| < margin, whenever a feature lies outside [lo, hi] -- the
+ * kernels test feature 0 first and run the network only inside its range
+ * (the band where the policy may overrule the rule) -- and always when no
+ * policy is installed. */
 #define BD_POLICY_PARAMS 1410
 #define BD_POLICY_FEATURES 8
 /* Installs (or, with params == NULL or margin == +inf, removes) the policy
