@@ -23,12 +23,12 @@
 // Which arcs are joined (symmetric CSR, every edge stored both ways), after
 // Sutton, Ben-Nun and Barak, "Optimizing Parallel Graph Connectivity
 // Computation via Subgraph Sampling" (IPDPS 2018, "Afforest"):
-//   cc_sample_kernel      every vertex joins its first kSampleArcs arcs,
-//                         one round per arc position, then every vertex is
-//                         pointed at its root (cc_flatten_kernel);
+//   cc_sample_kernel      every vertex joins its first arc, then its second,
+//                         each round followed by pointing every vertex at
+//                         its root (cc_flatten_kernel);
 //   the largest tree      found by sampling kProbe vertices' roots;
-//   cc_finish_kernel      every vertex OUTSIDE that tree joins the rest of
-//                         its arcs.  An edge between the largest tree and
+//   cc_walk_kernel        every vertex OUTSIDE that tree (its parent word is
+//                         not the tree's root) joins the rest of its arcs.  An edge between the largest tree and
 //                         another vertex is stored at that other vertex
 //                         too, and is joined from there, so skipping the
 //                         largest tree's own arcs loses no edge.  A warp
@@ -55,7 +55,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int64_t kHeavy = 4096;    // arcs above which a vertex is split over the grid
-constexpr int kSampleArcs = 2;      // arc positions joined before the largest tree is found
+constexpr int kSampleArcs = 2;      // arc positions joined before the rest of the lists
 constexpr int kProbe = 1024;        // vertices whose roots vote for the largest tree
 constexpr int64_t kHeavyChunk = 1024;  // arcs per unit of the heavy pass
 
@@ -412,11 +412,15 @@ bd_status bd_components_run(bd_components *c, bd_components_stats *stats)
     uint32_t skip = ~0u;
     int first = 0;
     if (g->symmetric) {
+        // the first and the second arc of every vertex, each round followed
+        // by pointing every vertex at its root (the next round's finds are
+        // short, and after the last one the largest tree's vertices are
+        // recognised by one parent word)
         for (int pos = 0; pos < bd::kSampleArcs; ++pos) {
             bd::cc_sample_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(g->d_off, g->d_adj, n,
                                                                          pos, c->parent);
+            bd::cc_flatten_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(c->parent, n);
         }
-        bd::cc_flatten_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(c->parent, n);
         bd::cc_probe_kernel<<<(bd::kProbe + 255) / 256, 256, 0, s>>>(c->parent, n, c->probe);
         BD_CUDA(cudaGetLastError());
         std::vector<uint32_t> probe(bd::kProbe);

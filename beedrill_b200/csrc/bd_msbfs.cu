@@ -360,7 +360,7 @@ __device__ __forceinline__ void push_arcs(const MsParams &p, MsAcc *acc, int cur
     for (int i = 0; i < kPushU; ++i) {
         deg[i] = 0;
         if (g[i]) {
-            write_rows(p, v[i], g[i], new_level, src[i]);
+            record_shared(p, v[i], g[i], new_level, src[i]);
             loc.lanes += __popcll(g[i]);
             loc.lanes_or |= g[i];
         }
