@@ -23,26 +23,28 @@
 // Which arcs are joined (symmetric CSR, every edge stored both ways), after
 // Sutton, Ben-Nun and Barak, "Optimizing Parallel Graph Connectivity
 // Computation via Subgraph Sampling" (IPDPS 2018, "Afforest"):
-//   cc_sample_kernel      every vertex joins its first arc, then its second,
-//                         each round followed by pointing every vertex at
-//                         its root (cc_flatten_kernel);
+//   cc_sample_first_kernel, cc_sample_second_kernel
+//                         every vertex joins its first arc, then its
+//                         second, each round followed by pointing every
+//                         vertex at its root (cc_flatten_kernel);
 //   the largest tree      found by sampling kProbe vertices' roots;
-//   cc_walk_kernel        every vertex OUTSIDE that tree (its parent word is
-//                         not the tree's root) joins the rest of its arcs.  An edge between the largest tree and
+//   cc_walk_kernel        every vertex OUTSIDE that tree (its parent word
+//                         is not the tree's root) joins the rest of its
+//                         arcs.  An edge between the largest tree and
 //                         another vertex is stored at that other vertex
 //                         too, and is joined from there, so skipping the
 //                         largest tree's own arcs loses no edge.  A warp
-//                         loads 32 vertices' roots at once and walks only
-//                         the lists of those with work; lists of more than
-//                         kHeavy arcs go to cc_finish_heavy_kernel, which
+//                         loads 32 vertices' parent words at once and walks
+//                         only the lists of those with work; lists of more
+//                         than kHeavy arcs go to cc_heavy_kernel, which
 //                         deals every listed vertex's arcs over the grid in
-//                         one flat range (a binary search per chunk).
+//                         one flat range (a binary search per chunk, the
+//                         chunk prefix from cc_heavy_chunks_kernel).
 //   cc_compress_kernel    labels (each vertex's root), sizes per label
 //                         (one atomic per distinct label of a warp) and the
 //                         count of roots.
-// A CSR that does not hold every edge both ways takes every arc instead
-// (cc_hook_kernel / cc_hook_heavy_kernel, the same warp walk over all
-// vertices).
+// A CSR that does not hold every edge both ways takes every arc of every
+// vertex instead (the same cc_walk_kernel / cc_heavy_kernel pair).
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -74,11 +76,23 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x)
 }
 
 // Root of x's tree, pointing each vertex on the way at its grandparent.
+//
+// The loads go through L1 (ld.ca), which is not coherent between SMs, so a
+// load may return an older value of a parent word.  That is safe: every
+// value a parent word ever holds is an ancestor of its vertex with a
+// smaller id (links and path splitting only write ancestors, and a tree
+// only grows), so a stale walk still descends strictly and ends at a
+// vertex that is, or was, a root of x's tree.  A join acts on such a root
+// only through atomicCAS, which sees the current word.  What L1 buys: after
+// a sampling round nearly every vertex points at the largest tree's root,
+// and checking that root's own word from every thread put millions of
+// loads on one L2 slice (a second sampling round ran 3x slower than the
+// first); from L1 each SM loads it once.
 __device__ __forceinline__ uint32_t cc_find(uint32_t *parent, uint32_t x)
 {
-    uint32_t p = __ldcg(&parent[x]);
+    uint32_t p = __ldca(&parent[x]);
     while (p != x) {
-        const uint32_t gp = __ldcg(&parent[p]);
+        const uint32_t gp = __ldca(&parent[p]);
         if (gp != p) { __stcg(&parent[x], gp); }
         x = p;
         p = gp;
@@ -86,9 +100,24 @@ __device__ __forceinline__ uint32_t cc_find(uint32_t *parent, uint32_t x)
     return x;
 }
 
+// Root of x's tree without writes, for passes in which no join runs (the
+// roots stay fixed, so the walk ends at x's current root).
+__device__ __forceinline__ uint32_t cc_root(const uint32_t *parent, uint32_t x)
+{
+    uint32_t p = __ldca(&parent[x]);
+    while (p != x) {
+        x = p;
+        p = __ldca(&parent[x]);
+    }
+    return x;
+}
+
 // Joins the trees of a and b: the larger root goes under the smaller.
 __device__ __forceinline__ void cc_join(uint32_t *parent, uint32_t a, uint32_t b)
 {
+    // one parent word each: vertices pointing at the same vertex share a
+    // tree (after a flatten, the common case)
+    if (__ldca(&parent[a]) == __ldca(&parent[b])) { return; }
     uint32_t ra = cc_find(parent, a), rb = cc_find(parent, b);
     while (ra != rb) {
         if (ra < rb) {
@@ -113,24 +142,48 @@ __global__ void cc_init_kernel(uint32_t *parent, int64_t n, int64_t *size)
     }
 }
 
-// Arc position `pos` of every vertex that has one.
-__global__ void cc_sample_kernel(const int64_t *off, const uint32_t *adj, int64_t n, int pos,
-                                 uint32_t *parent)
+// First sampling round: every vertex joins its first arc.  Its second arc
+// (in the same 32-byte sector of the adjacency) is kept in `second` for the
+// next round, which then reads 4 coalesced bytes per vertex instead of two
+// offsets and a random adjacency sector again; a vertex with fewer than two
+// arcs keeps its own id (joining itself does nothing).
+__global__ void cc_sample_first_kernel(const int64_t *off, const uint32_t *adj, int64_t n,
+                                       uint32_t *parent, uint32_t *second)
 {
     for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n;
          u += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t b = off[u];
-        if (off[u + 1] - b > pos) { cc_join(parent, (uint32_t)u, __ldg(&adj[b + pos])); }
+        const int64_t b = off[u], e = off[u + 1];
+        uint32_t nxt = (uint32_t)u;
+        if (e > b) {
+            const uint32_t a0 = __ldg(&adj[b]);
+            if (e - b > 1) { nxt = __ldg(&adj[b + 1]); }
+            cc_join(parent, (uint32_t)u, a0);
+        }
+        __stcs(&second[u], nxt);
     }
 }
 
-// Every vertex pointed at its root.
+// Second sampling round: every vertex joins its second arc.
+__global__ void cc_sample_second_kernel(const uint32_t *second, int64_t n, uint32_t *parent)
+{
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = __ldcs(&second[u]);
+        if (v != (uint32_t)u) { cc_join(parent, (uint32_t)u, v); }
+    }
+}
+
+// Every vertex pointed at its root (a vertex already there is not
+// written).  No join runs meanwhile, so the roots are fixed; the walks do
+// not split paths, so no thread moves a word another thread has already
+// pointed at its root.
 __global__ void cc_flatten_kernel(uint32_t *parent, int64_t n)
 {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
          v += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t r = cc_find(parent, (uint32_t)v);
-        __stcg(&parent[v], r);
+        const uint32_t p = __ldcg(&parent[v]);
+        const uint32_t r = cc_root(parent, p);
+        if (r != p) { __stcg(&parent[v], r); }
     }
 }
 
@@ -275,7 +328,7 @@ __global__ void cc_compress_kernel(uint32_t *parent, int64_t n, uint32_t hint, i
     __shared__ unsigned long long blk_giant, blk_roots;
     const int lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
-        giant = hint < n ? cc_find(parent, hint) : 0xFFFFFFFFu;
+        giant = hint < n ? cc_root(parent, hint) : 0xFFFFFFFFu;
         blk_giant = blk_roots = 0;
     }
     __syncthreads();
@@ -287,7 +340,9 @@ __global__ void cc_compress_kernel(uint32_t *parent, int64_t n, uint32_t hint, i
         const bool valid = v < n;
         uint32_t r = 0xFFFFFFFFu;
         if (valid) {
-            r = cc_find(parent, (uint32_t)v);
+            // a vertex pointing at the largest tree's root needs no walk
+            const uint32_t p = __ldcs(&parent[v]);
+            r = p == g ? g : cc_root(parent, p);
             __stcs(&label[v], (int64_t)r);
         }
         const bool other = valid && r != g;
@@ -416,11 +471,14 @@ bd_status bd_components_run(bd_components *c, bd_components_stats *stats)
         // by pointing every vertex at its root (the next round's finds are
         // short, and after the last one the largest tree's vertices are
         // recognised by one parent word)
-        for (int pos = 0; pos < bd::kSampleArcs; ++pos) {
-            bd::cc_sample_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(g->d_off, g->d_adj, n,
-                                                                         pos, c->parent);
-            bd::cc_flatten_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(c->parent, n);
-        }
+        // (the label array, written only by the final pass, holds the
+        // second arcs meanwhile)
+        uint32_t *second = reinterpret_cast<uint32_t *>(c->label);
+        bd::cc_sample_first_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(
+            g->d_off, g->d_adj, n, c->parent, second);
+        bd::cc_flatten_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(c->parent, n);
+        bd::cc_sample_second_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(second, n, c->parent);
+        bd::cc_flatten_kernel<<<bd::grid_for(n), bd::kThreads, 0, s>>>(c->parent, n);
         bd::cc_probe_kernel<<<(bd::kProbe + 255) / 256, 256, 0, s>>>(c->parent, n, c->probe);
         BD_CUDA(cudaGetLastError());
         std::vector<uint32_t> probe(bd::kProbe);
