@@ -90,6 +90,41 @@ def test_heavy_vertices_and_small_graphs():
     assert np.array_equal(labels, np.arange(7)) and k == 7 and ok and (sizes == 1).all()
 
 
+def test_relabelled_and_chain_graphs_against_the_oracle():
+    # Ids in random order: the largest component's minimum id is no longer
+    # a hub, so its root moves under smaller ones while joins race (the
+    # finds read parent words that may be stale); a path over a random
+    # permutation builds long chains of links; many small random cycles
+    # give many roots.  Labels must still be the oracle's.
+    rng = np.random.default_rng(77)
+    base = bd.Graph.rmat(16, seed=61)
+    src, dst = base.edges()
+    n = base.num_vertices()
+    perm = rng.permutation(n).astype(np.int64)
+    graphs = [bd.Graph.from_edges(n, perm[src], perm[dst])]
+    k = 50000
+    walk = rng.permutation(k).astype(np.int64)
+    graphs.append(bd.Graph.from_edges(k, walk[:-1], walk[1:]))
+    sizes_c = rng.integers(3, 40, size=2000)
+    order = rng.permutation(int(sizes_c.sum())).astype(np.int64)
+    cs, cd, at = [], [], 0
+    for c in sizes_c:
+        ring = order[at:at + c]
+        cs.append(ring)
+        cd.append(np.roll(ring, 1))
+        at += c
+    graphs.append(bd.Graph.from_edges(int(sizes_c.sum()), np.concatenate(cs), np.concatenate(cd)))
+    for g in graphs:
+        off, adj = g.csr()
+        want, want_sizes, count, _ = O.components(off, adj)
+        labels, sizes, kk, ok = _run(g)
+        assert np.array_equal(labels, want)
+        assert np.array_equal(sizes, want_sizes)
+        assert kk == count and ok
+        g.close()
+    base.close()
+
+
 def test_check_agrees_with_the_oracle_on_planted_labels():
     g = bd.Graph.grid(60, 60, 0.4, seed=5)
     off, adj = g.csr()
