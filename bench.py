@@ -741,9 +741,9 @@ def main():
     else:
         value, e2e_value = value_rank, e2e_rank
 
-    # roofline of the headline way over its timed launches: SURVEY's B_alg
-    # (one CSR pass per group + every root's int32 depth and int64 parent of
-    # each reached vertex) over the device time of the groups, which covers
+    # roofline of the headline way over its timed launches: the algorithmic
+    # bytes B_alg (one CSR pass per group + every root's int32 depth and
+    # int64 parent of each reached vertex) over the device time of the groups, which covers
     # the traversal kernel, the per-lane counts and the result rows
     achieved = float(head["b_alg"].sum() / (head["ms"].sum() * 1e-3) / 1e9)
     peak, peak_kind = peaks()
