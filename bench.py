@@ -160,6 +160,18 @@ def reference_cpu_run(el64_path: str, trials: int, timeout: float):
 REF_ROOTS_PER_STEP = 8
 
 
+def workload_config(desc: str, num_roots: int, scale, graph_seed: int, n: int, m: int) -> dict:
+    """The `config` object of a graph workload: what was run, nothing about
+    how.  Both arms print the same object for the same workload."""
+    return {
+        "workload": f"{desc}, {num_roots} roots per step",
+        "scale": scale, "edge_factor": EDGE_FACTOR if scale else None, "graph_seed": graph_seed,
+        "num_vertices": n, "num_edges": m, "roots": num_roots, "root_seed": 0,
+        "l2": "inputs larger than L2 (CSR %.2f GB), and L2 flushed (512 MB write) before "
+              "each way's runs on the GPU" % ((8 * (n + 1) + 8 * m) / 1e9),
+    }
+
+
 def write_graph_el64(path: str, scale: int) -> int:
     """Writes the benchmark graph as an el64 file from a child process, so
     the process that times the reference maps none of this repository's
@@ -204,20 +216,20 @@ def impl_reference(args):
     gteps = [e / (ms * 1e-3) / 1e9 for e, ms in timed]
     value = hmean(gteps)
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": float(np.sum([ms for _, ms in timed]) / args.steps),
         "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "i64", "data": "synthetic",
-        "config": {"workload": f"rmat-scale{SCALE}-ef{EDGE_FACTOR} seed {GRAPH_SEED}, "
-                               f"{REF_ROOTS_PER_STEP} lcg(0) roots per step (a bounded sample of "
-                               f"the 64-root step)",
-                   "scale": SCALE, "edge_factor": EDGE_FACTOR, "graph_seed": GRAPH_SEED,
-                   "num_vertices": n, "num_edges": m, "roots_per_step": REF_ROOTS_PER_STEP,
-                   "results": "parent_ complete per root (the reference's run_beamer)"},
+        "config": workload_config(f"rmat-scale{SCALE}-ef{EDGE_FACTOR} seed {GRAPH_SEED}",
+                                  NUM_ROOTS, SCALE, GRAPH_SEED, n, m),
+        "run": {"results": "parent_ complete per root (the reference's run_beamer)",
+                "roots_per_step": REF_ROOTS_PER_STEP,
+                "parallelism": "host CPU, 1 pinned core (serial elision; rank 0 only)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": f"{len(timed)} timed roots after "
-                                   f"{args.warmup * REF_ROOTS_PER_STEP} warm-up roots of lcg(0), "
+                         "sample": f"each step {REF_ROOTS_PER_STEP} lcg(0) roots of the "
+                                   f"{NUM_ROOTS}-root workload: {len(timed)} timed roots after "
+                                   f"{args.warmup * REF_ROOTS_PER_STEP} warm-up roots, "
                                    f"reference serial-elision build on 1 pinned core; process "
                                    f"wall {wall:.0f} s incl. el64 load + graph build"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -772,17 +784,14 @@ def main():
         "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {
-            "workload": f"{desc}, {num_roots} roots per step",
+        "config": workload_config(desc, num_roots, scale, graph_seed, n, m),
+        "run": {
             "mode": best,
             "results": "materialized: every root's int32 depths and int64 parents (caller ids, "
                        "reference encoding) in device memory when the step ends"
                        if "traversal" not in best else "traversal only",
-            "scale": scale, "edge_factor": EDGE_FACTOR if scale else None, "graph_seed": graph_seed,
-            "num_vertices": n, "num_edges": m, "roots": num_roots, "root_seed": rank,
-            "l2": "inputs larger than L2 (CSR %.2f GB), and L2 flushed (512 MB write) before "
-                  "each way's runs" % ((8 * (n + 1) + 8 * m) / 1e9),
-            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "parallelism": f"replicas x{world} (rank r takes lcg(r) roots)" if world > 1
+            else "1 GPU",
             "graph_build_s": round(gen_s, 2),
             "adjacency_order": args.order,
         },
