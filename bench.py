@@ -158,6 +158,8 @@ def reference_cpu_run(el64_path: str, trials: int, timeout: float):
 
 
 REF_ROOTS_PER_STEP = 8
+# B200 HBM3e nominal bandwidth (HGX figure), reported beside the measured peak
+HBM_NOMINAL_GBS = 7700.0
 
 
 def workload_config(desc: str, num_roots: int, scale, graph_seed: int, n: int, m: int) -> dict:
@@ -807,6 +809,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind,
+                     "peak_nominal": HBM_NOMINAL_GBS, "frac_nominal": achieved / HBM_NOMINAL_GBS,
                      "note": ("B_alg per 64-root group = 8(n+1) + 8m + 12 sum n_c" if best.startswith("batched")
                               else "B_alg = 8(n+1) + 8 m_c + 12 n_c per root") +
                              " over the device time of the " + best + " way (traffic: ncu DRAM "
