@@ -323,8 +323,9 @@ __device__ void ms_clear_old(const MsParams &p, const MsView &sv)
 // vertex's record count; every (vertex, lane) pair is delivered exactly
 // once, so no two records hold the same pair; one 16-byte store instead of
 // two 4-byte row stores per lane: 5 % off the scale-24 traversal) -- and an
-// atomicOr on the next frontier word tells which deliverer puts the
-// neighbour on the next frontier's list.
+// atomicOr on the next frontier word, issued together with the reach
+// update rather than after it, tells which deliverer puts the neighbour on
+// the next frontier's list.
 constexpr int kPushU = 4;
 
 // One round of up to kPushU arcs per lane: arc i of this lane goes from
@@ -343,17 +344,23 @@ __device__ __forceinline__ void push_arcs(const MsParams &p, MsAcc *acc, int cur
         const ull have = in[i] ? __ldcg(&p.reach[v[i]]) : ~0ull;
         g[i] = ((dn >> (v[i] & 31)) & 1u) ? 0ull : bits[i] & ~have;
     }
-    bool completed[kPushU];
+    // Both atomics at once.  The frontier word takes the lanes v lacked
+    // when the step began (the reach read above sees every earlier step's
+    // lanes), so it ends up holding exactly the lanes delivered to v in this
+    // step whichever deliverer's reach update lands first; the one writer
+    // that finds it empty lists v, even if others delivered its lanes first.
+    ull old_r[kPushU], old_f[kPushU];
 #pragma unroll
     for (int i = 0; i < kPushU; ++i) {
-        const ull old = g[i] ? atomicOr(&p.reach[v[i]], g[i]) : ~0ull;
-        g[i] &= ~old;
-        completed[i] = g[i] && ((old | g[i]) & p.all) == p.all;
+        old_r[i] = g[i] ? atomicOr(&p.reach[v[i]], g[i]) : ~0ull;
+        old_f[i] = g[i] ? atomicOr(&p.F[nxt][v[i]], g[i]) : ~0ull;
     }
-    bool first[kPushU];
+    bool completed[kPushU], first[kPushU];
 #pragma unroll
     for (int i = 0; i < kPushU; ++i) {
-        first[i] = g[i] && atomicOr(&p.F[nxt][v[i]], g[i]) == 0ull;
+        first[i] = g[i] && old_f[i] == 0ull;
+        g[i] &= ~old_r[i];
+        completed[i] = g[i] && ((old_r[i] | g[i]) & p.all) == p.all;
     }
     int64_t deg[kPushU];
 #pragma unroll
