@@ -60,3 +60,17 @@ def test_ranks_traverse_different_roots():
     assert not np.array_equal(r0, r1)
     deg = np.diff(off)
     assert (deg[r0] > 0).all() and (deg[r1] > 0).all()
+
+
+def test_both_arms_describe_the_workload_alike():
+    # the reference arm and the GPU arm print one `config` object for the
+    # headline workload; how each ran it lives elsewhere in the line
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    desc = f"rmat-scale{bench.SCALE}-ef{bench.EDGE_FACTOR} seed {bench.GRAPH_SEED}"
+    a = bench.workload_config(desc, bench.NUM_ROOTS, bench.SCALE, bench.GRAPH_SEED, 1 << 24, 259835455)
+    b = bench.workload_config(desc, bench.NUM_ROOTS, bench.SCALE, bench.GRAPH_SEED, 1 << 24, 259835455)
+    assert a == b and a["workload"].endswith("64 roots per step")
+    assert a["roots"] == 64 and a["root_seed"] == 0 and "CSR 2.21 GB" in a["l2"]
+    assert not {"mode", "parallelism", "graph_build_s", "roots_per_step"} & set(a)
