@@ -316,8 +316,9 @@ __device__ void ms_clear_old(const MsParams &p, const MsView &sv)
 
 // push: lanes of frontier vertex u flow into neighbours [b, e), four arcs
 // per lane per round with each stage's loads and atomics issued back to
-// back.  One plain read of the neighbour's reach word (and of its done bit,
-// in parallel) filters the arcs that deliver nothing; the atomicOr on the
+// back.  One plain read of the neighbour's reach word filters the arcs
+// that deliver nothing (a vertex every lane has reached holds all lanes in
+// it, so no done-bit read is needed); the atomicOr on the
 // reach word tells each deliverer which lanes it delivered first -- it
 // writes one delivery record for them (a slot from an atomicAdd on the
 // vertex's record count; every (vertex, lane) pair is delivered exactly
@@ -339,10 +340,10 @@ __device__ __forceinline__ void push_arcs(const MsParams &p, MsAcc *acc, int cur
     ull g[kPushU];  // lanes to give, then the lanes this writer delivered first
 #pragma unroll
     for (int i = 0; i < kPushU; ++i) {
-        const uint32_t dn = in[i] ? __ldcg(&p.done[v[i] >> 5]) : ~0u;
-        // a stale read only costs an atomic that changes nothing
+        // a stale read only costs an atomic that changes nothing (a vertex
+        // every lane has reached holds them all in its reach word)
         const ull have = in[i] ? __ldcg(&p.reach[v[i]]) : ~0ull;
-        g[i] = ((dn >> (v[i] & 31)) & 1u) ? 0ull : bits[i] & ~have;
+        g[i] = bits[i] & ~have;
     }
     // Both atomics at once.  The frontier word takes the lanes v lacked
     // when the step began (the reach read above sees every earlier step's
@@ -539,18 +540,22 @@ __device__ void ms_pull_heavy(const MsParams &p, const MsView &sv, MsLocal &loc)
                 if (!__any_sync(kFullMask, f != 0)) { continue; }
                 const ull mine = f & ~warp_excl_or(f);
                 const ull round = warp_or(f);
-                ull old = 0;
-                if (lane == 0) { old = atomicOr(&p.F[nxt][v], round); }
+                ull old = 0, before = 0;
+                if (lane == 0) {
+                    // both atomics at once: the reach update takes the whole
+                    // round (lanes another chunk delivered first are already
+                    // in it), and the one update that completes v marks it
+                    old = atomicOr(&p.F[nxt][v], round);
+                    before = atomicOr(&p.reach[v], round) & p.all;
+                }
                 old = __shfl_sync(kFullMask, old, 0);
                 const ull fresh = round & ~old;
                 if (mine & fresh) { record_shared(p, v, mine & fresh, new_level, u[i]); }
                 const bool first = lane == 0 && old == 0ull;
-                if (lane == 0 && fresh) {
+                if (lane == 0) {
                     loc.lanes += __popcll(fresh);
                     loc.lanes_or |= fresh;
-                    // the chunk whose update completes v's lanes marks it done
-                    const ull before = atomicOr(&p.reach[v], fresh) & p.all;
-                    if (before != p.all && ((before | fresh) & p.all) == p.all) {
+                    if (before != p.all && ((before | round) & p.all) == p.all) {
                         loc.done_degsum += (ull)(ve - vb);
                         atomicOr(&p.done[v >> 5], 1u << (v & 31));
                     }
